@@ -1,0 +1,1051 @@
+// rte_host.cpp -- host side of the B200 RTE solver: context, discretisation set-up and the
+// Neumann driver behind the C ABI of include/rte_b200.h.
+//
+// Reference entry points mirrored (paths inside the reference project):
+//   Neumann()              FisherInfo_IO/src/neumann.cu:23-120
+//   prop_abs()             FisherInfo_IO/src/kernels.cu:704-808
+//   generate_source_beam   FisherInfo_IO/src/dist.cu:66-101 (and CPU package/src/Dist.c:1077-1128)
+//   generate_trans_image   FisherInfo_IO/src/dist.cu:103-161
+//   generate_ref_image     FisherInfo_IO/src/dist.cu:229-268
+//   generate_diag_terms_host FisherInfo_IO/src/dist.cu:362-533 (self-voxel term)
+//   StopIteration          FisherInfo_IO/src/dist.cu:1132-1172
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/rte_b200.h"
+#include "rte_internal.h"
+
+namespace {
+
+inline int ncoef(int L) { return (L + 1) * (L + 1); }
+
+// ---------------------------------------------------------------------------------------
+// Real spherical harmonics (host copy of the device recurrence in rte_kernels.cu).
+// Normalisation K_lm = sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!) (times sqrt2 for m > 0) of the
+// reference's complex basis (FisherInfo_IO/src/sph_harm.cu:19-64), Condon-Shortley phase from
+// P_m^m = (-1)^m (2m-1)!! (1-z^2)^{m/2} (sph_harm.cu:133-137).
+ShTables make_sh_tables() {
+  ShTables t;
+  memset(&t, 0, sizeof t);
+  auto K = [](int l, int m) {
+    double f = 1.0;  // (l+m)!/(l-m)!
+    for (int i = l - m + 1; i <= l + m; i++) f *= (double)i;
+    double k = sqrt((2.0 * l + 1.0) / (4.0 * M_PI) / f);
+    return m > 0 ? k * sqrt(2.0) : k;
+  };
+  for (int m = 0; m <= RTE_MAX_L; m++) {
+    double dfact = 1.0;
+    for (int i = 2 * m - 1; i > 0; i -= 2) dfact *= (double)i;
+    t.Q0[m] = K(m, m) * ((m & 1) ? -1.0 : 1.0) * dfact;
+    for (int l = m + 1; l <= RTE_MAX_L; l++) {
+      int id = l * (l + 1) / 2 + m;
+      t.A[id] = K(l, m) * (2.0 * l - 1.0) / ((double)(l - m) * K(l - 1, m));
+      t.B[id] = (l - 2 >= m) ? K(l, m) * (double)(l + m - 1) / ((double)(l - m) * K(l - 2, m)) : 0.0;
+    }
+  }
+  return t;
+}
+
+void sh_real_host(const ShTables& t, int L, double x, double y, double z, double* R) {
+  double cmv = 1.0, smv = 0.0;
+  for (int m = 0; m <= L; m++) {
+    if (m > 0) {
+      double c2 = cmv * x - smv * y, s2 = cmv * y + smv * x;
+      cmv = c2;
+      smv = s2;
+    }
+    double q2 = 0.0, q1 = t.Q0[m];
+    if (m == 0)
+      R[0] = q1;
+    else {
+      R[m * m + 2 * m] = q1 * cmv;
+      R[m * m] = q1 * smv;
+    }
+    for (int l = m + 1; l <= L; l++) {
+      int id = l * (l + 1) / 2 + m;
+      double q = t.A[id] * z * q1 - t.B[id] * q2;
+      q2 = q1;
+      q1 = q;
+      if (m == 0)
+        R[l * l + l] = q;
+      else {
+        R[l * l + l + m] = q * cmv;
+        R[l * l + l - m] = q * smv;
+      }
+    }
+  }
+}
+
+// Legendre polynomial P_l(u) (m = 0 associated Legendre of sph_harm.cu:172-237).
+double legendre(int l, double u) {
+  double p0 = 1.0, p1 = u;
+  if (l == 0) return 1.0;
+  for (int k = 2; k <= l; k++) {
+    double p2 = ((2.0 * k - 1.0) * u * p1 - (k - 1.0) * p0) / k;
+    p0 = p1;
+    p1 = p2;
+  }
+  return p1;
+}
+
+// Gauss-Legendre nodes/weights on [0,1].
+void gauss01(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.resize(n);
+  w.resize(n);
+  for (int i = 0; i < n; i++) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 200; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; k++) {
+        double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      double dz = p1 / dp;
+      z -= dz;
+      if (fabs(dz) < 1e-17) break;
+    }
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= n; k++) {
+      double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = n * (z * p1 - p0) / (z * z - 1.0);
+    x[i] = 0.5 * (z + 1.0);
+    w[i] = 1.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Self-voxel quadrature.  For each sub-voxel and direction, beta = distance from the
+// sub-voxel centre to the voxel surface.  quad 0 follows FisherInfo_IO/src/dist.cu:404-480
+// (100x100 directions, direction cosines in double, face point in float, cube scaled by delX/2
+// on every axis); quad 1 follows CPU package/src/Kernels_selfsub.c:838-927 (200x200 directions,
+// direction cosines and face point in float, per-axis half widths).  The face tests are made
+// in the reference order and the last hit wins.
+template <typename FT>
+void exit_point(FT sx, FT sy, FT sz, float ii, float jj, float kk, int ssv, float& cx, float& cy, float& cz) {
+  const int face = 1;
+  FT fx, fy, fz;
+  if (sx != 0.0) {
+    for (int fc = 0; fc < 2; fc++) {
+      fx = fc == 0 ? face : -face;
+      fy = (fx - ii * 2.0 / ssv) * sy / sx + jj * 2.0 / ssv;
+      fz = (fx - ii * 2.0 / ssv) * sz / sx + kk * 2.0 / ssv;
+      if (fx <= face && fx >= -face && fy <= face && fy >= -face && fz <= face && fz >= -face && sx * fx >= 0) {
+        cx = fx;
+        cy = fy;
+        cz = fz;
+      }
+    }
+  }
+  if (sy != 0.0) {
+    for (int fc = 0; fc < 2; fc++) {
+      fy = fc == 0 ? face : -face;
+      fz = (fy - jj * 2.0 / ssv) * sz / sy + kk * 2.0 / ssv;
+      fx = (fy - jj * 2.0 / ssv) * sx / sy + ii * 2.0 / ssv;
+      if (fx <= face && fx >= -face && fy <= face && fy >= -face && fz <= face && fz >= -face && sy * fy >= 0) {
+        cx = fx;
+        cy = fy;
+        cz = fz;
+      }
+    }
+  }
+  if (sz != 0.0) {
+    for (int fc = 0; fc < 2; fc++) {
+      fz = fc == 0 ? face : -face;
+      fx = (fz - kk * 2.0 / ssv) * sx / sz + ii * 2.0 / ssv;
+      fy = (fz - kk * 2.0 / ssv) * sy / sz + jj * 2.0 / ssv;
+      if (fx <= face && fx >= -face && fy <= face && fy >= -face && fz <= face && fz >= -face && sz * fz >= 0) {
+        cx = fx;
+        cy = fy;
+        cz = fz;
+      }
+    }
+  }
+}
+
+// Self-term moments.  Dself(mu) W = sum_k mu^k M_k W with
+//   M_k[c][c'] = dth dph / (ssv^3 dV) * (-1)^k/(k+1)! * sum_sub sum_w sin(th) R_c R_c' beta^(k+1),
+// the power series of (1 - exp(-mu beta))/mu (dist.cu:479-500 divides by mu_t).
+struct SelfQuad {
+  int L = -1, quad = -1, ssv = 0;
+  double dx = 0, dy = 0, dz = 0;
+  int nw = 0, nsub = 0;
+  std::vector<double> R;      // [nw][C]
+  std::vector<double> wgt;    // [nw]  sin(theta) dth dph
+  std::vector<double> beta;   // [nsub][nw]
+  double beta_max = 0;
+};
+
+void build_quad(SelfQuad& q, int L, int quad, int ssv, double dx, double dy, double dz, const ShTables& sh) {
+  q.L = L;
+  q.quad = quad;
+  q.ssv = ssv;
+  q.dx = dx;
+  q.dy = dy;
+  q.dz = dz;
+  const int ang = quad == 0 ? 100 : 200;
+  const int C = ncoef(L);
+  q.nw = ang * ang;
+  std::vector<double> th(q.nw), ph(q.nw);
+  for (int t = 0; t < ang; t++)
+    for (int p = 0; p < ang; p++) {
+      th[t * ang + p] = t * M_PI / ang;
+      ph[t * ang + p] = p * 2.0 * M_PI / ang;
+    }
+  const double dth = th[ang] - th[0], dph = ph[1] - ph[0];
+  q.R.assign((size_t)q.nw * C, 0.0);
+  q.wgt.assign(q.nw, 0.0);
+  for (int w = 0; w < q.nw; w++) {
+    double st = sin(th[w]);
+    sh_real_host(sh, L, cos(ph[w]) * st, sin(ph[w]) * st, cos(th[w]), &q.R[(size_t)w * C]);
+    q.wgt[w] = st * dth * dph;
+  }
+  q.nsub = ssv * ssv * ssv;
+  q.beta.assign((size_t)q.nsub * q.nw, 0.0);
+  q.beta_max = 0;
+  int sub = 0;
+  float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+  for (float ii = -ssv / 2.0 + 0.5; ii <= ssv / 2.0 - 0.5; ii++)
+    for (float jj = -ssv / 2.0 + 0.5; jj <= ssv / 2.0 - 0.5; jj++)
+      for (float kk = -ssv / 2.0 + 0.5; kk <= ssv / 2.0 - 0.5; kk++, sub++)
+        for (int w = 0; w < q.nw; w++) {
+          double b;
+          if (quad == 0) {
+            double sx = cos(ph[w]) * sin(th[w]), sy = sin(ph[w]) * sin(th[w]), sz = cos(th[w]);
+            exit_point<double>(sx, sy, sz, ii, jj, kk, ssv, cx, cy, cz);
+            b = sqrt(pow(ii * 2.0 / ssv - cx, 2.0) + pow(jj * 2.0 / ssv - cy, 2.0) + pow(kk * 2.0 / ssv - cz, 2.0)) *
+                dx / 2.0;
+          } else {
+            float sx = cos(ph[w]) * sin(th[w]), sy = sin(ph[w]) * sin(th[w]), sz = cos(th[w]);
+            exit_point<float>(sx, sy, sz, ii, jj, kk, ssv, cx, cy, cz);
+            b = sqrt(pow(ii * 2.0 / ssv - cx, 2.0) * pow(dx / 2.0, 2.0) +
+                     pow(jj * 2.0 / ssv - cy, 2.0) * pow(dy / 2.0, 2.0) +
+                     pow(kk * 2.0 / ssv - cz, 2.0) * pow(dz / 2.0, 2.0));
+          }
+          q.beta[(size_t)sub * q.nw + w] = b;
+          q.beta_max = std::max(q.beta_max, b);
+        }
+}
+
+void build_moments(const SelfQuad& q, int K, double dV, std::vector<double>& mom) {
+  const int C = ncoef(q.L);
+  mom.assign((size_t)K * C * C, 0.0);
+  const int nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::vector<double>> part(nth, std::vector<double>((size_t)K * C * C, 0.0));
+  auto work = [&](int t) {
+    std::vector<double> g(K);
+    std::vector<double>& M = part[t];
+    for (int w = t; w < q.nw; w += nth) {
+      for (int k = 0; k < K; k++) g[k] = 0.0;
+      for (int s = 0; s < q.nsub; s++) {
+        double b = q.beta[(size_t)s * q.nw + w], bp = b;
+        for (int k = 0; k < K; k++) {
+          g[k] += bp;
+          bp *= b;
+        }
+      }
+      const double* R = &q.R[(size_t)w * C];
+      for (int k = 0; k < K; k++) {
+        const double gk = g[k] * q.wgt[w];
+        if (gk == 0.0) continue;
+        double* Mk = &M[(size_t)k * C * C];
+        for (int c = 0; c < C; c++) {
+          const double a = gk * R[c];
+          for (int cp = c; cp < C; cp++) Mk[c * C + cp] += a * R[cp];
+        }
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < nth; t++) th.emplace_back(work, t);
+  for (auto& x : th) x.join();
+  double fact = 1.0;
+  for (int k = 0; k < K; k++) {
+    fact *= (double)(k + 1);  // (k+1)!
+    const double sc = ((k & 1) ? -1.0 : 1.0) / fact / ((double)q.nsub * dV);
+    for (int c = 0; c < C; c++)
+      for (int cp = c; cp < C; cp++) {
+        double v = 0.0;
+        for (int t = 0; t < nth; t++) v += part[t][(size_t)k * C * C + c * C + cp];
+        mom[(size_t)k * C * C + c * C + cp] = v * sc;
+        mom[(size_t)k * C * C + cp * C + c] = v * sc;
+      }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+struct rte_ctx {
+  rte_config cfg;
+  int nx, ny, nz, N, L, C;
+  double dx, dy, dz, dV, cm, prop_thresh;
+  int model, precision, kernel_mode;
+  std::string err;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ShTables sh;
+  SelfQuad quad;
+  int K = 0;  // moments in use
+  int* d_perm = nullptr;
+  double *d_mut = nullptr, *d_mus = nullptr;
+  float* d_mutf = nullptr;
+  double *d_W = nullptr, *d_Wn = nullptr, *d_sum = nullptr, *d_part = nullptr, *d_mom = nullptr;
+  double *d_aux1 = nullptr, *d_aux2 = nullptr, *d_aux3 = nullptr, *d_aux4 = nullptr;  // real-basis staging
+  float* d_Wf = nullptr;
+  float* d_K = nullptr;
+  bool K_valid = false;
+  double* d_cplx = nullptr;
+  double* d_red = nullptr;
+  double* d_img = nullptr;  // trans, ref (complex)
+  std::vector<double> h_mut, h_mus;
+  bool medium_set = false;
+  int nsplit = 1, chunk = 0;
+  size_t bytes = 0;
+  double last_setup_ms = 0.0;
+};
+
+static thread_local std::string g_create_err;
+
+static int fail(rte_ctx* c, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c)
+    c->err = buf;
+  else
+    g_create_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                       \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? RTE_ERR_NOMEM : RTE_ERR_DEVICE,          \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);           \
+  } while (0)
+
+template <class T>
+static cudaError_t dalloc(rte_ctx* c, T** p, size_t n) {
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e == cudaSuccess) c->bytes += n * sizeof(T);
+  return e;
+}
+
+static void free_all(rte_ctx* c) {
+  void* ps[] = {c->d_perm, c->d_mut, c->d_mus, c->d_mutf, c->d_W, c->d_Wn, c->d_sum, c->d_part, c->d_mom,
+                c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->st) cudaStreamDestroy(c->st);
+}
+
+// destination order: Morton (z-order) over (x, y, z) so that a warp's 32 destinations form a
+// compact brick (coherent path walks, shared cache lines of mu_t).
+static std::vector<int> morton_perm(int nx, int ny, int nz) {
+  auto spread = [](uint64_t v) {
+    uint64_t r = 0;
+    for (int b = 0; b < 21; b++) r |= ((v >> b) & 1ull) << (3 * b);
+    return r;
+  };
+  std::vector<std::pair<uint64_t, int>> keys;
+  keys.reserve((size_t)nx * ny * nz);
+  for (int i = 0; i < nz; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nx; k++)
+        keys.push_back({spread(k) | (spread(j) << 1) | (spread(i) << 2), (i * ny + j) * nx + k});
+  std::sort(keys.begin(), keys.end());
+  std::vector<int> p(keys.size());
+  for (size_t q = 0; q < keys.size(); q++) p[q] = keys[q].second;
+  return p;
+}
+
+extern "C" {
+
+int rte_create(const rte_config* cfg, rte_ctx** out) {
+  g_create_err.clear();
+  if (!cfg || !out) return fail(nullptr, RTE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->nx <= 0 || cfg->ny <= 0 || cfg->nz <= 0 || cfg->nx > 1024 || cfg->ny > 1024 || cfg->nz > 1024)
+    return fail(nullptr, RTE_ERR_ARG, "grid %dx%dx%d out of range", cfg->nx, cfg->ny, cfg->nz);
+  if ((long long)cfg->nx * cfg->ny * cfg->nz > (1ll << 26))
+    return fail(nullptr, RTE_ERR_UNSUPPORTED, "more than 2^26 voxels");
+  if (cfg->nL < 0 || cfg->nL > RTE_MAX_L) return fail(nullptr, RTE_ERR_UNSUPPORTED, "nL=%d outside 0..%d", cfg->nL, RTE_MAX_L);
+  if (cfg->model < RTE_MODEL_EXACT || cfg->model > RTE_MODEL_CPU) return fail(nullptr, RTE_ERR_ARG, "bad model");
+  if (cfg->precision != RTE_PREC_FP64 && cfg->precision != RTE_PREC_MIXED)
+    return fail(nullptr, RTE_ERR_ARG, "bad precision");
+  if (cfg->n <= 0 || cfg->c <= 0) return fail(nullptr, RTE_ERR_ARG, "refractive index and speed must be > 0");
+  if (cfg->self_sub_vox < 1 || cfg->self_sub_vox > 16) return fail(nullptr, RTE_ERR_ARG, "selfsubVox out of range");
+  rte_ctx* c = new rte_ctx;
+  c->cfg = *cfg;
+  c->nx = cfg->nx;
+  c->ny = cfg->ny;
+  c->nz = cfg->nz;
+  c->N = cfg->nx * cfg->ny * cfg->nz;
+  c->L = cfg->nL;
+  c->C = ncoef(cfg->nL);
+  c->model = cfg->model;
+  c->precision = cfg->precision;
+  c->kernel_mode = cfg->kernel_mode;
+  if (c->model == RTE_MODEL_FIM) {
+    // Geometry extents and propThresh are float fields in the reference (rte.h:58-73) and
+    // cm = C/n with C = 1 is a float (rte.h:108, rte.cu:63).
+    c->dx = (double)((float)cfg->x_max - (float)cfg->x_min) / (double)cfg->nx;
+    c->dy = (double)((float)cfg->y_max - (float)cfg->y_min) / (double)cfg->ny;
+    c->dz = (double)((float)cfg->z_max - (float)cfg->z_min) / (double)cfg->nz;
+    c->prop_thresh = (double)(float)cfg->prop_thresh;
+    c->cm = (double)(float)(1.0 / cfg->n);
+  } else {
+    c->dx = (cfg->x_max - cfg->x_min) / cfg->nx;
+    c->dy = (cfg->y_max - cfg->y_min) / cfg->ny;
+    c->dz = (cfg->z_max - cfg->z_min) / cfg->nz;
+    c->prop_thresh = cfg->prop_thresh;
+    c->cm = cfg->c / cfg->n;
+  }
+  if (!(c->dx > 0 && c->dy > 0 && c->dz > 0)) {
+    delete c;
+    return fail(nullptr, RTE_ERR_ARG, "voxel size must be positive");
+  }
+  c->dV = c->dx * c->dy * c->dz;
+  c->sh = make_sh_tables();
+  int rc = RTE_OK;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == RTE_OK)
+      rc = fail(nullptr, e == cudaErrorMemoryAllocation ? RTE_ERR_NOMEM : RTE_ERR_DEVICE, "%s: %s", what,
+                cudaGetErrorString(e));
+  };
+  cu(cudaSetDevice(cfg->device), "cudaSetDevice");
+  if (rc == RTE_OK) cu(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "stream");
+  if (rc == RTE_OK) cu(cudaEventCreate(&c->ev0), "event");
+  if (rc == RTE_OK) cu(cudaEventCreate(&c->ev1), "event");
+  if (rc == RTE_OK) cu(rte_upload_sh_tables(c->sh), "SH tables");
+  const size_t NC = (size_t)c->N * c->C;
+  // split-K: enough CTAs for >= 4 per SM on a 148-SM part
+  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
+  int S = std::max(1, (4 * 148 + tiles - 1) / tiles);
+  if (const char* e = getenv("RTE_NSPLIT")) S = std::max(1, atoi(e));
+  S = std::min(S, std::max(1, c->N / RTE_PAIR_TS));
+  c->chunk = ((c->N + S - 1) / S + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
+  c->nsplit = (c->N + c->chunk - 1) / c->chunk;
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_perm, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_mut, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_mus, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_mutf, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_W, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_Wn, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_sum, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_aux1, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_aux2, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_aux3, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_aux4, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_part, NC * c->nsplit), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_cplx, 2 * NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_red, 8), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 4 * (size_t)c->nx * c->ny), "alloc");
+  if (rc == RTE_OK) {
+    std::vector<int> p = morton_perm(c->nx, c->ny, c->nz);
+    cu(cudaMemcpy(c->d_perm, p.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice), "perm upload");
+  }
+  if (rc != RTE_OK) {
+    free_all(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return RTE_OK;
+}
+
+void rte_destroy(rte_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  cudaStreamSynchronize(c->st);
+  free_all(c);
+  delete c;
+}
+
+const char* rte_last_error(const rte_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+size_t rte_device_bytes(const rte_ctx* c) { return c ? c->bytes : 0; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+static int ensure_moments(rte_ctx* c) {
+  const int quad = c->model == RTE_MODEL_FIM ? 0 : 1;
+  const int ssv = c->cfg.self_sub_vox;
+  if (c->quad.L != c->L || c->quad.quad != quad || c->quad.ssv != ssv)
+    build_quad(c->quad, c->L, quad, ssv, c->dx, c->dy, c->dz, c->sh);
+  double mumax = 0.0;
+  for (double m : c->h_mut) mumax = std::max(mumax, m);
+  const double x = mumax * c->quad.beta_max;
+  // terms until x^(k+1)/(k+1)! is below 1e-18 of the leading term
+  int K = 1;
+  double term = x;
+  while (K < RTE_MAX_MOM && term > 1e-18) {
+    term *= x / (K + 1);
+    K++;
+  }
+  if (x > 12.0 || term > 1e-18)
+    return fail(c, RTE_ERR_UNSUPPORTED, "self-voxel series: mu_t*voxel = %.3g too large", x);
+  K = std::max(K, 4);
+  if (K <= c->K && c->d_mom) return RTE_OK;
+  std::vector<double> mom;
+  build_moments(c->quad, K, c->dV, mom);
+  if (c->d_mom) {
+    cudaFree(c->d_mom);
+    c->bytes -= (size_t)c->K * c->C * c->C * sizeof(double);
+    c->d_mom = nullptr;
+  }
+  CUDA_TRY(c, dalloc(c, &c->d_mom, mom.size()));
+  CUDA_TRY(c, cudaMemcpy(c->d_mom, mom.data(), sizeof(double) * mom.size(), cudaMemcpyHostToDevice));
+  c->K = K;
+  return RTE_OK;
+}
+
+static int upload_medium(rte_ctx* c) {
+  std::vector<float> f(c->N);
+  for (int r = 0; r < c->N; r++) f[r] = (float)c->h_mut[r];
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mut, c->h_mut.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mus, c->h_mus.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mutf, f.data(), sizeof(float) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  c->K_valid = false;
+  c->medium_set = true;
+  return ensure_moments(c);
+}
+
+extern "C" int rte_set_medium_voxel(rte_ctx* c, const double* mua, const double* mus) {
+  if (!c || !mua || !mus) return fail(c, RTE_ERR_ARG, "null argument");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  c->h_mut.resize(c->N);
+  c->h_mus.resize(c->N);
+  for (int r = 0; r < c->N; r++) {
+    if (!(mua[r] >= 0.0) || !(mus[r] >= 0.0)) return fail(c, RTE_ERR_ARG, "negative or NaN coefficient at voxel %d", r);
+    c->h_mut[r] = mua[r] + mus[r];
+    c->h_mus[r] = mus[r];
+  }
+  return upload_medium(c);
+}
+
+extern "C" int rte_set_medium_tissue(rte_ctx* c, const uint8_t* tiss, int ntypes, const double* mua,
+                                     const double* mus) {
+  if (!c || !tiss || !mua || !mus || ntypes <= 0 || ntypes > 256) return fail(c, RTE_ERR_ARG, "bad tissue arguments");
+  std::vector<double> a(c->N), s(c->N);
+  for (int r = 0; r < c->N; r++) {
+    if (tiss[r] >= ntypes) return fail(c, RTE_ERR_ARG, "tissue type %d at voxel %d >= %d", tiss[r], r, ntypes);
+    a[r] = mua[tiss[r]];
+    s[r] = mus[tiss[r]];
+  }
+  return rte_set_medium_voxel(c, a.data(), s.data());
+}
+
+// scatter factor per l (prop_scat_dev, FisherInfo_IO/src/kernels.cu:385-418)
+static void scatter_factors(const rte_ctx* c, int flag, double* s) {
+  for (int l = 0; l <= RTE_MAX_L; l++) {
+    if (c->model == RTE_MODEL_FIM) {
+      if (flag) {
+        // pow(__int2double_rn(g), l): the int parameter truncates g (0.8 -> 0)
+        s[l] = (double)(float)c->cm * pow((double)(int)c->cfg.g, (double)l);
+      } else {
+        s[l] = 1.0;  // flag == 0 (g == 0): out *= mu_s only
+      }
+    } else {
+      s[l] = c->cm * pow(c->cfg.g, (double)l);
+    }
+  }
+}
+
+static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
+  *stored = false;
+  if (c->precision != RTE_PREC_MIXED || c->kernel_mode == RTE_KERNEL_RECOMPUTE) return RTE_OK;
+  const size_t need = (size_t)c->N * c->N * sizeof(float);
+  if (!c->d_K) {
+    size_t fr = 0, tot = 0;
+    CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
+    if (need + (1ull << 30) > fr) {
+      if (c->kernel_mode == RTE_KERNEL_STORE)
+        return fail(c, RTE_ERR_NOMEM, "pair kernel needs %.1f GB, %.1f GB free", need / 1e9, fr / 1e9);
+      return RTE_OK;  // auto: recompute
+    }
+    CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * c->N));
+  }
+  if (!c->K_valid) {
+    PairArgs a;
+    memset(&a, 0, sizeof a);
+    a.N = c->N;
+    a.nx = c->nx;
+    a.ny = c->ny;
+    a.nz = c->nz;
+    a.Cfull = c->C;
+    a.dx = c->dx;
+    a.dy = c->dy;
+    a.dz = c->dz;
+    a.prop_thresh = c->prop_thresh;
+    a.kscale = c->dV / c->cm;
+    a.perm = c->d_perm;
+    a.mut = c->d_mut;
+    a.Kmat = c->d_K;
+    // one source chunk per 128 destinations is plenty of parallelism here
+    const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
+    int S = std::max(1, (8 * 148 + tiles - 1) / tiles);
+    a.chunk = (c->N + S - 1) / S;
+    a.nsplit = (c->N + a.chunk - 1) / a.chunk;
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
+    CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->st));
+    CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_setup_ms = ms;
+    c->K_valid = true;
+  }
+  *stored = true;
+  return RTE_OK;
+}
+
+// One term on the real basis: out = [D] A in.  in64 is FP64 (and inf its FP32 copy for the
+// mixed kernels).  sum != null accumulates the result.  red receives the norms.
+static int apply_term(rte_ctx* c, const double* in64, const float* in32, double* out, float* out32, double* sum,
+                      int flag, int flag_scat) {
+  const int LA = flag ? c->L : 0;
+  bool stored = false;
+  int rc = ensure_pair_kernel(c, &stored);
+  if (rc) return rc;
+  PairArgs a;
+  memset(&a, 0, sizeof a);
+  a.N = c->N;
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  a.Cfull = c->C;
+  a.dx = c->dx;
+  a.dy = c->dy;
+  a.dz = c->dz;
+  a.prop_thresh = c->prop_thresh;
+  a.kscale = c->dV / c->cm;
+  a.perm = c->d_perm;
+  a.mut = c->d_mut;
+  a.mutf = c->d_mutf;
+  a.Win = in64;
+  a.Winf = in32;
+  a.Kmat = c->d_K;
+  a.part = c->d_part;
+  a.chunk = c->chunk;
+  a.nsplit = c->nsplit;
+  CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
+  EpiArgs e;
+  memset(&e, 0, sizeof e);
+  e.N = c->N;
+  e.nx = c->nx;
+  e.ny = c->ny;
+  e.nz = c->nz;
+  e.Cfull = c->C;
+  e.S = c->nsplit;
+  e.part = c->d_part;
+  e.Win = in64;
+  e.mut = c->d_mut;
+  e.mus = c->d_mus;
+  e.mom = c->d_mom;
+  e.K = c->K;
+  e.self_scale = c->dV / c->cm;
+  e.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
+  e.flag_scat = flag_scat;
+  scatter_factors(c, flag, e.scat);
+  e.Wout = out;
+  e.Woutf = out32;
+  e.sum = sum;
+  e.red = c->d_red;
+  CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
+  CUDA_TRY(c, rte_launch_epilogue(e, LA, c->st));
+  return RTE_OK;
+}
+
+// Neumann series on one real part.  W0 (FP64 real) is the first term, S0 the initial running
+// sum; the result A * sum is written to `res`.  rule/max_terms/tol as rte_stop.  When force_terms
+// >= 0 exactly that many terms are taken (used for the second real part of complex input).
+static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* res, int flag, const rte_stop* stop,
+                        int force_terms, int* nterms, double* last_rel) {
+  const size_t NC = (size_t)c->N * c->C;
+  const bool mixed = c->precision == RTE_PREC_MIXED;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_sum, S0, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  int terms = 0;
+  double rel = 0.0;
+  if (flag) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_W, W0, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_W, c->d_Wf, NC, c->st));
+    const int flag_l = c->cfg.g != 0.0 ? 1 : 0;  // neumann.cu:74-79
+    const int rule = force_terms >= 0 ? RTE_STOP_FIXED : stop->rule;
+    const int maxt = force_terms >= 0 ? force_terms : (rule == RTE_STOP_REFERENCE ? 10000 : stop->max_terms);
+    int n = c->model == RTE_MODEL_CPU ? 1 : 2;  // CPU package starts n at 1, FIM at 2
+    double fi = 1.0;
+    double hred[4] = {0, 0, 0, 0};
+    if (rule == RTE_STOP_REFERENCE) {
+      CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
+      CUDA_TRY(c, rte_launch_layer_sums(c->d_W, c->d_sum, c->N, c->nx, c->ny, c->nz, c->C, c->d_red, c->st));
+      CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+    }
+    for (;;) {
+      if (rule == RTE_STOP_REFERENCE) {
+        // StopIteration (dist.cu:1132-1172) on the layer sums of W and the running sum
+        const double sumW = hred[2], sumOut = hred[3];
+        double hi = 0.0;
+        bool stopnow = false;
+        if (n > 1) {
+          if (sumOut == 0.0) {
+            stopnow = true;
+          } else {
+            hi = 1.0 - (sumW / sumOut) * (1.0 / (1.0 - (sumW / sumOut) / fi));
+            fi = sumW / sumOut;
+            if (hi > 1.0 || hi < 0.0) hi = 0.0;
+          }
+        }
+        if (stopnow || hi > 0.9999 || terms >= maxt) break;
+      } else if (terms >= maxt) {
+        break;
+      }
+      n++;
+      int rc = apply_term(c, c->d_W, c->d_Wf, c->d_Wn, mixed ? c->d_Wf : nullptr, c->d_sum, flag_l, 1);
+      if (rc) return rc;
+      std::swap(c->d_W, c->d_Wn);
+      terms++;
+      if (rule != RTE_STOP_FIXED) {
+        CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CUDA_TRY(c, cudaStreamSynchronize(c->st));
+        rel = hred[1] > 0 ? sqrt(hred[0] / hred[1]) : 0.0;
+        if (rule == RTE_STOP_REL_L2 && rel < stop->tol) break;
+      }
+    }
+  }
+  // final A on the running sum (no scatter), neumann.cu:95-118
+  float* in32 = nullptr;
+  if (mixed) {
+    CUDA_TRY(c, rte_launch_f64_to_f32(c->d_sum, c->d_Wf, NC, c->st));
+    in32 = c->d_Wf;
+  }
+  int rc = apply_term(c, c->d_sum, in32, res, nullptr, nullptr, 1, 0);
+  if (rc) return rc;
+  if (nterms) *nterms = terms;
+  if (last_rel) *last_rel = rel;
+  return RTE_OK;
+}
+
+// complex (host) -> real parts on the device; returns whether the second (imaginary-function)
+// part is non-zero.
+static int upload_cplx(rte_ctx* c, const rte_cplx* h, double* u1, double* u2, bool* has2) {
+  const size_t NC = (size_t)c->N * c->C;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_cplx, h, NC * sizeof(rte_cplx), cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_red + 4, 0, sizeof(double), c->st));
+  CUDA_TRY(c, rte_launch_to_real(c->d_cplx, u1, u2, c->N, c->L, c->d_red + 4, c->st));
+  double n2 = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&n2, c->d_red + 4, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  *has2 = n2 > 0.0;
+  return RTE_OK;
+}
+
+static int download_cplx(rte_ctx* c, const double* u1, const double* u2, rte_cplx* h) {
+  const size_t NC = (size_t)c->N * c->C;
+  CUDA_TRY(c, rte_launch_to_cplx(u1, u2, c->d_cplx, c->N, c->L, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(h, c->d_cplx, NC * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  return RTE_OK;
+}
+
+extern "C" int rte_prop_abs(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int flag, int flag_scat) {
+  if (!c || !in || !out) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  bool has2 = false;
+  int rc = upload_cplx(c, in, c->d_aux1, c->d_aux2, &has2);
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C;
+  const bool mixed = c->precision == RTE_PREC_MIXED;
+  // part 1 -> d_W, part 2 -> d_sum (both scratch here)
+  if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_aux1, c->d_Wf, NC, c->st));
+  rc = apply_term(c, c->d_aux1, c->d_Wf, c->d_W, nullptr, nullptr, flag, flag_scat);
+  if (rc) return rc;
+  if (has2) {
+    if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_aux2, c->d_Wf, NC, c->st));
+    rc = apply_term(c, c->d_aux2, c->d_Wf, c->d_sum, nullptr, nullptr, flag, flag_scat);
+    if (rc) return rc;
+  }
+  return download_cplx(c, c->d_W, has2 ? c->d_sum : nullptr, out);
+}
+
+extern "C" int rte_neumann(rte_ctx* c, const rte_cplx* src, rte_cplx* out, int flag, const rte_stop* stop,
+                           int* nterms) {
+  if (!c || !out || (flag && (!src || !stop))) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  // real parts: src -> (aux1, aux2), out -> (aux3, aux4); each Neumann copies its inputs
+  // into its own work buffers first, so the result of part k overwrites the input sum of part k.
+  bool o_has2 = false, s_has2 = false;
+  int rc = upload_cplx(c, out, c->d_aux3, c->d_aux4, &o_has2);
+  if (rc) return rc;
+  if (flag) {
+    rc = upload_cplx(c, src, c->d_aux1, c->d_aux2, &s_has2);
+    if (rc) return rc;
+  }
+  int terms = 0;
+  double rel = 0;
+  rc = neumann_real(c, c->d_aux1, c->d_aux3, c->d_aux3, flag, stop, -1, &terms, &rel);
+  if (rc) return rc;
+  const bool has2 = o_has2 || s_has2;
+  if (has2) {
+    rc = neumann_real(c, c->d_aux2, c->d_aux4, c->d_aux4, flag, stop, terms, nullptr, nullptr);
+    if (rc) return rc;
+  }
+  rc = download_cplx(c, c->d_aux3, has2 ? c->d_aux4 : nullptr, out);
+  if (rc) return rc;
+  if (nterms) *nterms = terms;
+  return RTE_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Sources (real basis: the beam is m = 0 only, where both bases coincide).
+static int source_columns(const rte_ctx* c, const rte_source* s, std::vector<int>& cols, double& scale) {
+  cols.clear();
+  scale = 1.0;
+  if (s->kind == RTE_SRC_FIM) {
+    // k == nX/2.0 && j == nY/2.0 (dist.cu:76): no column for odd grids
+    if (c->nx % 2 == 0 && c->ny % 2 == 0) cols.push_back((c->ny / 2) * c->nx + c->nx / 2);
+    return RTE_OK;
+  }
+  if (s->kind == RTE_SRC_CPU) {
+    for (int j = 0; j < c->ny; j++)
+      for (int k = 0; k < c->nx; k++) {
+        const double xs = (double)k * c->dx + c->cfg.x_min + c->dx / 2.0;
+        const double ys = (double)j * c->dy + c->cfg.y_min + c->dy / 2.0;
+        const double rad = sqrt((xs - s->pos_x) * (xs - s->pos_x) + (ys - s->pos_y) * (ys - s->pos_y));
+        if (rad <= (s->diam + 1.0e-16) / 2.0) cols.push_back(j * c->nx + k);
+      }
+    if (!cols.empty()) scale = s->mag / (double)cols.size();
+    return RTE_OK;
+  }
+  if (s->kind != RTE_SRC_COLUMN) return RTE_ERR_ARG;
+  int cx = (int)floor((s->pos_x - c->cfg.x_min) / c->dx), cy = (int)floor((s->pos_y - c->cfg.y_min) / c->dy);
+  cx = std::min(std::max(cx, 0), c->nx - 1);
+  cy = std::min(std::max(cy, 0), c->ny - 1);
+  cols.push_back(cy * c->nx + cx);
+  scale = s->mag;
+  return RTE_OK;
+}
+
+// xi = D A xi_beam on the pencil columns (dist.cu:66-101; Dist.c:1077-1128 for RTE_SRC_CPU).
+static int make_source(rte_ctx* c, const rte_source* s, std::vector<double>& xi) {
+  if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
+  std::vector<int> cols;
+  double scale;
+  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d", s->kind);
+  xi.assign((size_t)c->N * c->C, 0.0);
+  const int plane = c->nx * c->ny;
+  for (int col : cols) {
+    double att = 1.0;
+    for (int i = 0; i < c->nz; i++) {
+      const int r = i * plane + col;
+      const double mt = c->h_mut[r], ms = c->h_mus[r];
+      double v;
+      if (s->kind == RTE_SRC_CPU) {
+        const double zs = (double)i * c->dz + c->cfg.z_min + c->dz / 2.0;
+        const double tz = zs - c->dz / 2.0;
+        v = (exp(-mt * tz) - exp(-mt * (tz + c->dz)));
+      } else {
+        v = att * (1 - exp(-mt * c->dz));
+        att *= exp(-mt * c->dz);
+      }
+      for (int l = 0; l <= c->L; l++)
+        xi[(size_t)r * c->C + l * l + l] =
+            scale * pow(c->cfg.g, (double)l) * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / c->dV;
+    }
+  }
+  return RTE_OK;
+}
+
+// per-l image weights and the ballistic pixel (dist.cu:103-161, 229-268; Dist.c:134-229)
+static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a, std::vector<int>& ballpix,
+                         std::vector<double>& ballval) {
+  memset(a.wt, 0, sizeof a.wt);
+  memset(a.wr, 0, sizeof a.wr);
+  const double mag = s ? s->mag : 1.0;
+  if (c->model == RTE_MODEL_FIM) {
+    const double fac = 2.0 * M_PI * 1.0 * c->dx * c->dy / sqrt(4.0 * M_PI);
+    for (int l = 0; l <= c->L; l++) {
+      double w = 0;
+      for (int q = 0; q < 100; q++) {
+        const double u = (double)q / (100 - 1.0);
+        w += sqrt(2.0 * l + 1.0) * legendre(l, u) * u / (100 - 1.0);
+      }
+      a.wt[l] = fac * w;
+      a.wr[l] = fac * w * mag;
+    }
+  } else if (c->model == RTE_MODEL_CPU) {
+    const double fac = 2.0 * M_PI * c->dx * c->dy * c->cm / sqrt(4.0 * M_PI);
+    for (int l = 0; l <= c->L; l++) {
+      double w = 0, v = 0;
+      for (int q = 0; q < 100; q++) {
+        const double u = (double)q / 100.0, u2 = (double)q / 100.0 - 1.0;
+        w += sqrt(2.0 * l + 1.0) * legendre(l, u) * u / 100.0;
+        v -= sqrt(2.0 * l + 1.0) * legendre(l, u2) * u2 / 100.0;
+      }
+      a.wt[l] = fac * w;
+      a.wr[l] = fac * v;
+    }
+  } else {
+    const double fac = 2.0 * M_PI * c->dx * c->dy * c->cm / sqrt(4.0 * M_PI);
+    std::vector<double> x, w;
+    gauss01(24, x, w);
+    for (int l = 0; l <= c->L; l++) {
+      double t = 0, f = 0;
+      for (size_t q = 0; q < x.size(); q++) {
+        t += sqrt(2.0 * l + 1.0) * legendre(l, x[q]) * x[q] * w[q];
+        f += sqrt(2.0 * l + 1.0) * legendre(l, -x[q]) * x[q] * w[q];
+      }
+      a.wt[l] = fac * t;
+      a.wr[l] = fac * f;
+    }
+  }
+  ballpix.clear();
+  ballval.clear();
+  if (!s) return RTE_OK;
+  std::vector<int> cols;
+  double scale;
+  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind");
+  const int plane = c->nx * c->ny;
+  for (int col : cols) {
+    double v;
+    if (s->kind == RTE_SRC_CPU) {
+      const double zs = (double)(c->nz - 1) * c->dz + c->cfg.z_min + c->dz / 2.0;
+      v = scale * exp(-c->h_mut[(size_t)(c->nz - 1) * plane + col] * (zs + c->dz / 2.0));
+    } else {
+      v = mag;
+      for (int i = 0; i < c->nz; i++) v *= exp(-c->h_mut[(size_t)i * plane + col] * c->dz);
+    }
+    ballpix.push_back(col);
+    ballval.push_back(v);
+  }
+  return RTE_OK;
+}
+
+static int run_images(rte_ctx* c, const double* d_out1, const double* d_out2, const rte_source* s, rte_cplx* trans,
+                      rte_cplx* ref) {
+  ImgArgs a;
+  memset(&a, 0, sizeof a);
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  a.Cfull = c->C;
+  a.L = c->L;
+  a.out = d_out1;
+  std::vector<int> bp;
+  std::vector<double> bv;
+  int rc = image_weights(c, s, a, bp, bv);
+  if (rc) return rc;
+  a.ball_pix = -1;
+  const size_t np = (size_t)c->nx * c->ny;
+  a.trans = c->d_img;
+  a.ref = c->d_img + 2 * np;
+  CUDA_TRY(c, rte_launch_images(a, c->st));
+  (void)d_out2;
+  std::vector<rte_cplx> ht(np), hr(np);
+  CUDA_TRY(c, cudaMemcpyAsync(ht.data(), a.trans, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(hr.data(), a.ref, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  for (size_t q = 0; q < bp.size(); q++) ht[bp[q]].re += bv[q];
+  if (trans) memcpy(trans, ht.data(), np * sizeof(rte_cplx));
+  if (ref) memcpy(ref, hr.data(), np * sizeof(rte_cplx));
+  return RTE_OK;
+}
+
+extern "C" int rte_source_beam(rte_ctx* c, const rte_source* s, rte_cplx* xi) {
+  if (!c || !s || !xi) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  std::vector<double> u;
+  int rc = make_source(c, s, u);
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C;
+  for (size_t q = 0; q < NC; q++) {
+    xi[q].re = u[q];  // m = 0 only: real and complex coefficients coincide
+    xi[q].im = 0.0;
+  }
+  return RTE_OK;
+}
+
+extern "C" int rte_images(rte_ctx* c, const rte_cplx* out, const rte_source* s, rte_cplx* trans, rte_cplx* ref) {
+  if (!c || !out) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  bool has2 = false;
+  int rc = upload_cplx(c, out, c->d_aux1, c->d_aux2, &has2);
+  if (rc) return rc;
+  rc = run_images(c, c->d_aux1, nullptr, s, trans, ref);
+  if (rc || !has2) return rc;
+  // imaginary-function part: images of part 2 go to the imaginary component
+  const size_t np = (size_t)c->nx * c->ny;
+  std::vector<rte_cplx> t2(np), r2(np);
+  rc = run_images(c, c->d_aux2, nullptr, nullptr, t2.data(), r2.data());
+  if (rc) return rc;
+  for (size_t q = 0; q < np; q++) {
+    if (trans) trans[q].im += t2[q].re;
+    if (ref) ref[q].im += r2[q].re;
+  }
+  return RTE_OK;
+}
+
+extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop, rte_cplx* W_out, rte_cplx* trans,
+                           rte_cplx* ref, rte_report* rep) {
+  if (!c || !s || !stop) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  std::vector<double> xi;
+  int rc = make_source(c, s, xi);
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_aux1, xi.data(), NC * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  cudaEvent_t t0, t1;
+  CUDA_TRY(c, cudaEventCreate(&t0));
+  CUDA_TRY(c, cudaEventCreate(&t1));
+  CUDA_TRY(c, cudaEventRecord(t0, c->st));
+  int terms = 0;
+  double rel = 0;
+  rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, &terms, &rel);
+  if (rc) {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
+  }
+  CUDA_TRY(c, cudaEventRecord(t1, c->st));
+  if (W_out) rc = download_cplx(c, c->d_aux2, nullptr, W_out);
+  if (!rc && (trans || ref)) rc = run_images(c, c->d_aux2, nullptr, s, trans, ref);
+  CUDA_TRY(c, cudaEventSynchronize(t1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (rep) {
+    rep->terms = terms;
+    rep->last_rel = rel;
+    rep->ms_device = ms;
+    rep->ms_setup = c->last_setup_ms;
+  }
+  return rc;
+}

@@ -1,0 +1,76 @@
+// rte_internal.h -- shared declarations between the host context (rte_host.cpp) and the
+// sm_100a kernels (rte_kernels.cu).  Not part of the public ABI (include/rte_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define RTE_MAX_L 7
+#define RTE_PAIR_THREADS 128  // destination voxels per CTA (one per thread)
+#define RTE_PAIR_TS 64        // source voxels staged in shared memory per step
+#define RTE_MAX_MOM 48        // self-term power-series terms
+
+struct PairArgs {
+  int N, nx, ny, nz, Cfull;
+  double dx, dy, dz;
+  double prop_thresh;
+  double kscale;        // dV / cm folded into the pair kernel
+  const int* perm;      // destination slot -> voxel index (spatially compact order)
+  const double* mut;    // mu_t per voxel, FP64
+  const float* mutf;    // mu_t per voxel, FP32
+  const double* Win;    // current term, real basis, N x Cfull, FP64
+  const float* Winf;    // current term, FP32 copy
+  float* Kmat;          // stored pair kernel [source voxel][destination slot]
+  double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
+  int chunk;            // source voxels per blockIdx.y
+  int nsplit;           // S
+};
+
+struct EpiArgs {
+  int N, nx, ny, nz, Cfull, S;
+  const double* part;
+  const double* Win;    // input of this term (for the self-voxel term)
+  const double* mut;
+  const double* mus;
+  const double* mom;    // self-term moments [K][Cfull][Cfull]
+  int K;
+  double self_scale;    // dV / cm
+  int air_no_self;      // FIM model: voxels with mu_t == 0 get no self term
+  int flag_scat;
+  double scat[RTE_MAX_L + 1];  // per-l scatter factor (times mu_s of the voxel)
+  double* Wout;         // FP64 result (may alias nothing else)
+  float* Woutf;         // FP32 copy (may be null)
+  double* sum;          // running sum (null = do not accumulate)
+  double* red;          // [0] ||Wout||^2 [1] ||sum||^2 [2] stop-layer sum of Wout [3] of sum
+};
+
+struct ImgArgs {
+  int nx, ny, nz, Cfull, L;
+  const double* out;
+  double wt[RTE_MAX_L + 1];  // transmission weights per l (m = 0 coefficient)
+  double wr[RTE_MAX_L + 1];  // reflection weights per l
+  int ball_pix;              // pixel index of the ballistic term (-1 = none)
+  double ball_val;
+  double* trans;  // nx*ny complex (re, im)
+  double* ref;
+};
+
+// SH recurrence tables (host-computed, see rte_host.cpp) uploaded to __constant__.
+struct ShTables {
+  double A[64], B[64];   // q_l^m = A z q_{l-1}^m - B q_{l-2}^m, index l*(l+1)/2 + m
+  double Q0[RTE_MAX_L + 1];  // q_m^m
+};
+
+extern "C++" {
+cudaError_t rte_upload_sh_tables(const ShTables& t);
+cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
+cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
+cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);
+cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st);
+cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
+                               cudaStream_t st);
+cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L,
+                               cudaStream_t st);
+cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
+                                  double* red, cudaStream_t st);
+cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
+}

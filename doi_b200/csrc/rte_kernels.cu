@@ -1,0 +1,661 @@
+// rte_kernels.cu -- sm_100a kernels of the Neumann-series RTE term W <- D A W.
+//
+// The attenuation operator A of the reference (FisherInfo_IO/src/kernels.cu:151-418,
+// compute_diagonal_abs + compute_propabs + scale_dist_dev, and prop_scat_dev for D) is
+// computed here in a REAL spherical-harmonic basis (the host converts at the boundary):
+//
+//   out[r,c] = sum_{r' != r, |r-r'| < propThresh} R_c(w) k(r,r') sum_c' R_c'(w) W[r',c']
+//            + (dV/cm) sum_c' Dself_cc'(mu_t(r)) W[r,c'],
+//   w = (r - r')/|r - r'|,  k = exp(-tau(r,r')) dV / (cm |r - r'|^2),
+//
+// then D multiplies coefficient (l,m) by scat[l] * mu_s(r).  One CUDA thread owns one
+// destination voxel and streams all source voxels through shared memory (the warp
+// reads the same source at the same time, so source data is a shared-memory
+// broadcast).  The source range is split over blockIdx.y (split-K); the epilogue
+// kernel adds the partial sums in a fixed order, so results are deterministic.
+//
+// Path integrals follow mu_int (FisherInfo_IO/src/kernels.cu:50-148): a Siddon walk
+// between voxel centres whose axis crossings are ordered here with exact integer
+// arithmetic (crossing n on an axis with |delta| = D sits at alpha = (2n+1)/(2D)).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "rte_internal.h"
+
+__constant__ ShTables c_sh;
+__constant__ float c_shAf[64];
+__constant__ float c_shBf[64];
+__constant__ float c_shQ0f[RTE_MAX_L + 1];
+
+cudaError_t rte_upload_sh_tables(const ShTables& t) {
+  float af[64], bf[64], qf[RTE_MAX_L + 1];
+  for (int i = 0; i < 64; i++) {
+    af[i] = (float)t.A[i];
+    bf[i] = (float)t.B[i];
+  }
+  for (int i = 0; i <= RTE_MAX_L; i++) qf[i] = (float)t.Q0[i];
+  cudaError_t e = cudaMemcpyToSymbol(c_sh, &t, sizeof(ShTables));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_shAf, af, sizeof af);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_shBf, bf, sizeof bf);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_shQ0f, qf, sizeof qf);
+  return e;
+}
+
+template <typename T> __device__ __forceinline__ T shA(int i);
+template <typename T> __device__ __forceinline__ T shB(int i);
+template <typename T> __device__ __forceinline__ T shQ0(int i);
+template <> __device__ __forceinline__ double shA<double>(int i) { return c_sh.A[i]; }
+template <> __device__ __forceinline__ double shB<double>(int i) { return c_sh.B[i]; }
+template <> __device__ __forceinline__ double shQ0<double>(int i) { return c_sh.Q0[i]; }
+template <> __device__ __forceinline__ float shA<float>(int i) { return c_shAf[i]; }
+template <> __device__ __forceinline__ float shB<float>(int i) { return c_shBf[i]; }
+template <> __device__ __forceinline__ float shQ0<float>(int i) { return c_shQ0f[i]; }
+
+// Real orthonormal SH R_lm at the unit direction (x, y, z), index l*l + l + m.
+// R_l0 = q_l^0(z), R_l,+m = q_l^m(z) Re((x+iy)^m), R_l,-m = q_l^m(z) Im((x+iy)^m), with the
+// normalised associated-Legendre polynomials q (Condon-Shortley phase included) from the
+// upward recurrence in l.  No trigonometric calls.
+template <int L, typename T>
+__device__ __forceinline__ void sh_eval(T x, T y, T z, T* R) {
+  T cmv = T(1), smv = T(0);
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m > 0) {
+      T c2 = cmv * x - smv * y;
+      T s2 = cmv * y + smv * x;
+      cmv = c2;
+      smv = s2;
+    }
+    T q2 = T(0), q1 = shQ0<T>(m);
+    if (m == 0) {
+      R[0] = q1;
+    } else {
+      R[m * m + 2 * m] = q1 * cmv;
+      R[m * m] = q1 * smv;
+    }
+#pragma unroll
+    for (int l = m + 1; l <= L; ++l) {
+      const int id = l * (l + 1) / 2 + m;
+      T q = shA<T>(id) * z * q1 - shB<T>(id) * q2;
+      q2 = q1;
+      q1 = q;
+      if (m == 0) {
+        R[l * l + l] = q;
+      } else {
+        R[l * l + l + m] = q * cmv;
+        R[l * l + l - m] = q * smv;
+      }
+    }
+  }
+}
+
+// Direction snapped to the reference's 100x100 SH table cell (FisherInfo_IO/src/defines.h:53-56
+// and kernels.cu:326-333: theta = acos(dz/dist), phi = atan2(dy,dx) NOT wrapped to [0,2pi), so a
+// negative phi index reads the previous theta row of the flat table).
+__device__ __forceinline__ void table_direction(double ddx, double ddy, double ddz, double dist, double& ux,
+                                                double& uy, double& uz) {
+  double theta = acos(ddz / dist);
+  double phi = atan2(ddy, ddx);
+  int ti = (int)rintf((float)((100 - 1) * (theta) / (M_PI)));
+  int pj = (int)rintf((float)((100 - 1) * (phi) / (2 * M_PI)));
+  int off = ti * 100 + pj;
+  if (off < 0) off = 0;
+  int tq = off / 100, pq = off - tq * 100;
+  double th = (tq * M_PI) / (100 - 1);
+  double ph = (pq * 2.0 * M_PI) / (100 - 1);
+  double st, ct, sp, cp;
+  sincos(th, &st, &ct);
+  sincos(ph, &sp, &cp);
+  ux = st * cp;
+  uy = st * sp;
+  uz = ct;
+}
+
+// Radiological path sum_v mu_t(v) len(v) between the centres of voxels (i,j,k) and (ip,jp,kp).
+// Axis crossings are compared as integers: with m_a = max(D_a, 1) and Q = 2 m_x m_y m_z, the
+// n-th crossing on axis a is at alpha*Q = (2n+1) * Q / (2 m_a).  Ties step z, then y, then x
+// (as mu_int); a tie leaves a zero-length segment, so the order does not change the sum.
+template <typename A, typename MU>
+__device__ __forceinline__ A path_sum(int i, int j, int k, int ip, int jp, int kp, const MU* __restrict__ mu,
+                                      int nx, int plane, int& Q) {
+  const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
+  const int mz = max(Dz, 1), my = max(Dy, 1), mx = max(Dx, 1);
+  Q = 2 * mx * my * mz;
+  const int BIG = 0x3fffffff;
+  const int incz = 2 * mx * my, incy = 2 * mx * mz, incx = 2 * my * mz;
+  int Az = Dz ? mx * my : BIG, Ay = Dy ? mx * mz : BIG, Ax = Dx ? my * mz : BIG;
+  const int stz = ip > i ? plane : -plane, sty = jp > j ? nx : -nx, stx = kp > k ? 1 : -1;
+  int v = i * plane + j * nx + k;
+  int prev = 0;
+  A acc = A(0);
+  const int steps = Dx + Dy + Dz;
+  for (int s = 0; s < steps; ++s) {
+    const int m = min(Az, min(Ay, Ax));
+    const A muv = (A)__ldg(mu + v);
+    acc = fma(muv, (A)(m - prev), acc);
+    prev = m;
+    const bool bz = Az == m;
+    const bool by = !bz && (Ay == m);
+    const bool bx = !bz && !by;
+    v += bz ? stz : (by ? sty : stx);
+    Az += bz ? incz : 0;
+    Ay += by ? incy : 0;
+    Ax += bx ? incx : 0;
+  }
+  acc = fma((A)__ldg(mu + v), (A)(Q - prev), acc);
+  return acc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Plain FP64 method: every pair recomputed in FP64 (path integral, SH, projections).
+template <int LA, bool TABLE>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  __shared__ double sW[RTE_PAIR_TS * C];
+  const int tid = threadIdx.x;
+  const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
+  const bool act = slot < a.N;
+  const int r = act ? a.perm[slot] : 0;
+  const int plane = a.nx * a.ny;
+  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  double acc[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) acc[c] = 0.0;
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  for (int s0 = sb; s0 < se; s0 += RTE_PAIR_TS) {
+    const int ns = min(RTE_PAIR_TS, se - s0);
+    __syncthreads();
+    for (int q = tid; q < ns * C; q += RTE_PAIR_THREADS) {
+      const int sv = q / C, c = q - sv * C;
+      sW[q] = a.Win[(size_t)(s0 + sv) * a.Cfull + c];
+    }
+    __syncthreads();
+    if (!act) continue;
+    int kp = s0 % a.nx, jp = (s0 / a.nx) % a.ny, ip = s0 / plane;
+    for (int sv = 0; sv < ns; ++sv) {
+      const int rp = s0 + sv;
+      if (rp != r) {
+        const double ddx = (double)(k - kp) * a.dx, ddy = (double)(j - jp) * a.dy, ddz = (double)(i - ip) * a.dz;
+        const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        const double dist = sqrt(d2);
+        if (dist < a.prop_thresh) {
+          double ux, uy, uz;
+          if (TABLE) {
+            table_direction(ddx, ddy, ddz, dist, ux, uy, uz);
+          } else {
+            const double inv = 1.0 / dist;
+            ux = ddx * inv;
+            uy = ddy * inv;
+            uz = ddz * inv;
+          }
+          double R[C];
+          sh_eval<LA, double>(ux, uy, uz, R);
+          double S = 0.0;
+#pragma unroll
+          for (int c = 0; c < C; ++c) S = fma(R[c], sW[sv * C + c], S);
+          int Q;
+          const double ps = path_sum<double, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q);
+          const double tau = ps * dist / (double)Q;
+          const double t = exp(-tau) * a.kscale / d2 * S;
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[c] = fma(R[c], t, acc[c]);
+        }
+      }
+      if (++kp == a.nx) {
+        kp = 0;
+        if (++jp == a.ny) {
+          jp = 0;
+          ++ip;
+        }
+      }
+    }
+  }
+  if (act) {
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * a.Cfull;
+#pragma unroll
+    for (int c = 0; c < C; ++c) o[c] = acc[c];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed precision: path integrals, SH and projections in FP32 (SH in FP64 for l >= 7); FP32
+// partial sums over one shared-memory tile of sources are flushed into FP64 accumulators
+// (shared memory), so no FP32 sum runs over more than RTE_PAIR_TS terms.  STORED reads the
+// precomputed pair kernel k[r'][slot] (FP32) instead of walking the path.
+template <int LA, bool TABLE, bool STORED>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
+  __shared__ float sW[RTE_PAIR_TS * C];
+  extern __shared__ double sAcc[];  // [C][RTE_PAIR_THREADS]
+  const int tid = threadIdx.x;
+  const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
+  const bool act = slot < a.N;
+  const int r = act ? a.perm[slot] : 0;
+  const int plane = a.nx * a.ny;
+  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
+  const float kscalef = (float)a.kscale;
+  const float thr = (float)a.prop_thresh;
+#pragma unroll
+  for (int c = 0; c < C; ++c) sAcc[c * RTE_PAIR_THREADS + tid] = 0.0;
+  float acc[C];
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  for (int s0 = sb; s0 < se; s0 += RTE_PAIR_TS) {
+    const int ns = min(RTE_PAIR_TS, se - s0);
+    __syncthreads();
+    for (int q = tid; q < ns * C; q += RTE_PAIR_THREADS) {
+      const int sv = q / C, c = q - sv * C;
+      sW[q] = a.Winf[(size_t)(s0 + sv) * a.Cfull + c];
+    }
+    __syncthreads();
+    if (!act) continue;
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.f;
+    int kp = s0 % a.nx, jp = (s0 / a.nx) % a.ny, ip = s0 / plane;
+    const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.N + slot : nullptr;
+    float knext = STORED ? __ldg(Kcol) : 0.f;
+    for (int sv = 0; sv < ns; ++sv) {
+      float kk;
+      if (STORED) {
+        kk = knext;
+        if (sv + 1 < ns) knext = __ldg(Kcol + (size_t)(sv + 1) * a.N);
+      }
+      const float ddx = (float)(k - kp) * dxf, ddy = (float)(j - jp) * dyf, ddz = (float)(i - ip) * dzf;
+      const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      bool live;
+      float dist = 0.f;
+      if (STORED) {
+        live = kk != 0.f;
+      } else {
+        dist = sqrtf(d2);
+        live = (s0 + sv != r) && dist < thr;
+      }
+      if (live) {
+        ShT R[C];
+        if (TABLE) {
+          const double ex = (double)(k - kp) * a.dx, ey = (double)(j - jp) * a.dy, ez = (double)(i - ip) * a.dz;
+          double ux, uy, uz;
+          table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
+          sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
+        } else {
+          const float inv = rsqrtf(d2);
+          sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+        }
+        float S = 0.f;
+#pragma unroll
+        for (int c = 0; c < C; ++c) S = fmaf((float)R[c], sW[sv * C + c], S);
+        if (!STORED) {
+          int Q;
+          const float ps = path_sum<float, float>(i, j, k, ip, jp, kp, a.mutf, a.nx, plane, Q);
+          const float tau = ps * dist / (float)Q;
+          kk = __expf(-tau) * kscalef / d2;
+        }
+        const float t = kk * S;
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = fmaf((float)R[c], t, acc[c]);
+      }
+      if (++kp == a.nx) {
+        kp = 0;
+        if (++jp == a.ny) {
+          jp = 0;
+          ++ip;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) sAcc[c * RTE_PAIR_THREADS + tid] += (double)acc[c];
+  }
+  if (act) {
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * a.Cfull;
+#pragma unroll
+    for (int c = 0; c < C; ++c) o[c] = sAcc[c * RTE_PAIR_THREADS + tid];
+  }
+}
+
+// Precompute of the pair kernel k[r'][slot] = exp(-tau) dV/(cm d^2) (0 for r' == r or beyond
+// propThresh), path sums in FP64, stored as FP32.  Coalesced over destination slots.
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_store_kernel(PairArgs a) {
+  const int slot = blockIdx.x * RTE_PAIR_THREADS + threadIdx.x;
+  if (slot >= a.N) return;
+  const int r = a.perm[slot];
+  const int plane = a.nx * a.ny;
+  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  int kp = sb % a.nx, jp = (sb / a.nx) % a.ny, ip = sb / plane;
+  for (int rp = sb; rp < se; ++rp) {
+    float kk = 0.f;
+    if (rp != r) {
+      const double ddx = (double)(k - kp) * a.dx, ddy = (double)(j - jp) * a.dy, ddz = (double)(i - ip) * a.dz;
+      const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      const double dist = sqrt(d2);
+      if (dist < a.prop_thresh) {
+        int Q;
+        const double ps = path_sum<double, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q);
+        kk = (float)(exp(-ps * dist / (double)Q) * a.kscale / d2);
+      }
+    }
+    a.Kmat[(size_t)rp * a.N + slot] = kk;
+    if (++kp == a.nx) {
+      kp = 0;
+      if (++jp == a.ny) {
+        jp = 0;
+        ++ip;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Epilogue: add split-K partials, self-voxel term, scatter; write the next term (FP64 and FP32),
+// accumulate the running sum and the norms used by the stop rules.
+// Self term: Dself(mu) = sum_k mu^k M_k (Horner), see the moment construction in rte_host.cpp.
+template <int LA>
+__global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double w2 = 0.0, s2 = 0.0, lw = 0.0, ls = 0.0;
+  if (r < a.N) {
+    double v[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) v[c] = 0.0;
+    for (int s = 0; s < a.S; ++s) {
+      const double* p = a.part + ((size_t)s * a.N + r) * a.Cfull;
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] += p[c];
+    }
+    const double mu = a.mut[r];
+    if (a.K > 0 && !(a.air_no_self && mu == 0.0)) {
+      double w[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) w[c] = a.Win[(size_t)r * a.Cfull + c];
+      double selfv[C];
+      // Horner in mu per output coefficient: u = sum_k mu^k (M_k w)_c
+      for (int c = 0; c < C; ++c) {
+        double u = 0.0;
+        for (int kk = a.K - 1; kk >= 0; --kk) {
+          const double* Mrow = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
+          double t = 0.0;
+#pragma unroll
+          for (int cp = 0; cp < C; ++cp) t = fma(__ldg(Mrow + cp), w[cp], t);
+          u = fma(mu, u, t);
+        }
+        selfv[c] = u;
+      }
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] = fma(a.self_scale, selfv[c], v[c]);
+    }
+    if (a.flag_scat) {
+      const double ms = a.mus[r];
+#pragma unroll
+      for (int l = 0; l <= LA; ++l)
+#pragma unroll
+        for (int m = -l; m <= l; ++m) v[l * l + l + m] *= a.scat[l] * ms;
+    }
+    const bool stop_layer = (r / (a.nx * a.ny)) == a.nz - 1;
+    for (int c = 0; c < a.Cfull; ++c) {
+      const double x = c < C ? v[c] : 0.0;
+      a.Wout[(size_t)r * a.Cfull + c] = x;
+      if (a.Woutf) a.Woutf[(size_t)r * a.Cfull + c] = (float)x;
+      w2 += x * x;
+      double sv = 0.0;
+      if (a.sum) {
+        sv = a.sum[(size_t)r * a.Cfull + c] + x;
+        a.sum[(size_t)r * a.Cfull + c] = sv;
+        s2 += sv * sv;
+      }
+      if (stop_layer) {
+        // sum of Re(w_lm) over m in the complex basis = R_l0 + sqrt2 * R_l,m for even m > 0
+        int l = 0;
+        while ((l + 1) * (l + 1) <= c) ++l;
+        const int m = c - l * l - l;
+        const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
+        lw += wgt * x;
+        ls += wgt * sv;
+      }
+    }
+  }
+  // block reduction of the four norms
+  __shared__ double red[4][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double vals[4] = {w2, s2, lw, ls};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double x = vals[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][wid] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double x = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += red[threadIdx.x][w];
+    atomicAdd(a.red + threadIdx.x, x);
+  }
+}
+
+// Exitance images of the z = nZ-1 and z = 0 faces from the m = 0 coefficients
+// (FisherInfo_IO/src/dist.cu:103-161, 229-268; the per-l weights come from the host).
+__global__ void k_images(ImgArgs a, const double* out_im) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.nx * a.ny) return;
+  const size_t rt = (size_t)(a.nz - 1) * a.nx * a.ny + p, rr = (size_t)p;
+  double t = 0.0, f = 0.0, ti = 0.0, fi = 0.0;
+  for (int l = 0; l <= a.L; ++l) {
+    const int c = l * l + l;
+    t += a.wt[l] * a.out[rt * a.Cfull + c];
+    f += a.wr[l] * a.out[rr * a.Cfull + c];
+    if (out_im) {
+      ti += a.wt[l] * out_im[rt * a.Cfull + c];
+      fi += a.wr[l] * out_im[rr * a.Cfull + c];
+    }
+  }
+  if (p == a.ball_pix) t += a.ball_val;
+  if (a.trans) {
+    a.trans[2 * p] = t;
+    a.trans[2 * p + 1] = ti;
+  }
+  if (a.ref) {
+    a.ref[2 * p] = f;
+    a.ref[2 * p + 1] = fi;
+  }
+}
+
+// Complex reference basis <-> real basis.  w = w1 + i w2 with w1, w2 the coefficient sets of
+// real functions (w_{l,-m} = (-1)^m conj(w_{l,m})).  u_l0 = Re(w_l0), u_l,m = sqrt2 Re(w_lm),
+// u_l,-m = -sqrt2 Im(w_lm) (m > 0).  red[0] accumulates ||u2||^2.
+__global__ void k_to_real(const double* __restrict__ w, double* u1, double* u2, int N, int L, double* red) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double n2 = 0.0;
+  if (r < N) {
+    const int C = (L + 1) * (L + 1);
+    const double s2 = 1.4142135623730951;
+    for (int l = 0; l <= L; ++l) {
+      const int c0 = l * l + l;
+      const double re0 = w[2 * ((size_t)r * C + c0)], im0 = w[2 * ((size_t)r * C + c0) + 1];
+      u1[(size_t)r * C + c0] = re0;
+      if (u2) u2[(size_t)r * C + c0] = im0;
+      n2 += im0 * im0;
+      for (int m = 1; m <= l; ++m) {
+        const double sg = (m & 1) ? -1.0 : 1.0;
+        const size_t ip = (size_t)r * C + c0 + m, in = (size_t)r * C + c0 - m;
+        const double rp = w[2 * ip], mp = w[2 * ip + 1], rn = w[2 * in], mn = w[2 * in + 1];
+        // w1 = (w + P w)/2, P w_lm = (-1)^m conj(w_l,-m)
+        const double r1 = 0.5 * (rp + sg * rn), i1 = 0.5 * (mp - sg * mn);
+        // w2 = (w - P w)/(2i)
+        const double dr = rp - sg * rn, di = mp + sg * mn;
+        const double r2 = 0.5 * di, i2 = -0.5 * dr;
+        u1[ip] = s2 * r1;
+        u1[in] = -s2 * i1;
+        if (u2) {
+          u2[ip] = s2 * r2;
+          u2[in] = -s2 * i2;
+        }
+        n2 += r2 * r2 + i2 * i2;
+      }
+    }
+  }
+  if (red) {
+    for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+    if ((threadIdx.x & 31) == 0 && n2 != 0.0) atomicAdd(red, n2);
+  }
+}
+
+__global__ void k_to_cplx(const double* __restrict__ u1, const double* __restrict__ u2, double* w, int N, int L) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  const int C = (L + 1) * (L + 1);
+  const double is2 = 0.70710678118654752;
+  for (int l = 0; l <= L; ++l) {
+    const int c0 = l * l + l;
+    const size_t i0 = (size_t)r * C + c0;
+    // w = w1 + i w2
+    w[2 * i0] = u1[i0];
+    w[2 * i0 + 1] = u2 ? u2[i0] : 0.0;
+    for (int m = 1; m <= l; ++m) {
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      const size_t ip = i0 + m, in = i0 - m;
+      // w1_lm = (a - i b)/sqrt2, w1_l,-m = (-1)^m (a + i b)/sqrt2 with a = u_l,m, b = u_l,-m
+      const double a1 = u1[ip], b1 = u1[in];
+      double wr_p = a1 * is2, wi_p = -b1 * is2, wr_n = sg * a1 * is2, wi_n = sg * b1 * is2;
+      if (u2) {
+        const double a2 = u2[ip], b2 = u2[in];
+        // + i * w2: i(a2 - i b2)/sqrt2 = (b2 + i a2)/sqrt2 ; i * (-1)^m (a2 + i b2)/sqrt2 = (-1)^m(-b2 + i a2)/sqrt2
+        wr_p += b2 * is2;
+        wi_p += a2 * is2;
+        wr_n += -sg * b2 * is2;
+        wi_n += sg * a2 * is2;
+      }
+      w[2 * ip] = wr_p;
+      w[2 * ip + 1] = wi_p;
+      w[2 * in] = wr_n;
+      w[2 * in + 1] = wi_n;
+    }
+  }
+}
+
+// Stop-rule sums of the layer z = nZ-1 (FisherInfo_IO/src/dist.cu:1143-1152) in the real basis.
+__global__ void k_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
+                             double* red) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double lw = 0.0, ls = 0.0;
+  if (p < nx * ny) {
+    const size_t r = (size_t)(nz - 1) * nx * ny + p;
+    for (int c = 0; c < Cfull; ++c) {
+      int l = 0;
+      while ((l + 1) * (l + 1) <= c) ++l;
+      const int m = c - l * l - l;
+      const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
+      lw += wgt * W[r * Cfull + c];
+      ls += wgt * S[r * Cfull + c];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lw += __shfl_xor_sync(0xffffffffu, lw, o);
+    ls += __shfl_xor_sync(0xffffffffu, ls, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(red + 2, lw);
+    atomicAdd(red + 3, ls);
+  }
+}
+
+__global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+// launchers
+template <int LA>
+static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, int stored, cudaStream_t st) {
+  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+  constexpr int C = (LA + 1) * (LA + 1);
+  if (precision == 0) {
+    if (table)
+      k_pair_fp64<LA, true><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+    else
+      k_pair_fp64<LA, false><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  const size_t smem = (size_t)C * RTE_PAIR_THREADS * sizeof(double);
+  void (*kern)(PairArgs);
+  if (table)
+    kern = stored ? k_pair_mixed<LA, true, true> : k_pair_mixed<LA, true, false>;
+  else
+    kern = stored ? k_pair_mixed<LA, false, true> : k_pair_mixed<LA, false, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, RTE_PAIR_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st) {
+  switch (LA) {
+    case 0: return launch_pair_LA<0>(a, precision, table, stored, st);
+    case 1: return launch_pair_LA<1>(a, precision, table, stored, st);
+    case 2: return launch_pair_LA<2>(a, precision, table, stored, st);
+    case 3: return launch_pair_LA<3>(a, precision, table, stored, st);
+    case 4: return launch_pair_LA<4>(a, precision, table, stored, st);
+    case 5: return launch_pair_LA<5>(a, precision, table, stored, st);
+    case 6: return launch_pair_LA<6>(a, precision, table, stored, st);
+    case 7: return launch_pair_LA<7>(a, precision, table, stored, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st) {
+  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+  k_store_kernel<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st) {
+  const int blocks = (a.N + 127) / 128;
+  switch (LA) {
+    case 0: k_epilogue<0><<<blocks, 128, 0, st>>>(a); break;
+    case 1: k_epilogue<1><<<blocks, 128, 0, st>>>(a); break;
+    case 2: k_epilogue<2><<<blocks, 128, 0, st>>>(a); break;
+    case 3: k_epilogue<3><<<blocks, 128, 0, st>>>(a); break;
+    case 4: k_epilogue<4><<<blocks, 128, 0, st>>>(a); break;
+    case 5: k_epilogue<5><<<blocks, 128, 0, st>>>(a); break;
+    case 6: k_epilogue<6><<<blocks, 128, 0, st>>>(a); break;
+    case 7: k_epilogue<7><<<blocks, 128, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st) {
+  const int n = a.nx * a.ny;
+  k_images<<<(n + 127) / 128, 128, 0, st>>>(a, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
+                               cudaStream_t st) {
+  k_to_real<<<(N + 127) / 128, 128, 0, st>>>(cplx, u1, u2, N, L, red);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L, cudaStream_t st) {
+  k_to_cplx<<<(N + 127) / 128, 128, 0, st>>>(u1, u2, cplx, N, L);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
+                                  double* red, cudaStream_t st) {
+  const int n = nx * ny;
+  k_layer_sums<<<(n + 127) / 128, 128, 0, st>>>(W, S, N, nx, ny, nz, Cfull, red);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st) {
+  k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, n);
+  return cudaGetLastError();
+}

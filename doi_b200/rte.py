@@ -1,0 +1,243 @@
+"""Python binding of the C ABI in include/rte_b200.h (ctypes over doi_b200/lib/librte_b200.so).
+
+Mirrors the reference entry points for the Neumann-series RTE path:
+  Context.prop_abs      <- prop_abs()            FisherInfo_IO/src/kernels.cu:704-808
+  Context.neumann       <- Neumann(src,out,flag)  FisherInfo_IO/src/neumann.cu:23-120
+  Context.source_beam   <- generate_source_beam  FisherInfo_IO/src/dist.cu:66-101
+  Context.images        <- generate_trans_image / generate_ref_image (dist.cu:103-268)
+  Context.forward       <- the forward main      FisherInfo_IO/src/rte.cu:92-236
+Distributions are complex128 arrays of shape (N, C), N = nX*nY*nZ (x fastest), C = (nL+1)^2.
+Every failure raises RteError with the library's message; there is no CPU fallback: the library
+must be built (python -m doi_b200.build) and a CUDA device present.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librte_b200.so")
+
+MODEL_EXACT, MODEL_FIM, MODEL_CPU = 0, 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+KERNEL_AUTO, KERNEL_STORE, KERNEL_RECOMPUTE = 0, 1, 2
+SRC_COLUMN, SRC_FIM, SRC_CPU = 0, 1, 2
+STOP_REFERENCE, STOP_FIXED, STOP_REL_L2 = 0, 1, 2
+
+# exported symbols of include/rte_b200.h (checked by the CPU tests)
+EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "rte_set_medium_tissue",
+           "rte_set_medium_voxel", "rte_source_beam", "rte_prop_abs", "rte_neumann", "rte_images",
+           "rte_forward")
+
+
+class RteError(RuntimeError):
+    pass
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+                ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("nL", ctypes.c_int), ("prop_thresh", ctypes.c_double), ("self_sub_vox", ctypes.c_int),
+                ("g", ctypes.c_double), ("n", ctypes.c_double), ("c", ctypes.c_double),
+                ("model", ctypes.c_int), ("precision", ctypes.c_int), ("kernel_mode", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class _Source(ctypes.Structure):
+    _fields_ = [("pos_x", ctypes.c_double), ("pos_y", ctypes.c_double), ("pos_z", ctypes.c_double),
+                ("diam", ctypes.c_double), ("theta", ctypes.c_double), ("phi", ctypes.c_double),
+                ("mag", ctypes.c_double), ("modulation", ctypes.c_double), ("kind", ctypes.c_int)]
+
+
+class _Stop(ctypes.Structure):
+    _fields_ = [("rule", ctypes.c_int), ("max_terms", ctypes.c_int), ("tol", ctypes.c_double)]
+
+
+class _Report(ctypes.Structure):
+    _fields_ = [("terms", ctypes.c_int), ("last_rel", ctypes.c_double), ("ms_device", ctypes.c_double),
+                ("ms_setup", ctypes.c_double)]
+
+
+@dataclass
+class Source:
+    pos_x: float = 0.0
+    pos_y: float = 0.0
+    pos_z: float = 0.0
+    diam: float = 0.2
+    theta: float = 0.0
+    phi: float = 0.0
+    mag: float = 1.0
+    modulation: float = 0.0
+    kind: int = SRC_COLUMN
+
+    def c(self):
+        return _Source(self.pos_x, self.pos_y, self.pos_z, self.diam, self.theta, self.phi, self.mag,
+                       self.modulation, self.kind)
+
+
+@dataclass
+class Stop:
+    rule: int = STOP_FIXED
+    max_terms: int = 20
+    tol: float = 1e-7
+
+    def c(self):
+        return _Stop(self.rule, self.max_terms, self.tol)
+
+
+_LIB = None
+
+
+def load_library():
+    """Load librte_b200.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RteError(f"{LIB_PATH} is missing: build it with `python -m doi_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    dp = ctypes.c_void_p
+    L.rte_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)]
+    L.rte_destroy.argtypes = [P]
+    L.rte_destroy.restype = None
+    L.rte_last_error.argtypes = [P]
+    L.rte_last_error.restype = ctypes.c_char_p
+    L.rte_device_bytes.argtypes = [P]
+    L.rte_device_bytes.restype = ctypes.c_size_t
+    L.rte_set_medium_tissue.argtypes = [P, dp, ctypes.c_int, dp, dp]
+    L.rte_set_medium_voxel.argtypes = [P, dp, dp]
+    L.rte_source_beam.argtypes = [P, ctypes.POINTER(_Source), dp]
+    L.rte_prop_abs.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int]
+    L.rte_neumann.argtypes = [P, dp, dp, ctypes.c_int, ctypes.POINTER(_Stop), ctypes.POINTER(ctypes.c_int)]
+    L.rte_images.argtypes = [P, dp, ctypes.POINTER(_Source), dp, dp]
+    L.rte_forward.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
+                              ctypes.POINTER(_Report)]
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Context:
+    """One solver context on one GPU (rte_create / rte_destroy)."""
+
+    def __init__(self, nx, ny, nz, dx=0.1, dy=None, dz=None, nL=3, g=0.8, n=1.0, c=1.0, prop_thresh=None,
+                 model=MODEL_EXACT, precision=PREC_FP64, kernel_mode=KERNEL_AUTO, self_sub_vox=1, device=0,
+                 x_min=None, x_max=None, y_min=None, y_max=None, z_min=0.0, z_max=None):
+        dy = dx if dy is None else dy
+        dz = dx if dz is None else dz
+        x_min = -nx * dx / 2 if x_min is None else x_min
+        x_max = x_min + nx * dx if x_max is None else x_max
+        y_min = -ny * dy / 2 if y_min is None else y_min
+        y_max = y_min + ny * dy if y_max is None else y_max
+        z_max = z_min + nz * dz if z_max is None else z_max
+        if prop_thresh is None:  # couple every pair
+            prop_thresh = 2.0 * np.sqrt((nx * dx) ** 2 + (ny * dy) ** 2 + (nz * dz) ** 2)
+        self.lib = load_library()
+        self.nx, self.ny, self.nz, self.nL = nx, ny, nz, nL
+        self.N = nx * ny * nz
+        self.C = (nL + 1) ** 2
+        cfg = _Config(nx, ny, nz, x_min, x_max, y_min, y_max, z_min, z_max, nL, prop_thresh, self_sub_vox,
+                      g, n, c, model, precision, kernel_mode, device)
+        h = ctypes.c_void_p()
+        rc = self.lib.rte_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise RteError(f"rte_create failed ({rc}): {self.lib.rte_last_error(None).decode()}")
+        self.h = h
+        self.cfg = cfg
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rte_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RteError(f"{what} failed ({rc}): {self.lib.rte_last_error(self.h).decode()}")
+
+    def device_bytes(self):
+        return int(self.lib.rte_device_bytes(self.h))
+
+    def set_medium_voxel(self, mua, mus):
+        mua = np.ascontiguousarray(mua, np.float64).ravel()
+        mus = np.ascontiguousarray(mus, np.float64).ravel()
+        if mua.size != self.N or mus.size != self.N:
+            raise RteError("medium arrays must have nX*nY*nZ entries")
+        self._check(self.lib.rte_set_medium_voxel(self.h, _ptr(mua), _ptr(mus)), "rte_set_medium_voxel")
+
+    def set_medium_tissue(self, tiss, mua_tab, mus_tab):
+        tiss = np.ascontiguousarray(tiss, np.uint8).ravel()
+        a = np.ascontiguousarray(mua_tab, np.float64)
+        s = np.ascontiguousarray(mus_tab, np.float64)
+        self._check(self.lib.rte_set_medium_tissue(self.h, _ptr(tiss), len(a), _ptr(a), _ptr(s)),
+                    "rte_set_medium_tissue")
+
+    def _dist(self, W):
+        W = np.ascontiguousarray(W, np.complex128).reshape(self.N, self.C)
+        return W
+
+    def source_beam(self, src):
+        out = np.zeros((self.N, self.C), np.complex128)
+        s = src.c()
+        self._check(self.lib.rte_source_beam(self.h, ctypes.byref(s), _ptr(out)), "rte_source_beam")
+        return out
+
+    def prop_abs(self, W, flag=1, flag_scat=1):
+        W = self._dist(W)
+        out = np.zeros_like(W)
+        self._check(self.lib.rte_prop_abs(self.h, _ptr(W), _ptr(out), flag, flag_scat), "rte_prop_abs")
+        return out
+
+    def neumann(self, src, out, flag=1, stop=None):
+        stop = stop or Stop()
+        src = self._dist(src)
+        o = np.array(self._dist(out), copy=True)
+        nt = ctypes.c_int(0)
+        st = stop.c()
+        self._check(self.lib.rte_neumann(self.h, _ptr(src), _ptr(o), flag, ctypes.byref(st), ctypes.byref(nt)),
+                    "rte_neumann")
+        return o, nt.value
+
+    def images(self, out, src=None):
+        out = self._dist(out)
+        tr = np.zeros(self.nx * self.ny, np.complex128)
+        rf = np.zeros(self.nx * self.ny, np.complex128)
+        s = src.c() if src is not None else None
+        self._check(self.lib.rte_images(self.h, _ptr(out), ctypes.byref(s) if s is not None else None,
+                                        _ptr(tr), _ptr(rf)), "rte_images")
+        return tr.reshape(self.ny, self.nx), rf.reshape(self.ny, self.nx)
+
+    def forward(self, src, stop=None, want_W=True, want_images=True):
+        stop = stop or Stop()
+        W = np.zeros((self.N, self.C), np.complex128) if want_W else None
+        tr = np.zeros(self.nx * self.ny, np.complex128) if want_images else None
+        rf = np.zeros(self.nx * self.ny, np.complex128) if want_images else None
+        rep = _Report()
+        s, st = src.c(), stop.c()
+        self._check(self.lib.rte_forward(self.h, ctypes.byref(s), ctypes.byref(st), _ptr(W), _ptr(tr), _ptr(rf),
+                                         ctypes.byref(rep)), "rte_forward")
+        res = dict(terms=rep.terms, last_rel=rep.last_rel, ms_device=rep.ms_device, ms_setup=rep.ms_setup)
+        if want_W:
+            res["W"] = W
+        if want_images:
+            res["trans"] = tr.reshape(self.ny, self.nx)
+            res["ref"] = rf.reshape(self.ny, self.nx)
+        return res

@@ -1,0 +1,146 @@
+/* rte_b200.h -- C ABI of the B200 Neumann-series radiative transport solver.
+ *
+ * Drop-in boundary for the forward, inverse-gradient and Fisher-information paths of
+ * the reference research code (ajha4/DOI, FisherInfo_IO and GPU package).  Plain C
+ * types only: caller-owned host buffers, opaque context, int status codes.  Nothing
+ * here ever calls exit().
+ *
+ * Distributions crossing this boundary use the reference layout: complex double
+ * (re, im) pairs, W[r*C + cnt] with voxel r = (z*nY + y)*nX + x and coefficient
+ * cnt = l*l + l + m (l = 0..nL, m = -l..l), C = (nL+1)^2, in the reference's complex
+ * orthonormal spherical-harmonic basis (FisherInfo_IO/src/sph_harm.cu:19-102).
+ * Images are nX*nY complex values, x fastest (FisherInfo_IO/src/dist.cu:316-345 writes
+ * the same order).
+ */
+#ifndef RTE_B200_H
+#define RTE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define RTE_OK 0
+#define RTE_ERR_ARG 1         /* bad argument or configuration */
+#define RTE_ERR_STATE 2       /* call out of order (e.g. no medium set) */
+#define RTE_ERR_DEVICE 3      /* CUDA error */
+#define RTE_ERR_NOMEM 4       /* device allocation failed / admission refused */
+#define RTE_ERR_IO 5          /* file could not be read or written */
+#define RTE_ERR_UNSUPPORTED 6 /* feature outside this build's limits */
+#define RTE_ERR_TIMEOUT 7     /* a bounded device wait ran out */
+
+/* ---- discretisation models (which reference the numbers follow) ------------------- */
+#define RTE_MODEL_EXACT 0 /* exact Y_lm, exact path integral, 200x200 self term, exact exitance */
+#define RTE_MODEL_FIM 1   /* FisherInfo_IO kernels as shipped: 100x100 SH table, g truncated ... */
+#define RTE_MODEL_CPU 2   /* CPU package (uniform medium) discretisation */
+
+#define RTE_PREC_FP64 0  /* plain FP64 method: every pair recomputed in FP64 each term */
+#define RTE_PREC_MIXED 1 /* FP32 path integrals + SH projection, FP64 sums and norms */
+
+#define RTE_KERNEL_AUTO 0      /* store the voxel-pair kernel when it fits, else recompute */
+#define RTE_KERNEL_STORE 1     /* store exp(-tau)/r^2 per voxel pair in HBM (FP32) */
+#define RTE_KERNEL_RECOMPUTE 2 /* recompute path integrals every term */
+
+#define RTE_SRC_COLUMN 0 /* collimated pencil on the z=0 face, column containing (pos_x,pos_y) */
+#define RTE_SRC_FIM 1    /* FisherInfo_IO rule: column x == nX/2.0 && y == nY/2.0 (even grids only) */
+#define RTE_SRC_CPU 2    /* CPU package rule: columns within diam/2, normalised by column count */
+
+#define RTE_STOP_REFERENCE 0 /* reference lambda > 0.9999 rule (dist.cu:1132-1172) */
+#define RTE_STOP_FIXED 1     /* exactly max_terms terms */
+#define RTE_STOP_REL_L2 2    /* ||W_k|| < tol * ||sum|| or max_terms */
+
+typedef struct {
+  double re, im;
+} rte_cplx;
+
+/* Mirror of the reference Geometry / Phantom-optics / Algorithm .par keys
+ * (FisherInfo_IO/src/inits.cu:198-269, :22-153; rte.cu:123-128). */
+typedef struct {
+  int nx, ny, nz;                 /* [Geometry] nX nY nZ */
+  double x_min, x_max;            /* [Geometry] xMin xMax (delX = (xMax-xMin)/nX) */
+  double y_min, y_max;
+  double z_min, z_max;
+  int nL;                         /* [Algorithm] nL (0..7) */
+  double prop_thresh;             /* [Geometry] propThresh: pairs with |r-r'| < propThresh couple */
+  int self_sub_vox;               /* [Geometry] selfsubVox */
+  double g;                       /* [Phantom] g */
+  double n;                       /* [Phantom] n */
+  double c;                       /* speed of light; the FIM model uses 1 (rte.h:15) */
+  int model;                      /* RTE_MODEL_* */
+  int precision;                  /* RTE_PREC_* */
+  int kernel_mode;                /* RTE_KERNEL_* */
+  int device;                     /* CUDA device ordinal */
+} rte_config;
+
+/* [Source] section (FisherInfo_IO/src/inits.cu:167-185). */
+typedef struct {
+  double pos_x, pos_y, pos_z;
+  double diam;
+  double theta, phi; /* read by the reference, unused */
+  double mag;
+  double modulation; /* must be 0: the steady-state path only */
+  int kind;          /* RTE_SRC_* */
+} rte_source;
+
+typedef struct {
+  int rule;      /* RTE_STOP_* */
+  int max_terms; /* RTE_STOP_FIXED / RTE_STOP_REL_L2 cap (the reference rule is capped at 10000) */
+  double tol;    /* RTE_STOP_REL_L2 tolerance */
+} rte_stop;
+
+typedef struct {
+  int terms;             /* Neumann terms taken (scatter-propagate applications) */
+  double last_rel;       /* ||W_last|| / ||sum|| */
+  double ms_device;      /* device time of the solve, CUDA events */
+  double ms_setup;       /* pair-kernel precompute time (0 when not stored) */
+} rte_report;
+
+typedef struct rte_ctx rte_ctx;
+
+/* ---- context -------------------------------------------------------------------- */
+int rte_create(const rte_config* cfg, rte_ctx** out);
+void rte_destroy(rte_ctx* ctx);
+const char* rte_last_error(const rte_ctx* ctx); /* message of the last failed call */
+size_t rte_device_bytes(const rte_ctx* ctx);    /* HBM held by this context */
+
+/* ---- medium ----------------------------------------------------------------------
+ * Tissue map form of LoadPhantom (FisherInfo_IO/src/inits.cu:22-153): tiss is nX*nY*nZ
+ * uint8, z-major, x fastest; types index mua[]/mus[] of length ntypes (type 0 = air,
+ * mua[0] = mus[0] = 0 in the reference). */
+int rte_set_medium_tissue(rte_ctx* ctx, const uint8_t* tiss, int ntypes, const double* mua,
+                          const double* mus);
+/* Per-voxel form (new): mua, mus of length nX*nY*nZ in cm^-1. */
+int rte_set_medium_voxel(rte_ctx* ctx, const double* mua, const double* mus);
+
+/* ---- reference entry points ----------------------------------------------------- */
+/* generate_source_beam (FisherInfo_IO/src/dist.cu:66-101): xi = D A (collimated beam). */
+int rte_source_beam(rte_ctx* ctx, const rte_source* src, rte_cplx* xi);
+
+/* One prop_abs pass (FisherInfo_IO/src/kernels.cu:704-808): out = [D] A in.  flag = 1 uses
+ * all orders, flag = 0 only l = 0; flag_scat = 1 applies the scatter D. */
+int rte_prop_abs(rte_ctx* ctx, const rte_cplx* in, rte_cplx* out, int flag, int flag_scat);
+
+/* Neumann (FisherInfo_IO/src/neumann.cu:23-120).  flag = 1: W_0 = src, sum_0 = out (the
+ * caller passes out = src as rte.cu:148-149 does), W_{k+1} = D A W_k, sum += W_{k+1} until
+ * the stop rule, then out = A sum.  flag = 0: out = A out.  src is not modified (the
+ * reference used it as scratch).  nterms may be NULL. */
+int rte_neumann(rte_ctx* ctx, const rte_cplx* src, rte_cplx* out, int flag, const rte_stop* stop,
+                int* nterms);
+
+/* generate_trans_image / generate_ref_image (FisherInfo_IO/src/dist.cu:103-161, 229-268)
+ * of a final distribution; trans/ref are nX*nY complex (either may be NULL). */
+int rte_images(rte_ctx* ctx, const rte_cplx* out, const rte_source* src, rte_cplx* trans,
+               rte_cplx* ref);
+
+/* Whole forward solve (rte.cu:139-210): source, Neumann, images.  W_out (N*C complex),
+ * trans, ref and report may each be NULL. */
+int rte_forward(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, rte_cplx* W_out,
+                rte_cplx* trans, rte_cplx* ref, rte_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTE_B200_H */

@@ -1,0 +1,4 @@
+/* Host-only stand-in for <cuda.h> used to compile the reference's FisherInfo_IO sources
+ * as plain C++ on a machine without a GPU (test infrastructure; see oracle/Makefile). */
+#pragma once
+#include "cuda_runtime.h"

@@ -1,0 +1,136 @@
+"""GPU parity: the CUDA library (through its C ABI) against the FP64 oracle on the same inputs.
+
+Tolerances: FP64 method 1e-11 relative L2 (rounding only); mixed precision 1e-5 relative L2 (the
+north-star bound); FIM compat model 1e-6: the oracle's FIM mode walks paths with the reference's float
+alpha (kernels.cu:56-60), the library with exact integer crossings, so tau differs by ~1e-7 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import real_to_complex, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _medium(rng, N, hetero=True):
+    if not hetero:
+        return np.full(N, 0.01), np.full(N, 1.0)
+    mua = rng.uniform(0.005, 0.1, N)
+    mus = rng.uniform(0.5, 2.0, N)
+    return mua, mus
+
+
+def _ctx(rte, O, nx, ny, nz, L, model, prec, g=0.8, kernel_mode=0, n=1.0, prop=None):
+    dx = 0.1
+    ctx = rte.Context(nx, ny, nz, dx=dx, nL=L, g=g, n=n, model=model, precision=prec, kernel_mode=kernel_mode,
+                      prop_thresh=prop)
+    cm = 1.0 / n if model != rte.MODEL_FIM else float(np.float32(1.0 / n))
+    p = O.params(nx, ny, nz, dx, dx, dx, L, g, cm, ctx.cfg.prop_thresh, mode=model, ssv=1,
+                 x_min=ctx.cfg.x_min, y_min=ctx.cfg.y_min, z_min=ctx.cfg.z_min)
+    return ctx, p
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-11), (1, 1e-5)])
+@pytest.mark.parametrize("kernel_mode", [1, 2])
+def test_prop_abs_exact_hetero(rte, oracle, prec, tol, kernel_mode):
+    if prec == 0 and kernel_mode == 1:
+        pytest.skip("the FP64 method always recomputes")
+    rng = np.random.default_rng(1)
+    nx, ny, nz, L = 7, 6, 5, 3
+    N, C = nx * ny * nz, (L + 1) ** 2
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_EXACT, prec, kernel_mode=kernel_mode)
+    mua, mus = _medium(rng, N)
+    ctx.set_medium_voxel(mua, mus)
+    W = real_to_complex(rng.standard_normal((N, C)), L)
+    for flag_scat in (1, 0):
+        got = ctx.prop_abs(W, 1, flag_scat)
+        ref = oracle.apply(p, mua, mus, W, 1, flag_scat)
+        assert rel(got, ref) < tol, (flag_scat, rel(got, ref))
+    ctx.close()
+
+
+def test_prop_abs_general_complex_input(rte, oracle):
+    """Input that is not the coefficient set of a real function takes two real solves."""
+    rng = np.random.default_rng(2)
+    nx, ny, nz, L = 5, 5, 4, 2
+    N, C = nx * ny * nz, (L + 1) ** 2
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_EXACT, 0)
+    mua, mus = _medium(rng, N)
+    ctx.set_medium_voxel(mua, mus)
+    W = rng.standard_normal((N, C)) + 1j * rng.standard_normal((N, C))
+    got = ctx.prop_abs(W, 1, 1)
+    ref = oracle.apply(p, mua, mus, W, 1, 1)
+    assert rel(got, ref) < 1e-11
+    ctx.close()
+
+
+def test_prop_abs_fim_model(rte, oracle):
+    """FisherInfo_IO discretisation: SH table with the un-wrapped phi index, tissue-0 self term 0,
+    g truncated to int in the scatter."""
+    rng = np.random.default_rng(3)
+    nx, ny, nz, L = 10, 10, 10, 2
+    N, C = nx * ny * nz, (L + 1) ** 2
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_FIM, 0, g=0.8)
+    tiss = rng.integers(0, 3, N).astype(np.uint8)
+    mua_t = np.array([0.0, 0.01, 0.05])
+    mus_t = np.array([0.0, 1.0, 1.5])
+    ctx.set_medium_tissue(tiss, mua_t, mus_t)
+    W = real_to_complex(rng.standard_normal((N, C)), L)
+    for flag, fs in ((1, 1), (1, 0), (0, 1)):
+        got = ctx.prop_abs(W, flag, fs)
+        ref = oracle.apply(p, mua_t[tiss], mus_t[tiss], W, flag, fs)
+        assert rel(got, ref) < 1e-6, (flag, fs, rel(got, ref))
+    ctx.close()
+
+
+def test_prop_abs_cpu_model(rte, oracle):
+    rng = np.random.default_rng(4)
+    nx, ny, nz, L = 6, 7, 8, 3
+    N, C = nx * ny * nz, (L + 1) ** 2
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_CPU, 0, g=0.8)
+    mua, mus = _medium(rng, N, hetero=False)
+    ctx.set_medium_voxel(mua, mus)
+    W = real_to_complex(rng.standard_normal((N, C)), L)
+    got = ctx.prop_abs(W, 1, 1)
+    ref = oracle.apply(p, mua, mus, W, 1, 1)
+    assert rel(got, ref) < 1e-11
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-11), (1, 1e-5)])
+def test_forward_exact_spheres(rte, oracle, prec, tol):
+    """Whole forward solve (source, 20 terms, final A, images) on a sphere phantom."""
+    n, L = 11, 3
+    mua, mus, _ = rte.sphere_phantom(n, nspheres=2, seed=5, rmin=0.15, rmax=0.3)
+    ctx, p = _ctx(rte, oracle, n, n, n, L, rte.MODEL_EXACT, prec)
+    ctx.set_medium_voxel(mua, mus)
+    src = rte.Source(pos_x=0.0, pos_y=0.0, mag=1.0, kind=rte.SRC_COLUMN)
+    res = ctx.forward(src, rte.Stop(rte.STOP_FIXED, 20))
+    ref = oracle.forward(p, mua, mus, src_kind=oracle.SRC_COLUMN, img_mode=0, stop_rule=oracle.STOP_FIXED,
+                         max_terms=20)
+    assert res["terms"] == 20
+    assert rel(res["W"], ref["out"]) < tol
+    assert rel(res["trans"], ref["trans"]) < tol
+    assert rel(res["ref"], ref["ref"]) < tol
+    ctx.close()
+
+
+def test_neumann_reference_stop_rule_fim(rte, oracle):
+    """Neumann(W, out, 1) with the reference's lambda rule: same term count, same distribution."""
+    nx, ny, nz, L = 10, 10, 20, 2
+    N = nx * ny * nz
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_FIM, 0, g=0.8, prop=10.0)
+    tiss = np.ones(N, np.uint8)
+    ctx.set_medium_tissue(tiss, [0.0, 0.01], [0.0, 1.0])
+    src = ctx.source_beam(rte.Source(kind=rte.SRC_FIM))
+    mua, mus = np.full(N, 0.01), np.full(N, 1.0)
+    ref_src = oracle.source(p, mua, mus, kind=oracle.SRC_FIM)
+    assert rel(src, ref_src) < 1e-14
+    out, nt = ctx.neumann(src, src, 1, rte.Stop(rte.STOP_REFERENCE))
+    ref_out, _, ref_nt = oracle.neumann(p, mua, mus, ref_src, ref_src, 1, oracle.STOP_REFERENCE, n0=2)
+    assert nt == ref_nt
+    assert rel(out, ref_out) < 1e-6
+    tr, rf = ctx.images(out, rte.Source(kind=rte.SRC_FIM))
+    otr, orf = oracle.images(p, mua, mus, ref_out, 1)
+    assert rel(tr, otr) < 1e-6 and rel(rf, orf) < 1e-6
+    ctx.close()
