@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Forward-solve throughput of the B200 Neumann-series RTE solver.
+
+Workload (one step = one forward solve): 33x33x33 voxels of 0.1 cm, SH order L=5 (36 coefficients),
+uniform background mu_a=0.01, mu_s=1 cm^-1, g=0.8, n=1, plus 3 seeded spherical inclusions
+(radius U[0.2,0.6] cm, mu_a x U[2,10], mu_s x U[0.5,2]); collimated pencil at the centre of the z=0
+face; 20 Neumann terms plus the final attenuation pass; exitance images of both z faces.  Every
+step solves a different seeded phantom, so the voxel-pair kernel is recomputed inside every step.
+
+`value`  : solves/s with the media already resident in HBM (rte_set_medium_device + rte_forward).
+`e2e`    : the same through the C ABI with HOST buffers: medium H2D, full distribution + images D2H.
+Multi-GPU: replicas only (one process per GPU, independent solves, max-over-ranks device time).
+--impl reference: the FP64 CPU port of the reference path (oracle/, OpenMP on all host cores) on a
+bounded sample of the same workload, extrapolated to solves/s.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd solves/s @33³ L=5 (mixed+batched vs FP64, ≤1e-5 rel); serve p50/p99 ms"
+N_SIDE, L, TERMS, DX = 33, 5, 20, 0.1
+
+
+def phantom(seed):
+    from doi_b200.phantoms import sphere_phantom
+    mua, mus, _ = sphere_phantom(N_SIDE, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=3, seed=seed)
+    return mua, mus
+
+
+def algorithmic_counts(n=N_SIDE, Lo=L):
+    """Coupled ordered pairs and the summed Siddon step count sum(|dx|+|dy|+|dz|) over them (all pairs
+    couple at propThresh > diagonal)."""
+    N = n ** 3
+    C = (Lo + 1) ** 2
+    pairs = N * (N - 1)
+    # sum over ordered pairs of |di| for one axis = n^2 * n^2 * sum_{a,b} |a-b| = n^4 * (n^3 - n)/3
+    s1 = (n ** 4) * (n ** 3 - n) / 3.0
+    steps = 3 * s1
+    # FLOP per launch of the pair-apply kernel: 7C (SH recurrence 3C + two C-length MACs 4C) + 10
+    # (direction) per coupled pair; the precompute: 2 per Siddon step + 25 (geometry, exp, scale).
+    apply_flop = pairs * (7 * C + 10)
+    store_flop = 2 * steps + 25 * pairs
+    # canonical per-solve count (flops_term = pairs(7C + 2S + 25) + N(2C^2 + 4C), (terms+1) terms)
+    term = pairs * (7 * C + 25) + 2 * steps + N * (2 * C * C + 4 * C)
+    return dict(N=N, C=C, pairs=pairs, steps=steps, apply_flop=apply_flop, store_flop=store_flop,
+                solve_flop=(TERMS + 1) * term)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-i", str(index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip() == "Active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(seconds=10.0, seed=0):
+    """The FP64 oracle (CPU port of the reference path) on a bounded sample: the operator for a set of
+    destination voxels against all sources, extrapolated to a full solve (21 applications)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
+        subprocess.run(["bash", os.path.join(ROOT, "oracle", "build.sh")], check=True,
+                       env=dict(os.environ, RTE_REFERENCE_DIR="/nonexistent"))
+    mua, mus = phantom(seed)
+    N = N_SIDE ** 3
+    p = O.params(N_SIDE, N_SIDE, N_SIDE, DX, DX, DX, L, 0.8, 1.0, 100.0, mode=O.MODE_EXACT)
+    rng = np.random.default_rng(0)
+    W = O.source(p, mua, mus, kind=O.SRC_COLUMN)
+    W = W + 1e-3 * rng.standard_normal(W.shape)  # dense input so every pair does full work
+    O.apply_subset(p, mua, mus, W, rng.choice(N, 4, replace=False))  # builds the self-term tables
+    nd = 16
+    t = time.perf_counter()
+    O.apply_subset(p, mua, mus, W, rng.choice(N, nd, replace=False))
+    dt = time.perf_counter() - t
+    nd2 = max(nd, int(nd * seconds / max(dt, 1e-3)))
+    t = time.perf_counter()
+    O.apply_subset(p, mua, mus, W, rng.choice(N, nd2, replace=False))
+    dt = time.perf_counter() - t
+    per_app = dt * N / nd2
+    solve_s = per_app * (TERMS + 1)
+    cores = os.cpu_count()
+    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"operator D*A for {nd2} random destination voxels x all {N} sources of the 33^3 L=5 "
+                      f"phantom ({dt:.1f} s), extrapolated x{N / nd2:.0f} voxels x{TERMS + 1} applications",
+            "seconds_per_solve": solve_s}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(seconds=args.ref_seconds)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(seconds=args.ref_seconds))
+    wall = time.perf_counter() - t0
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "33^3 voxels, L=5, 3-sphere phantom, 20 Neumann terms + final A, images",
+                       "parallelism": "host OpenMP"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import doi_b200 as R
+    ws, rank, local = dist_setup()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if ws > 1 else 0
+    torch.cuda.set_device(dev)
+    prec = R.PREC_MIXED if args.precision == "mixed" else R.PREC_FP64
+    kmode = R.KERNEL_STORE if prec == R.PREC_MIXED else R.KERNEL_RECOMPUTE
+    ctx = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, n=1.0, precision=prec, kernel_mode=kmode,
+                    device=dev)
+    src = R.Source(pos_x=0.0, pos_y=0.0, kind=R.SRC_COLUMN)
+    stop = R.Stop(R.STOP_FIXED, TERMS)
+    nsteps = args.steps + args.warmup
+    seeds = [1000 * rank + s for s in range(nsteps)]
+    media = [phantom(s) for s in seeds]
+    dmedia = [(torch.tensor(a, dtype=torch.float64, device=f"cuda:{dev}"),
+               torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")) for a, b in media]
+    peak32 = R.rte.measure_fma_peak(False, dev)
+    peak64 = R.rte.measure_fma_peak(True, dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
+    counts = algorithmic_counts(N_SIDE, L)
+
+    def step(k):
+        a, b = dmedia[k]
+        ctx.set_medium_device(a.data_ptr(), b.data_ptr())
+        return ctx.forward(src, stop, want_W=False, want_images=True)
+
+    for k in range(args.warmup):
+        step(k)
+    ctx.stats()  # reset counters
+    ctx.set_profiling(True)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = Clocks(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.warmup, nsteps):
+        step(k)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    st = ctx.stats()
+    ctx.set_profiling(False)
+    if ws > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+        ms = float(t.item())
+    value = ws * args.steps / (ms / 1e3)
+
+    # e2e through the C ABI with host buffers (medium H2D, distribution + images D2H)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    h2d = 2 * counts["N"] * 8
+    d2h = counts["N"] * counts["C"] * 16 + 2 * N_SIDE * N_SIDE * 16
+    torch.cuda.synchronize(dev)
+    e2.record(stream)
+    for k in range(args.warmup, nsteps):
+        ctx.set_medium_voxel(*media[k])
+        ctx.forward(src, stop, want_W=True, want_images=True)
+    e3.record(stream)
+    e3.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if ws > 1:
+        t = torch.tensor([ms_e2e], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = ws * args.steps / (ms_e2e / 1e3)
+
+    out = None
+    if rank == 0:
+        # accuracy of this precision against the plain FP64 method (itself held to the oracle by the
+        # parity tests) on the first timed phantom, and the plain method's own speed
+        ctx.set_medium_voxel(*media[args.warmup])
+        r_mixed = ctx.forward(src, stop, want_W=True)
+        ref_err, plain = None, None
+        if prec == R.PREC_MIXED and not args.skip_fp64_check:
+            c64 = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_FP64, device=dev)
+            c64.set_medium_voxel(*media[args.warmup])
+            r64 = c64.forward(src, stop, want_W=True)
+            rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+            ref_err = {"W": rel(r_mixed["W"], r64["W"]), "trans": rel(r_mixed["trans"], r64["trans"]),
+                       "ref": rel(r_mixed["ref"], r64["ref"])}
+            plain = 1e3 / r64["ms_device"]
+            c64.close()
+        avg_pair_ms = st["ms_pair"] / max(st["n_pair"], 1)
+        achieved = counts["apply_flop"] / (avg_pair_ms * 1e-3) / 1e12
+        peak = peak32 if prec == R.PREC_MIXED else peak64
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("pair_apply_bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64acc" if prec == R.PREC_MIXED else "f64", "data": "synthetic",
+            "config": {"workload": "33^3 voxels (0.1 cm), L=5, 3-sphere seeded phantom per step, collimated "
+                                   "centre source, 20 Neumann terms + final A, z-face images",
+                       "precision": args.precision, "pair_kernel": "stored FP32 (recomputed per solve)"
+                       if prec == R.PREC_MIXED else "recomputed per term",
+                       "grid": N_SIDE, "L": L, "terms": TERMS,
+                       "l2": f"inputs larger than L2: {counts['N'] ** 2 * 4 / 1e9:.1f} GB pair kernel streamed per term",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "fp32-cuda-core" if prec == R.PREC_MIXED else "fp64-cuda-core",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": "k_pair_mixed<5,stored>" if prec == R.PREC_MIXED
+                         else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
+                         "flop_per_launch": counts["apply_flop"],
+                         "peak_source": "measured by rte_measure_fma_peak (8-chain FMA probe) in this run"},
+            "cpu_baseline": None,
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": st["launches"],
+            "clocks": clocks,
+            "fp64_rel_err": ref_err,
+            "plain_fp64_solves_per_s": plain,
+            "kernel_ms_per_step": {"pair": st["ms_pair"] / args.steps, "store": st["ms_store"] / args.steps,
+                                   "epilogue": st["ms_epi"] / args.steps},
+            "solve_tflops_canonical": counts["solve_flop"] / (ms / args.steps / 1e3) / 1e12,
+            "peaks_tflops": {"fp32": peak32, "fp64": peak64},
+        }
+        if ws == 1 and not args.skip_cpu:
+            line["cpu_baseline"] = cpu_baseline(args.ref_seconds)
+        out = line
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-fp64-check", action="store_true")
+    ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
+    args = ap.parse_args()
+    global N_SIDE
+    N_SIDE = args.n
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

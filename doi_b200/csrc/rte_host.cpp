@@ -311,11 +311,49 @@ struct rte_ctx {
   double* d_cplx = nullptr;
   double* d_red = nullptr;
   double* d_img = nullptr;  // trans, ref (complex)
-  std::vector<double> h_mut, h_mus;
   bool medium_set = false;
   int nsplit = 1, chunk = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
+  // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
+  long long launches = 0;
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];
+  std::vector<cudaEvent_t> ev_pool;
+  double ms_acc[3] = {0, 0, 0};
+  long long n_acc[3] = {0, 0, 0};
+};
+
+static cudaEvent_t pool_event(rte_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// brackets one launch of class k with events when profiling
+struct ProfScope {
+  rte_ctx* c;
+  int k;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(rte_ctx* c_, int k_) : c(c_), k(k_) {
+    c->launches++;
+    if (c->profiling) {
+      a = pool_event(c);
+      b = pool_event(c);
+      cudaEventRecord(a, c->st);
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEventRecord(b, c->st);
+      c->ev[k].push_back({a, b});
+    }
+  }
 };
 
 static thread_local std::string g_create_err;
@@ -349,6 +387,12 @@ static cudaError_t dalloc(rte_ctx* c, T** p, size_t n) {
 }
 
 static void free_all(rte_ctx* c) {
+  for (int k = 0; k < 3; k++)
+    for (auto& p : c->ev[k]) {
+      cudaEventDestroy(p.first);
+      cudaEventDestroy(p.second);
+    }
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   void* ps[] = {c->d_perm, c->d_mut, c->d_mus, c->d_mutf, c->d_W, c->d_Wn, c->d_sum, c->d_part, c->d_mom,
                 c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img};
   for (void* p : ps)
@@ -460,7 +504,7 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_cplx, 2 * NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_red, 8), "alloc");
-  if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 4 * (size_t)c->nx * c->ny), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 5 * (size_t)c->nx * c->ny), "alloc");  // trans, ref (complex), ballistic
   if (rc == RTE_OK) {
     std::vector<int> p = morton_perm(c->nx, c->ny, c->nz);
     cu(cudaMemcpy(c->d_perm, p.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice), "perm upload");
@@ -489,13 +533,11 @@ size_t rte_device_bytes(const rte_ctx* c) { return c ? c->bytes : 0; }
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------
-static int ensure_moments(rte_ctx* c) {
+static int ensure_moments(rte_ctx* c, double mumax) {
   const int quad = c->model == RTE_MODEL_FIM ? 0 : 1;
   const int ssv = c->cfg.self_sub_vox;
   if (c->quad.L != c->L || c->quad.quad != quad || c->quad.ssv != ssv)
     build_quad(c->quad, c->L, quad, ssv, c->dx, c->dy, c->dz, c->sh);
-  double mumax = 0.0;
-  for (double m : c->h_mut) mumax = std::max(mumax, m);
   const double x = mumax * c->quad.beta_max;
   // terms until x^(k+1)/(k+1)! is below 1e-18 of the leading term
   int K = 1;
@@ -521,29 +563,32 @@ static int ensure_moments(rte_ctx* c) {
   return RTE_OK;
 }
 
-static int upload_medium(rte_ctx* c) {
-  std::vector<float> f(c->N);
-  for (int r = 0; r < c->N; r++) f[r] = (float)c->h_mut[r];
-  CUDA_TRY(c, cudaMemcpyAsync(c->d_mut, c->h_mut.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
-  CUDA_TRY(c, cudaMemcpyAsync(c->d_mus, c->h_mus.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
-  CUDA_TRY(c, cudaMemcpyAsync(c->d_mutf, f.data(), sizeof(float) * c->N, cudaMemcpyHostToDevice, c->st));
+// mu_t, mu_s (and the FP32 mu_t) from device arrays; the pair kernel becomes stale.
+static int medium_from_device(rte_ctx* c, const double* d_mua, const double* d_mus) {
+  CUDA_TRY(c, cudaMemsetAsync(c->d_red + 6, 0, sizeof(double), c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_medium(d_mua, d_mus, c->d_mut, c->d_mus, c->d_mutf, c->N, c->d_red + 6, c->st)));
+  double mumax = 0.0;
+  CUDA_TRY(c, cudaMemcpyAsync(&mumax, c->d_red + 6, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->K_valid = false;
   c->medium_set = true;
-  return ensure_moments(c);
+  return ensure_moments(c, mumax);
 }
 
 extern "C" int rte_set_medium_voxel(rte_ctx* c, const double* mua, const double* mus) {
   if (!c || !mua || !mus) return fail(c, RTE_ERR_ARG, "null argument");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
-  c->h_mut.resize(c->N);
-  c->h_mus.resize(c->N);
-  for (int r = 0; r < c->N; r++) {
+  for (int r = 0; r < c->N; r++)
     if (!(mua[r] >= 0.0) || !(mus[r] >= 0.0)) return fail(c, RTE_ERR_ARG, "negative or NaN coefficient at voxel %d", r);
-    c->h_mut[r] = mua[r] + mus[r];
-    c->h_mus[r] = mus[r];
-  }
-  return upload_medium(c);
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_aux1, mua, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_aux2, mus, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  return medium_from_device(c, c->d_aux1, c->d_aux2);
+}
+
+extern "C" int rte_set_medium_device(rte_ctx* c, const double* d_mua, const double* d_mus) {
+  if (!c || !d_mua || !d_mus) return fail(c, RTE_ERR_ARG, "null argument");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  return medium_from_device(c, d_mua, d_mus);
 }
 
 extern "C" int rte_set_medium_tissue(rte_ctx* c, const uint8_t* tiss, int ntypes, const double* mua,
@@ -610,7 +655,10 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     a.chunk = (c->N + S - 1) / S;
     a.nsplit = (c->N + a.chunk - 1) / a.chunk;
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
-    CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+    {
+      ProfScope ps(c, 1);
+      CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+    }
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->st));
     CUDA_TRY(c, cudaEventSynchronize(c->ev1));
     float ms = 0;
@@ -651,7 +699,10 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   a.part = c->d_part;
   a.chunk = c->chunk;
   a.nsplit = c->nsplit;
-  CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
+  {
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
+  }
   EpiArgs e;
   memset(&e, 0, sizeof e);
   e.N = c->N;
@@ -675,7 +726,10 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   e.sum = sum;
   e.red = c->d_red;
   CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
-  CUDA_TRY(c, rte_launch_epilogue(e, LA, c->st));
+  {
+    ProfScope ps(c, 2);
+    CUDA_TRY(c, rte_launch_epilogue(e, LA, c->st));
+  }
   return RTE_OK;
 }
 
@@ -691,7 +745,7 @@ static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* 
   double rel = 0.0;
   if (flag) {
     CUDA_TRY(c, cudaMemcpyAsync(c->d_W, W0, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_W, c->d_Wf, NC, c->st));
+    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_W, c->d_Wf, NC, c->st)));
     const int flag_l = c->cfg.g != 0.0 ? 1 : 0;  // neumann.cu:74-79
     const int rule = force_terms >= 0 ? RTE_STOP_FIXED : stop->rule;
     const int maxt = force_terms >= 0 ? force_terms : (rule == RTE_STOP_REFERENCE ? 10000 : stop->max_terms);
@@ -700,7 +754,7 @@ static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* 
     double hred[4] = {0, 0, 0, 0};
     if (rule == RTE_STOP_REFERENCE) {
       CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
-      CUDA_TRY(c, rte_launch_layer_sums(c->d_W, c->d_sum, c->N, c->nx, c->ny, c->nz, c->C, c->d_red, c->st));
+      CUDA_TRY(c, (c->launches++, rte_launch_layer_sums(c->d_W, c->d_sum, c->N, c->nx, c->ny, c->nz, c->C, c->d_red, c->st)));
       CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
       CUDA_TRY(c, cudaStreamSynchronize(c->st));
     }
@@ -739,7 +793,7 @@ static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* 
   // final A on the running sum (no scatter), neumann.cu:95-118
   float* in32 = nullptr;
   if (mixed) {
-    CUDA_TRY(c, rte_launch_f64_to_f32(c->d_sum, c->d_Wf, NC, c->st));
+    CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_sum, c->d_Wf, NC, c->st)));
     in32 = c->d_Wf;
   }
   int rc = apply_term(c, c->d_sum, in32, res, nullptr, nullptr, 1, 0);
@@ -755,7 +809,7 @@ static int upload_cplx(rte_ctx* c, const rte_cplx* h, double* u1, double* u2, bo
   const size_t NC = (size_t)c->N * c->C;
   CUDA_TRY(c, cudaMemcpyAsync(c->d_cplx, h, NC * sizeof(rte_cplx), cudaMemcpyHostToDevice, c->st));
   CUDA_TRY(c, cudaMemsetAsync(c->d_red + 4, 0, sizeof(double), c->st));
-  CUDA_TRY(c, rte_launch_to_real(c->d_cplx, u1, u2, c->N, c->L, c->d_red + 4, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_to_real(c->d_cplx, u1, u2, c->N, c->L, c->d_red + 4, c->st)));
   double n2 = 0;
   CUDA_TRY(c, cudaMemcpyAsync(&n2, c->d_red + 4, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
@@ -765,7 +819,7 @@ static int upload_cplx(rte_ctx* c, const rte_cplx* h, double* u1, double* u2, bo
 
 static int download_cplx(rte_ctx* c, const double* u1, const double* u2, rte_cplx* h) {
   const size_t NC = (size_t)c->N * c->C;
-  CUDA_TRY(c, rte_launch_to_cplx(u1, u2, c->d_cplx, c->N, c->L, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_to_cplx(u1, u2, c->d_cplx, c->N, c->L, c->st)));
   CUDA_TRY(c, cudaMemcpyAsync(h, c->d_cplx, NC * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   return RTE_OK;
@@ -781,11 +835,11 @@ extern "C" int rte_prop_abs(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int f
   const size_t NC = (size_t)c->N * c->C;
   const bool mixed = c->precision == RTE_PREC_MIXED;
   // part 1 -> d_W, part 2 -> d_sum (both scratch here)
-  if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_aux1, c->d_Wf, NC, c->st));
+  if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_aux1, c->d_Wf, NC, c->st)));
   rc = apply_term(c, c->d_aux1, c->d_Wf, c->d_W, nullptr, nullptr, flag, flag_scat);
   if (rc) return rc;
   if (has2) {
-    if (mixed) CUDA_TRY(c, rte_launch_f64_to_f32(c->d_aux2, c->d_Wf, NC, c->st));
+    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_aux2, c->d_Wf, NC, c->st)));
     rc = apply_term(c, c->d_aux2, c->d_Wf, c->d_sum, nullptr, nullptr, flag, flag_scat);
     if (rc) return rc;
   }
@@ -851,39 +905,45 @@ static int source_columns(const rte_ctx* c, const rte_source* s, std::vector<int
   return RTE_OK;
 }
 
-// xi = D A xi_beam on the pencil columns (dist.cu:66-101; Dist.c:1077-1128 for RTE_SRC_CPU).
-static int make_source(rte_ctx* c, const rte_source* s, std::vector<double>& xi) {
+// xi = D A xi_beam on the pencil columns, built on the device into d_dst (real basis), with the
+// ballistic transmission per column in d_ball (dist.cu:66-101; Dist.c:1077-1128 for RTE_SRC_CPU).
+static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst) {
   if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
   std::vector<int> cols;
   double scale;
   if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d", s->kind);
-  xi.assign((size_t)c->N * c->C, 0.0);
-  const int plane = c->nx * c->ny;
-  for (int col : cols) {
-    double att = 1.0;
-    for (int i = 0; i < c->nz; i++) {
-      const int r = i * plane + col;
-      const double mt = c->h_mut[r], ms = c->h_mus[r];
-      double v;
-      if (s->kind == RTE_SRC_CPU) {
-        const double zs = (double)i * c->dz + c->cfg.z_min + c->dz / 2.0;
-        const double tz = zs - c->dz / 2.0;
-        v = (exp(-mt * tz) - exp(-mt * (tz + c->dz)));
-      } else {
-        v = att * (1 - exp(-mt * c->dz));
-        att *= exp(-mt * c->dz);
-      }
-      for (int l = 0; l <= c->L; l++)
-        xi[(size_t)r * c->C + l * l + l] =
-            scale * pow(c->cfg.g, (double)l) * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / c->dV;
-    }
-  }
+  if ((int)cols.size() > RTE_MAX_SRC_COLS) return fail(c, RTE_ERR_UNSUPPORTED, "beam covers more than %d columns", RTE_MAX_SRC_COLS);
+  const size_t NC = (size_t)c->N * c->C;
+  double* d_ball = c->d_img + 4 * (size_t)c->nx * c->ny;
+  CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, NC * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(d_ball, 0, (size_t)c->nx * c->ny * sizeof(double), c->st));
+  if (cols.empty()) return RTE_OK;
+  SrcArgs a;
+  memset(&a, 0, sizeof a);
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  a.Cfull = c->C;
+  a.L = c->L;
+  a.kind = s->kind;
+  a.ncols = (int)cols.size();
+  for (size_t q = 0; q < cols.size(); q++) a.cols[q] = cols[q];
+  a.scale = scale;
+  a.mag = s->mag;
+  a.g = c->cfg.g;
+  a.dz = c->dz;
+  a.dV = c->dV;
+  a.z_min = c->cfg.z_min;
+  a.mut = c->d_mut;
+  a.mus = c->d_mus;
+  a.W = d_dst;
+  a.ball = d_ball;
+  CUDA_TRY(c, (c->launches++, rte_launch_source(a, c->st)));
   return RTE_OK;
 }
 
 // per-l image weights and the ballistic pixel (dist.cu:103-161, 229-268; Dist.c:134-229)
-static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a, std::vector<int>& ballpix,
-                         std::vector<double>& ballval) {
+static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a) {
   memset(a.wt, 0, sizeof a.wt);
   memset(a.wr, 0, sizeof a.wr);
   const double mag = s ? s->mag : 1.0;
@@ -924,29 +984,12 @@ static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a, std::vecto
       a.wr[l] = fac * f;
     }
   }
-  ballpix.clear();
-  ballval.clear();
-  if (!s) return RTE_OK;
-  std::vector<int> cols;
-  double scale;
-  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind");
-  const int plane = c->nx * c->ny;
-  for (int col : cols) {
-    double v;
-    if (s->kind == RTE_SRC_CPU) {
-      const double zs = (double)(c->nz - 1) * c->dz + c->cfg.z_min + c->dz / 2.0;
-      v = scale * exp(-c->h_mut[(size_t)(c->nz - 1) * plane + col] * (zs + c->dz / 2.0));
-    } else {
-      v = mag;
-      for (int i = 0; i < c->nz; i++) v *= exp(-c->h_mut[(size_t)i * plane + col] * c->dz);
-    }
-    ballpix.push_back(col);
-    ballval.push_back(v);
-  }
   return RTE_OK;
 }
 
-static int run_images(rte_ctx* c, const double* d_out1, const double* d_out2, const rte_source* s, rte_cplx* trans,
+// images of a real-basis distribution on the device; with_ball adds the ballistic term left in
+// d_ball by the last launch_source.
+static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool with_ball, rte_cplx* trans,
                       rte_cplx* ref) {
   ImgArgs a;
   memset(&a, 0, sizeof a);
@@ -955,54 +998,47 @@ static int run_images(rte_ctx* c, const double* d_out1, const double* d_out2, co
   a.nz = c->nz;
   a.Cfull = c->C;
   a.L = c->L;
-  a.out = d_out1;
-  std::vector<int> bp;
-  std::vector<double> bv;
-  int rc = image_weights(c, s, a, bp, bv);
+  a.out = d_out;
+  int rc = image_weights(c, s, a);
   if (rc) return rc;
-  a.ball_pix = -1;
   const size_t np = (size_t)c->nx * c->ny;
+  a.ball = with_ball ? c->d_img + 4 * np : nullptr;
   a.trans = c->d_img;
   a.ref = c->d_img + 2 * np;
-  CUDA_TRY(c, rte_launch_images(a, c->st));
-  (void)d_out2;
-  std::vector<rte_cplx> ht(np), hr(np);
-  CUDA_TRY(c, cudaMemcpyAsync(ht.data(), a.trans, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
-  CUDA_TRY(c, cudaMemcpyAsync(hr.data(), a.ref, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_images(a, c->st)));
+  if (trans) CUDA_TRY(c, cudaMemcpyAsync(trans, a.trans, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  if (ref) CUDA_TRY(c, cudaMemcpyAsync(ref, a.ref, np * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
-  for (size_t q = 0; q < bp.size(); q++) ht[bp[q]].re += bv[q];
-  if (trans) memcpy(trans, ht.data(), np * sizeof(rte_cplx));
-  if (ref) memcpy(ref, hr.data(), np * sizeof(rte_cplx));
   return RTE_OK;
 }
 
 extern "C" int rte_source_beam(rte_ctx* c, const rte_source* s, rte_cplx* xi) {
   if (!c || !s || !xi) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
-  std::vector<double> u;
-  int rc = make_source(c, s, u);
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  int rc = launch_source(c, s, c->d_aux1);
   if (rc) return rc;
-  const size_t NC = (size_t)c->N * c->C;
-  for (size_t q = 0; q < NC; q++) {
-    xi[q].re = u[q];  // m = 0 only: real and complex coefficients coincide
-    xi[q].im = 0.0;
-  }
-  return RTE_OK;
+  return download_cplx(c, c->d_aux1, nullptr, xi);
 }
 
 extern "C" int rte_images(rte_ctx* c, const rte_cplx* out, const rte_source* s, rte_cplx* trans, rte_cplx* ref) {
   if (!c || !out) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  int rc;
+  if (s) {  // ballistic term of this source (the source itself goes to scratch)
+    rc = launch_source(c, s, c->d_aux3);
+    if (rc) return rc;
+  }
   bool has2 = false;
-  int rc = upload_cplx(c, out, c->d_aux1, c->d_aux2, &has2);
+  rc = upload_cplx(c, out, c->d_aux1, c->d_aux2, &has2);
   if (rc) return rc;
-  rc = run_images(c, c->d_aux1, nullptr, s, trans, ref);
+  rc = run_images(c, c->d_aux1, s, s != nullptr, trans, ref);
   if (rc || !has2) return rc;
-  // imaginary-function part: images of part 2 go to the imaginary component
+  // imaginary-function part: its images go to the imaginary component
   const size_t np = (size_t)c->nx * c->ny;
   std::vector<rte_cplx> t2(np), r2(np);
-  rc = run_images(c, c->d_aux2, nullptr, nullptr, t2.data(), r2.data());
+  rc = run_images(c, c->d_aux2, s, false, t2.data(), r2.data());
   if (rc) return rc;
   for (size_t q = 0; q < np; q++) {
     if (trans) trans[q].im += t2[q].re;
@@ -1016,36 +1052,97 @@ extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop
   if (!c || !s || !stop) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
-  std::vector<double> xi;
-  int rc = make_source(c, s, xi);
-  if (rc) return rc;
-  const size_t NC = (size_t)c->N * c->C;
-  CUDA_TRY(c, cudaMemcpyAsync(c->d_aux1, xi.data(), NC * sizeof(double), cudaMemcpyHostToDevice, c->st));
   cudaEvent_t t0, t1;
   CUDA_TRY(c, cudaEventCreate(&t0));
   CUDA_TRY(c, cudaEventCreate(&t1));
   CUDA_TRY(c, cudaEventRecord(t0, c->st));
   int terms = 0;
   double rel = 0;
-  rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, &terms, &rel);
-  if (rc) {
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    return rc;
-  }
-  CUDA_TRY(c, cudaEventRecord(t1, c->st));
-  if (W_out) rc = download_cplx(c, c->d_aux2, nullptr, W_out);
-  if (!rc && (trans || ref)) rc = run_images(c, c->d_aux2, nullptr, s, trans, ref);
-  CUDA_TRY(c, cudaEventSynchronize(t1));
+  int rc = launch_source(c, s, c->d_aux1);
+  if (!rc) rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, &terms, &rel);
+  if (!rc && (trans || ref)) rc = run_images(c, c->d_aux2, s, true, trans, ref);
+  if (!rc) CUDA_TRY(c, cudaEventRecord(t1, c->st));
+  if (!rc && W_out) rc = download_cplx(c, c->d_aux2, nullptr, W_out);
   float ms = 0;
-  cudaEventElapsedTime(&ms, t0, t1);
+  if (!rc) {
+    CUDA_TRY(c, cudaEventSynchronize(t1));
+    cudaEventElapsedTime(&ms, t0, t1);
+  }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  if (rc) return rc;
   if (rep) {
     rep->terms = terms;
     rep->last_rel = rel;
     rep->ms_device = ms;
     rep->ms_setup = c->last_setup_ms;
   }
-  return rc;
+  return RTE_OK;
+}
+
+extern "C" int rte_measure_fma_peak(int device, int fp64, double* tflops) {
+  if (!tflops) return RTE_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return RTE_ERR_DEVICE;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  float* sink = nullptr;
+  if (cudaMalloc(&sink, 65536 * sizeof(float)) != cudaSuccess) return RTE_ERR_NOMEM;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, iters = fp64 ? 20000 : 40000;
+  double best = 0;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0, 0);
+    rte_launch_fma_peak(fp64, iters, sink, 0, blocks);
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0;
+    if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  *tflops = best;
+  return e == cudaSuccess ? RTE_OK : RTE_ERR_DEVICE;
+}
+
+extern "C" void* rte_get_stream(rte_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+extern "C" int rte_set_profiling(rte_ctx* c, int on) {
+  if (!c) return RTE_ERR_ARG;
+  c->profiling = on != 0;
+  return RTE_OK;
+}
+
+extern "C" int rte_get_stats(rte_ctx* c, rte_stats* out) {
+  if (!c || !out) return fail(c, RTE_ERR_ARG, "null argument");
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  for (int k = 0; k < 3; k++) {
+    for (auto& p : c->ev[k]) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, p.first, p.second);
+      c->ms_acc[k] += ms;
+      c->n_acc[k]++;
+      c->ev_pool.push_back(p.first);
+      c->ev_pool.push_back(p.second);
+    }
+    c->ev[k].clear();
+  }
+  out->launches = c->launches;
+  out->ms_pair = c->ms_acc[0];
+  out->n_pair = c->n_acc[0];
+  out->ms_store = c->ms_acc[1];
+  out->n_store = c->n_acc[1];
+  out->ms_epi = c->ms_acc[2];
+  out->n_epi = c->n_acc[2];
+  c->launches = 0;
+  for (int k = 0; k < 3; k++) {
+    c->ms_acc[k] = 0;
+    c->n_acc[k] = 0;
+  }
+  return RTE_OK;
 }

@@ -48,8 +48,7 @@ struct ImgArgs {
   const double* out;
   double wt[RTE_MAX_L + 1];  // transmission weights per l (m = 0 coefficient)
   double wr[RTE_MAX_L + 1];  // reflection weights per l
-  int ball_pix;              // pixel index of the ballistic term (-1 = none)
-  double ball_val;
+  const double* ball;        // nx*ny ballistic transmission added to trans (may be null)
   double* trans;  // nx*ny complex (re, im)
   double* ref;
 };
@@ -60,7 +59,23 @@ struct ShTables {
   double Q0[RTE_MAX_L + 1];  // q_m^m
 };
 
+#define RTE_MAX_SRC_COLS 512
+
+struct SrcArgs {
+  int nx, ny, nz, Cfull, L, kind, ncols;
+  int cols[RTE_MAX_SRC_COLS];
+  double scale, mag, g, dz, dV, z_min;
+  const double* mut;
+  const double* mus;
+  double* W;     // N x Cfull, zeroed by the caller
+  double* ball;  // nx*ny ballistic transmission, zeroed by the caller
+};
+
 extern "C++" {
+cudaError_t rte_launch_source(const SrcArgs& a, cudaStream_t st);
+cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut, double* mus_out, float* mutf,
+                              int N, double* red_max, cudaStream_t st);
+cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks);
 cudaError_t rte_upload_sh_tables(const ShTables& t);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);

@@ -455,7 +455,7 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
       fi += a.wr[l] * out_im[rr * a.Cfull + c];
     }
   }
-  if (p == a.ball_pix) t += a.ball_val;
+  if (a.ball) t += a.ball[p];
   if (a.trans) {
     a.trans[2 * p] = t;
     a.trans[2 * p + 1] = ti;
@@ -464,6 +464,76 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
     a.ref[2 * p] = f;
     a.ref[2 * p + 1] = fi;
   }
+}
+
+// Collimated-beam source xi = D A xi_beam on the pencil columns (one thread per column), with the
+// ballistic transmission of each column.  FisherInfo_IO/src/dist.cu:66-101 (product of per-layer
+// attenuations) and, for kind 2, CPU package/src/Dist.c:1077-1128 (attenuation from the absolute
+// depth of the voxel, normalised by the number of columns).
+__global__ void k_source(SrcArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.ncols) return;
+  const int col = a.cols[q];
+  const int plane = a.nx * a.ny;
+  double att = 1.0, mt = 0.0;
+  for (int i = 0; i < a.nz; ++i) {
+    const size_t r = (size_t)i * plane + col;
+    mt = a.mut[r];
+    const double ms = a.mus[r];
+    double v;
+    if (a.kind == 2) {
+      const double tz = (double)i * a.dz + a.z_min + a.dz / 2.0 - a.dz / 2.0;
+      v = exp(-mt * tz) - exp(-mt * (tz + a.dz));
+    } else {
+      v = att * (1 - exp(-mt * a.dz));
+    }
+    att *= exp(-mt * a.dz);
+    double gl = 1.0;
+    for (int l = 0; l <= a.L; ++l) {
+      a.W[r * a.Cfull + l * l + l] = a.scale * gl * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / a.dV;
+      gl *= a.g;
+    }
+  }
+  if (a.kind == 2) {
+    const double zs = (double)(a.nz - 1) * a.dz + a.z_min + a.dz / 2.0;
+    a.ball[col] = a.scale * exp(-mt * (zs + a.dz / 2.0));
+  } else {
+    a.ball[col] = a.mag * att;
+  }
+}
+
+// mu_t = mu_a + mu_s (FP64 and FP32 copies), mu_s copy, and max(mu_t) into red_max (>= 0 values,
+// so the bit pattern orders like the value).
+__global__ void k_medium(const double* mua, const double* mus, double* mut, double* mus_out, float* mutf, int N,
+                         double* red_max) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (r < N) {
+    m = mua[r] + mus[r];
+    mut[r] = m;
+    mutf[r] = (float)m;
+    if (mus_out != mus) mus_out[r] = mus[r];
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)red_max, (unsigned long long)__double_as_longlong(m));
+}
+
+// FMA throughput probe (roofline denominator for the CUDA-core-bound kernels): 8 independent FMA
+// chains per thread; the result is written so the work cannot be removed.
+template <typename T>
+__global__ void k_fma_peak(int iters, float* sink) {
+  T a[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) a[q] = (T)(threadIdx.x + q) * (T)1e-3;
+  const T b = (T)0.999999, c = (T)1e-7;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = fma(a[q], b, c);
+  }
+  T s = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) s += a[q];
+  if (s == (T)-1.2345) sink[blockIdx.x] = (float)s;
 }
 
 // Complex reference basis <-> real basis.  w = w1 + i w2 with w1, w2 the coefficient sets of
@@ -652,6 +722,25 @@ cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int n
                                   double* red, cudaStream_t st) {
   const int n = nx * ny;
   k_layer_sums<<<(n + 127) / 128, 128, 0, st>>>(W, S, N, nx, ny, nz, Cfull, red);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_source(const SrcArgs& a, cudaStream_t st) {
+  k_source<<<(a.ncols + 31) / 32, 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut, double* mus_out, float* mutf,
+                              int N, double* red_max, cudaStream_t st) {
+  k_medium<<<(N + 127) / 128, 128, 0, st>>>(mua, mus, mut, mus_out, mutf, N, red_max);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks) {
+  if (fp64)
+    k_fma_peak<double><<<blocks, 256, 0, st>>>(iters, sink);
+  else
+    k_fma_peak<float><<<blocks, 256, 0, st>>>(iters, sink);
   return cudaGetLastError();
 }
 

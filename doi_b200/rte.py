@@ -27,8 +27,9 @@ STOP_REFERENCE, STOP_FIXED, STOP_REL_L2 = 0, 1, 2
 
 # exported symbols of include/rte_b200.h (checked by the CPU tests)
 EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "rte_set_medium_tissue",
-           "rte_set_medium_voxel", "rte_source_beam", "rte_prop_abs", "rte_neumann", "rte_images",
-           "rte_forward")
+           "rte_set_medium_voxel", "rte_set_medium_device", "rte_source_beam", "rte_prop_abs", "rte_neumann",
+           "rte_images", "rte_forward", "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling",
+           "rte_get_stats")
 
 
 class RteError(RuntimeError):
@@ -54,6 +55,12 @@ class _Source(ctypes.Structure):
 
 class _Stop(ctypes.Structure):
     _fields_ = [("rule", ctypes.c_int), ("max_terms", ctypes.c_int), ("tol", ctypes.c_double)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_longlong), ("ms_pair", ctypes.c_double), ("n_pair", ctypes.c_longlong),
+                ("ms_store", ctypes.c_double), ("n_store", ctypes.c_longlong), ("ms_epi", ctypes.c_double),
+                ("n_epi", ctypes.c_longlong)]
 
 
 class _Report(ctypes.Structure):
@@ -110,6 +117,12 @@ def load_library():
     L.rte_device_bytes.restype = ctypes.c_size_t
     L.rte_set_medium_tissue.argtypes = [P, dp, ctypes.c_int, dp, dp]
     L.rte_set_medium_voxel.argtypes = [P, dp, dp]
+    L.rte_set_medium_device.argtypes = [P, dp, dp]
+    L.rte_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.rte_get_stream.argtypes = [P]
+    L.rte_get_stream.restype = ctypes.c_void_p
+    L.rte_set_profiling.argtypes = [P, ctypes.c_int]
+    L.rte_get_stats.argtypes = [P, ctypes.POINTER(_Stats)]
     L.rte_source_beam.argtypes = [P, ctypes.POINTER(_Source), dp]
     L.rte_prop_abs.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int]
     L.rte_neumann.argtypes = [P, dp, dp, ctypes.c_int, ctypes.POINTER(_Stop), ctypes.POINTER(ctypes.c_int)]
@@ -122,6 +135,16 @@ def load_library():
 
 def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def measure_fma_peak(fp64=False, device=0):
+    """Measured FMA throughput (TFLOP/s) of the device's CUDA cores."""
+    lib = load_library()
+    v = ctypes.c_double(0.0)
+    rc = lib.rte_measure_fma_peak(device, int(bool(fp64)), ctypes.byref(v))
+    if rc != 0:
+        raise RteError(f"rte_measure_fma_peak failed ({rc})")
+    return v.value
 
 
 class Context:
@@ -173,6 +196,19 @@ class Context:
         if rc != 0:
             raise RteError(f"{what} failed ({rc}): {self.lib.rte_last_error(self.h).decode()}")
 
+    def stream_ptr(self):
+        """cudaStream_t of this context (wrap with torch.cuda.ExternalStream to time on it)."""
+        return int(self.lib.rte_get_stream(self.h) or 0)
+
+    def set_profiling(self, on=True):
+        self._check(self.lib.rte_set_profiling(self.h, int(bool(on))), "rte_set_profiling")
+
+    def stats(self):
+        """Launch count and per-class kernel times since the last call (synchronises)."""
+        st = _Stats()
+        self._check(self.lib.rte_get_stats(self.h, ctypes.byref(st)), "rte_get_stats")
+        return {k: getattr(st, k) for k, _ in _Stats._fields_}
+
     def device_bytes(self):
         return int(self.lib.rte_device_bytes(self.h))
 
@@ -182,6 +218,11 @@ class Context:
         if mua.size != self.N or mus.size != self.N:
             raise RteError("medium arrays must have nX*nY*nZ entries")
         self._check(self.lib.rte_set_medium_voxel(self.h, _ptr(mua), _ptr(mus)), "rte_set_medium_voxel")
+
+    def set_medium_device(self, mua_ptr, mus_ptr):
+        """Medium from device pointers (e.g. torch.Tensor.data_ptr() of float64 CUDA tensors)."""
+        self._check(self.lib.rte_set_medium_device(self.h, ctypes.c_void_p(mua_ptr), ctypes.c_void_p(mus_ptr)),
+                    "rte_set_medium_device")
 
     def set_medium_tissue(self, tiss, mua_tab, mus_tab):
         tiss = np.ascontiguousarray(tiss, np.uint8).ravel()

@@ -114,6 +114,8 @@ int rte_set_medium_tissue(rte_ctx* ctx, const uint8_t* tiss, int ntypes, const d
                           const double* mus);
 /* Per-voxel form (new): mua, mus of length nX*nY*nZ in cm^-1. */
 int rte_set_medium_voxel(rte_ctx* ctx, const double* mua, const double* mus);
+/* Same with DEVICE pointers (on the context's GPU), for callers whose media are already in HBM. */
+int rte_set_medium_device(rte_ctx* ctx, const double* d_mua, const double* d_mus);
 
 /* ---- reference entry points ----------------------------------------------------- */
 /* generate_source_beam (FisherInfo_IO/src/dist.cu:66-101): xi = D A (collimated beam). */
@@ -139,6 +141,28 @@ int rte_images(rte_ctx* ctx, const rte_cplx* out, const rte_source* src, rte_cpl
  * trans, ref and report may each be NULL. */
 int rte_forward(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, rte_cplx* W_out,
                 rte_cplx* trans, rte_cplx* ref, rte_report* report);
+
+/* ---- measurement helpers (no reference counterpart) ------------------------------ */
+typedef struct {
+  long long launches;     /* kernels launched by this context since the last reset */
+  double ms_pair;         /* summed device time of the pair (A operator) kernels */
+  long long n_pair;
+  double ms_store;        /* pair-kernel precompute */
+  long long n_store;
+  double ms_epi;          /* epilogue (self term, scatter, sums) */
+  long long n_epi;
+} rte_stats;
+
+/* The CUDA stream (cudaStream_t) all of this context's work is queued on. */
+void* rte_get_stream(rte_ctx* ctx);
+/* on = 1: time every pair / precompute / epilogue launch with CUDA events on that stream. */
+int rte_set_profiling(rte_ctx* ctx, int on);
+/* Synchronises the stream, returns the counters and resets them. */
+int rte_get_stats(rte_ctx* ctx, rte_stats* out);
+
+/* FP32 (fp64 = 0) or FP64 (fp64 = 1) FMA throughput of the device in TFLOP/s, measured with an
+ * 8-chain FMA loop: the denominator of the roofline of the CUDA-core-bound kernels. */
+int rte_measure_fma_peak(int device, int fp64, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -42,6 +42,8 @@ def lib():
         P = ctypes.POINTER(OrcParams)
         S = ctypes.POINTER(OrcSource)
         L.orc_apply.argtypes = [P, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
+        L.orc_apply_subset.argtypes = [P, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.c_long]
         L.orc_source.argtypes = [P, dp, dp, S, dp]
         L.orc_neumann.argtypes = [P, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -86,6 +88,20 @@ def apply(p, mua, mus, W, flag=1, flag_scat=1):
     out = np.zeros((N, C), np.complex128)
     lib().orc_apply(ctypes.byref(p), _dp(mua), _dp(mus), _dp(W.view(np.float64)),
                     _dp(out.view(np.float64)), flag, flag_scat)
+    return out
+
+
+def apply_subset(p, mua, mus, W, dests, flag=1, flag_scat=1):
+    """The operator for the listed destination voxels only (rows of the result outside the list are 0)."""
+    N = p.nx * p.ny * p.nz
+    C = ncoef(p.L)
+    mua = np.ascontiguousarray(mua, np.float64).ravel()
+    mus = np.ascontiguousarray(mus, np.float64).ravel()
+    W = np.ascontiguousarray(W, np.complex128).reshape(N, C)
+    d = np.ascontiguousarray(dests, np.int32)
+    out = np.zeros((N, C), np.complex128)
+    lib().orc_apply_subset(ctypes.byref(p), _dp(mua), _dp(mus), _dp(W.view(np.float64)), _dp(out.view(np.float64)),
+                           flag, flag_scat, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(d))
     return out
 
 

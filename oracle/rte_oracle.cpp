@@ -337,7 +337,7 @@ static const std::vector<cd>* self_matrix(int quad, int L, int ssv, double mut, 
 // FisherInfo_IO/src/kernels.cu: compute_diagonal_abs :151-178, compute_propabs :289-366,
 // scale_dist_dev :368-383, prop_scat_dev :385-418; host sequence prop_abs :704-808.
 static void apply_op(const orc_params* p, const double* mua, const double* mus, const cd* in, cd* out, int flag,
-                     int flag_scat) {
+                     int flag_scat, const int* dests = nullptr, long ndest = -1) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   const size_t N = (size_t)nx * ny * nz;
   const int Cfull = ncoef(p->L);
@@ -358,11 +358,13 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
     }
   const double cm = p->cm;
   const double dV = p->dx * p->dy * p->dz;
+  const long nloop = dests ? ndest : (long)N;
 #ifdef _OPENMP
   int nth = p->nthreads > 0 ? p->nthreads : omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nth)
 #endif
-  for (long r = 0; r < (long)N; r++) {
+  for (long q = 0; q < nloop; q++) {
+    const long r = dests ? dests[q] : q;
     int i = (int)(r / ((size_t)nx * ny)), j = (int)((r / nx) % ny), k = (int)(r % nx);
     std::vector<cd> acc(Cfull, cd(0, 0)), Y(Cfull);
     // self voxel
@@ -473,6 +475,13 @@ double orc_path_integral(const orc_params* p, const double* mut, int si, int sj,
 void orc_self_matrix(int quad, int L, int ssv, double mut, double dx, double dy, double dz, double* out) {
   const std::vector<cd>* D = self_matrix(quad, L, ssv, mut, dx, dy, dz);
   memcpy(out, D->data(), sizeof(cd) * D->size());
+}
+
+// out = [D] A in for the listed destination voxels only (CPU-baseline samples)
+int orc_apply_subset(const orc_params* p, const double* mua, const double* mus, const double* in, double* out,
+                     int flag, int flag_scat, const int* dests, long ndest) {
+  apply_op(p, mua, mus, (const cd*)in, (cd*)out, flag, flag_scat, dests, ndest);
+  return 0;
 }
 
 // out = [D] A in  (complex interleaved, N*C*2 doubles)
