@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librte_b200.so")
-SOURCES = ["rte_kernels.cu", "rte_host.cpp"]
+SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -358,6 +358,8 @@ struct ProfScope {
 
 static thread_local std::string g_create_err;
 
+void rte_set_global_error(const char* msg) { g_create_err = msg ? msg : ""; }
+
 static int fail(rte_ctx* c, int code, const char* fmt, ...) {
   char buf[1024];
   va_list ap;

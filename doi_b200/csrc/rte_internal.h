@@ -72,6 +72,8 @@ struct SrcArgs {
 };
 
 extern "C++" {
+// message returned by rte_last_error(NULL) on this thread
+__attribute__((visibility("hidden"))) void rte_set_global_error(const char* msg);
 cudaError_t rte_launch_source(const SrcArgs& a, cudaStream_t st);
 cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut, double* mus_out, float* mutf,
                               int N, double* red_max, cudaStream_t st);

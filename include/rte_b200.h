@@ -142,6 +142,26 @@ int rte_images(rte_ctx* ctx, const rte_cplx* out, const rte_source* src, rte_cpl
 int rte_forward(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, rte_cplx* W_out,
                 rte_cplx* trans, rte_cplx* ref, rte_report* report);
 
+/* ---- allocation-free entry point (no counterpart in the reference) ------------------
+ * For callers that must not allocate device memory when they run the solver: work recorded
+ * into a CUDA graph (cudaMalloc is illegal during stream capture), plug-ins whose host
+ * application owns all device memory through its own pool, real-time loops that cannot
+ * wait on the allocator.  It needs no context (rte_create allocates).
+ *
+ * One application of the off-diagonal attenuation operator in exact FP64 (the pair sum of
+ * compute_propabs x dV, without the self-voxel term and without scatter):
+ *   out[r] = sum_{r' != r, |r-r'| < prop_thresh} conj(Y(w)) (Y(w) . in[r']) exp(-tau) dV/(cm |r-r'|^2)
+ * on caller-owned DEVICE buffers: d_mut (N doubles, mu_a + mu_s), d_in and d_out (N*C complex,
+ * reference layout), queued on `stream` (a cudaStream_t, may be NULL).  Scratch memory is a fixed
+ * 64 MiB array inside the library, held on every GPU that loads it; problems whose
+ * (4 + 1) * N * C doubles plus N ints exceed it are rejected with RTE_ERR_UNSUPPORTED (33^3
+ * voxels at nL = 5 fit; the message from rte_last_error(NULL) gives the need).  The first call
+ * on a device looks up the scratch address and uploads constant tables: make it before any
+ * stream capture.  Calls share the scratch array, so calls whose GPU work overlaps race. */
+int rte_attenuate_noalloc(int nx, int ny, int nz, double dx, double dy, double dz, int nL,
+                          double prop_thresh, double cm, const double* d_mut, const rte_cplx* d_in,
+                          rte_cplx* d_out, void* stream);
+
 /* ---- measurement helpers (no reference counterpart) ------------------------------ */
 typedef struct {
   long long launches;     /* kernels launched by this context since the last reset */
