@@ -100,6 +100,20 @@ def dist_setup():
     return ws, rank, local
 
 
+def max_over_ranks(value, device=None):
+    """Max of a per-rank scalar over the process group (device time of a multi-GPU run)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def throughput(world, steps, ms_max):
+    """Whole-job solves/s: every rank solves `steps` phantoms; the job takes the slowest rank's time."""
+    return world * steps / (ms_max / 1e3)
+
+
 def cpu_baseline(seconds=10.0, seed=0):
     """The FP64 oracle (CPU port of the reference path) on a bounded sample: the operator for a set of
     destination voxels against all sources, extrapolated to a full solve (21 applications)."""
@@ -211,11 +225,9 @@ def run_ours(args):
     st = ctx.stats()
     ctx.set_profiling(False)
     if ws > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = max_over_ranks(ms, f"cuda:{dev}")
         torch.distributed.barrier()
-        ms = float(t.item())
-    value = ws * args.steps / (ms / 1e3)
+    value = throughput(ws, args.steps, ms)
 
     # e2e through the C ABI with host buffers (medium H2D, distribution + images D2H)
     e2 = torch.cuda.Event(enable_timing=True)
@@ -231,10 +243,8 @@ def run_ours(args):
     e3.synchronize()
     ms_e2e = e2.elapsed_time(e3)
     if ws > 1:
-        t = torch.tensor([ms_e2e], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = ws * args.steps / (ms_e2e / 1e3)
+        ms_e2e = max_over_ranks(ms_e2e, f"cuda:{dev}")
+    e2e = throughput(ws, args.steps, ms_e2e)
 
     out = None
     if rank == 0:

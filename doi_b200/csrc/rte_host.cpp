@@ -16,6 +16,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
+#include <unordered_map>
 #include <cstdlib>
 #include <string>
 #include <thread>
@@ -312,7 +314,15 @@ struct rte_ctx {
   double* d_red = nullptr;
   double* d_img = nullptr;  // trans, ref (complex)
   bool medium_set = false;
-  int nsplit = 1, chunk = 0;
+  int max_split = 8;
+  std::vector<std::array<int, 3>> splits;  // (kernel key, S, chunk)
+  size_t Kld = 0;
+  double* d_selfp = nullptr;    // self-voxel term [N][nb][C]
+  int* d_self_idx = nullptr;    // voxel -> distinct mu_t
+  double* d_self_lut = nullptr; // [ndistinct][C][C]
+  bool self_lut_ok = false;
+  size_t lut_cap = 0;
+  std::vector<double> h_mom;    // host copy of the moments [K][C][C]
   size_t bytes = 0;
   double last_setup_ms = 0.0;
   // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
@@ -396,7 +406,8 @@ static void free_all(rte_ctx* c) {
     }
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   void* ps[] = {c->d_perm, c->d_mut, c->d_mus, c->d_mutf, c->d_W, c->d_Wn, c->d_sum, c->d_part, c->d_mom,
-                c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img};
+                c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img,
+                c->d_selfp, c->d_self_idx, c->d_self_lut};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -484,13 +495,7 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(cudaEventCreate(&c->ev1), "event");
   if (rc == RTE_OK) cu(rte_upload_sh_tables(c->sh), "SH tables");
   const size_t NC = (size_t)c->N * c->C;
-  // split-K: enough CTAs for >= 4 per SM on a 148-SM part
-  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
-  int S = std::max(1, (4 * 148 + tiles - 1) / tiles);
-  if (const char* e = getenv("RTE_NSPLIT")) S = std::max(1, atoi(e));
-  S = std::min(S, std::max(1, c->N / RTE_PAIR_TS));
-  c->chunk = ((c->N + S - 1) / S + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
-  c->nsplit = (c->N + c->chunk - 1) / c->chunk;
+  if (const char* e = getenv("RTE_MAX_SPLIT")) c->max_split = std::max(1, std::min(32, atoi(e)));
   if (rc == RTE_OK) cu(dalloc(c, &c->d_perm, c->N), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_mut, c->N), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_mus, c->N), "alloc");
@@ -502,7 +507,9 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(dalloc(c, &c->d_aux2, NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_aux3, NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_aux4, NC), "alloc");
-  if (rc == RTE_OK) cu(dalloc(c, &c->d_part, NC * c->nsplit), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_part, NC * c->max_split), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_selfp, NC), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_self_idx, c->N), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_cplx, 2 * NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_red, 8), "alloc");
@@ -552,7 +559,7 @@ static int ensure_moments(rte_ctx* c, double mumax) {
     return fail(c, RTE_ERR_UNSUPPORTED, "self-voxel series: mu_t*voxel = %.3g too large", x);
   K = std::max(K, 4);
   if (K <= c->K && c->d_mom) return RTE_OK;
-  std::vector<double> mom;
+  std::vector<double>& mom = c->h_mom;
   build_moments(c->quad, K, c->dV, mom);
   if (c->d_mom) {
     cudaFree(c->d_mom);
@@ -565,6 +572,51 @@ static int ensure_moments(rte_ctx* c, double mumax) {
   return RTE_OK;
 }
 
+// Self-voxel matrices D(mu) = sum_k mu^k M_k for each distinct mu_t of the medium (a handful for
+// tissue maps and sphere phantoms), and the voxel -> matrix index.  Media with more than 4096
+// distinct values use the power series on the device instead.
+static int build_self_lut(rte_ctx* c) {
+  std::vector<double> mut(c->N);
+  CUDA_TRY(c, cudaMemcpyAsync(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  std::unordered_map<double, int> id;
+  std::vector<int> idx(c->N);
+  std::vector<double> vals;
+  for (int r = 0; r < c->N; r++) {
+    auto it = id.find(mut[r]);
+    if (it == id.end()) {
+      if (vals.size() >= 4096) {
+        c->self_lut_ok = false;
+        return RTE_OK;
+      }
+      it = id.emplace(mut[r], (int)vals.size()).first;
+      vals.push_back(mut[r]);
+    }
+    idx[r] = it->second;
+  }
+  const int C = c->C, K = c->K;
+  std::vector<double> lut(vals.size() * C * C, 0.0);
+  for (size_t q = 0; q < vals.size(); q++) {
+    double* D = &lut[q * C * C];
+    for (int k = K - 1; k >= 0; k--)  // Horner in mu
+      for (int e = 0; e < C * C; e++) D[e] = D[e] * vals[q] + c->h_mom[(size_t)k * C * C + e];
+  }
+  if (lut.size() > c->lut_cap) {
+    if (c->d_self_lut) {
+      cudaFree(c->d_self_lut);
+      c->bytes -= c->lut_cap * sizeof(double);
+      c->d_self_lut = nullptr;
+    }
+    CUDA_TRY(c, dalloc(c, &c->d_self_lut, lut.size()));
+    c->lut_cap = lut.size();
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_self_lut, lut.data(), sizeof(double) * lut.size(), cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_self_idx, idx.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  c->self_lut_ok = true;
+  return RTE_OK;
+}
+
 // mu_t, mu_s (and the FP32 mu_t) from device arrays; the pair kernel becomes stale.
 static int medium_from_device(rte_ctx* c, const double* d_mua, const double* d_mus) {
   CUDA_TRY(c, cudaMemsetAsync(c->d_red + 6, 0, sizeof(double), c->st));
@@ -574,7 +626,9 @@ static int medium_from_device(rte_ctx* c, const double* d_mua, const double* d_m
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->K_valid = false;
   c->medium_set = true;
-  return ensure_moments(c, mumax);
+  int rc = ensure_moments(c, mumax);
+  if (rc) return rc;
+  return build_self_lut(c);
 }
 
 extern "C" int rte_set_medium_voxel(rte_ctx* c, const double* mua, const double* mus) {
@@ -624,7 +678,8 @@ static void scatter_factors(const rte_ctx* c, int flag, double* s) {
 static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
   *stored = false;
   if (c->precision != RTE_PREC_MIXED || c->kernel_mode == RTE_KERNEL_RECOMPUTE) return RTE_OK;
-  const size_t need = (size_t)c->N * c->N * sizeof(float);
+  const size_t ld = ((size_t)c->N + 31) / 32 * 32;  // 128-byte rows
+  const size_t need = (size_t)c->N * ld * sizeof(float);
   if (!c->d_K) {
     size_t fr = 0, tot = 0;
     CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
@@ -633,7 +688,8 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
         return fail(c, RTE_ERR_NOMEM, "pair kernel needs %.1f GB, %.1f GB free", need / 1e9, fr / 1e9);
       return RTE_OK;  // auto: recompute
     }
-    CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * c->N));
+    CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * ld));
+    c->Kld = ld;
   }
   if (!c->K_valid) {
     PairArgs a;
@@ -649,13 +705,9 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     a.prop_thresh = c->prop_thresh;
     a.kscale = c->dV / c->cm;
     a.perm = c->d_perm;
-    a.mut = c->d_mut;
+    a.mutf = c->d_mutf;
     a.Kmat = c->d_K;
-    // one source chunk per 128 destinations is plenty of parallelism here
-    const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
-    int S = std::max(1, (8 * 148 + tiles - 1) / tiles);
-    a.chunk = (c->N + S - 1) / S;
-    a.nsplit = (c->N + a.chunk - 1) / a.chunk;
+    a.Kld = c->Kld;
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
     {
       ProfScope ps(c, 1);
@@ -672,13 +724,57 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
   return RTE_OK;
 }
 
-// One term on the real basis: out = [D] A in.  in64 is FP64 (and inf its FP32 copy for the
-// mixed kernels).  sum != null accumulates the result.  red receives the norms.
+// Split-K plan: the number of source chunks S so that tiles x S CTAs fill whole waves of the
+// kernel's resident CTAs (a partial last wave idles SMs).
+static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
+  const int key = ((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0);
+  for (auto& e : c->splits)
+    if (e[0] == key) {
+      *S_out = e[1];
+      *chunk_out = e[2];
+      return RTE_OK;
+    }
+  int occ = 0;
+  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored, nb, &occ));
+  int sms = 0;
+  CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+  const long long slots = (long long)std::max(occ, 1) * sms;
+  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
+  int bestS = 1;
+  double best = -1.0;
+  for (int S = 1; S <= c->max_split; S++) {
+    const int chunk = ((c->N + S - 1) / S + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
+    const int Sreal = (c->N + chunk - 1) / chunk;
+    if (Sreal != S) continue;
+    const double waves = (double)tiles * S / (double)slots;
+    const double eff = waves / ceil(waves);
+    // prefer the smallest S within 3% of the best fill, and at least one full wave when possible
+    if (eff > best + 0.03 || (best < 0.97 && eff > best)) {
+      best = eff;
+      bestS = S;
+    }
+    if (waves >= 1.0 && eff >= 0.97) break;
+  }
+  if (const char* e = getenv("RTE_NSPLIT")) bestS = std::max(1, std::min(c->max_split, atoi(e)));
+  const int chunk = ((c->N + bestS - 1) / bestS + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
+  const int S = (c->N + chunk - 1) / chunk;
+  c->splits.push_back({key, S, chunk});
+  *S_out = S;
+  *chunk_out = chunk;
+  return RTE_OK;
+}
+
+// One term on the real basis for nb right-hand sides (layout [N][nb][C]): out = [D] A in.
+// in64 is FP64 (and in32 its FP32 copy for the mixed kernels).  sum != null accumulates the result;
+// d_red receives the norms.
 static int apply_term(rte_ctx* c, const double* in64, const float* in32, double* out, float* out32, double* sum,
-                      int flag, int flag_scat) {
+                      int flag, int flag_scat, int nb = 1) {
   const int LA = flag ? c->L : 0;
   bool stored = false;
   int rc = ensure_pair_kernel(c, &stored);
+  if (rc) return rc;
+  int S = 1, chunk = c->N;
+  rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
   if (rc) return rc;
   PairArgs a;
   memset(&a, 0, sizeof a);
@@ -698,12 +794,34 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   a.Win = in64;
   a.Winf = in32;
   a.Kmat = c->d_K;
+  a.Kld = c->Kld;
   a.part = c->d_part;
-  a.chunk = c->chunk;
-  a.nsplit = c->nsplit;
+  a.chunk = chunk;
+  a.nsplit = S;
+  a.nb = nb;
   {
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
+  }
+  SelfArgs sa;
+  memset(&sa, 0, sizeof sa);
+  sa.N = c->N;
+  sa.nb = nb;
+  sa.Cfull = c->C;
+  sa.Cact = (LA + 1) * (LA + 1);
+  sa.K = c->K;
+  sa.W = in64;
+  sa.mut = c->d_mut;
+  sa.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
+  sa.lut = c->d_self_lut;
+  sa.mom = c->d_mom;
+  sa.scale = c->dV / c->cm;
+  sa.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
+  sa.out = c->d_selfp;
+  if (LA < c->L) CUDA_TRY(c, cudaMemsetAsync(c->d_selfp, 0, (size_t)c->N * nb * c->C * sizeof(double), c->st));
+  {
+    ProfScope ps(c, 2);
+    CUDA_TRY(c, rte_launch_self(sa, c->st));
   }
   EpiArgs e;
   memset(&e, 0, sizeof e);
@@ -712,15 +830,11 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   e.ny = c->ny;
   e.nz = c->nz;
   e.Cfull = c->C;
-  e.S = c->nsplit;
+  e.S = S;
+  e.nb = nb;
   e.part = c->d_part;
-  e.Win = in64;
-  e.mut = c->d_mut;
+  e.selfp = c->d_selfp;
   e.mus = c->d_mus;
-  e.mom = c->d_mom;
-  e.K = c->K;
-  e.self_scale = c->dV / c->cm;
-  e.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
   e.flag_scat = flag_scat;
   scatter_factors(c, flag, e.scat);
   e.Wout = out;

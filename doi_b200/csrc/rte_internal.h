@@ -19,28 +19,37 @@ struct PairArgs {
   const float* mutf;    // mu_t per voxel, FP32
   const double* Win;    // current term, real basis, N x Cfull, FP64
   const float* Winf;    // current term, FP32 copy
-  float* Kmat;          // stored pair kernel [source voxel][destination slot]
+  float* Kmat;          // stored pair kernel [source slot][destination slot], row stride Kld
+  size_t Kld;
   double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
   int chunk;            // source voxels per blockIdx.y
   int nsplit;           // S
+  int nb;               // right-hand sides sharing the medium (mixed kernels), layout [N][nb][Cfull]
 };
 
 struct EpiArgs {
-  int N, nx, ny, nz, Cfull, S;
-  const double* part;
-  const double* Win;    // input of this term (for the self-voxel term)
-  const double* mut;
+  int N, nx, ny, nz, Cfull, S, nb;  // nb right-hand sides, layout [N][nb][Cfull]
+  const double* part;   // [S][N][nb][Cfull]
+  const double* selfp;  // self-voxel term [N][nb][Cfull] (may be null)
   const double* mus;
-  const double* mom;    // self-term moments [K][Cfull][Cfull]
-  int K;
-  double self_scale;    // dV / cm
-  int air_no_self;      // FIM model: voxels with mu_t == 0 get no self term
   int flag_scat;
   double scat[RTE_MAX_L + 1];  // per-l scatter factor (times mu_s of the voxel)
   double* Wout;         // FP64 result (may alias nothing else)
   float* Woutf;         // FP32 copy (may be null)
   double* sum;          // running sum (null = do not accumulate)
   double* red;          // [0] ||Wout||^2 [1] ||sum||^2 [2] stop-layer sum of Wout [3] of sum
+};
+
+struct SelfArgs {
+  int N, nb, Cfull, Cact, K;
+  const double* W;      // [N][nb][Cfull]
+  const double* mut;
+  const int* idx;       // voxel -> row of lut (null: power series)
+  const double* lut;    // [ndistinct][Cfull][Cfull]
+  const double* mom;    // [K][Cfull][Cfull]
+  double scale;         // dV / cm
+  int air_no_self;
+  double* out;          // [N][nb][Cfull]
 };
 
 struct ImgArgs {
@@ -81,8 +90,10 @@ cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t s
 cudaError_t rte_upload_sh_tables(const ShTables& t);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int* blocks_per_sm);
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);
 cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st);
+cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st);
 cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
                                cudaStream_t st);
 cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L,

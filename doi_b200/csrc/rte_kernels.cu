@@ -21,6 +21,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <string.h>
+
 #include <type_traits>
 
 #include "rte_internal.h"
@@ -222,64 +224,87 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Mixed precision: path integrals, SH and projections in FP32 (SH in FP64 for l >= 7); FP32
-// partial sums over one shared-memory tile of sources are flushed into FP64 accumulators
-// (shared memory), so no FP32 sum runs over more than RTE_PAIR_TS terms.  STORED reads the
-// precomputed pair kernel k[r'][slot] (FP32) instead of walking the path.
-template <int LA, bool TABLE, bool STORED>
+// Mixed precision: path integrals, SH and projections in FP32 (SH in FP64 for l >= 7).  NB right-
+// hand sides that share the medium are propagated together: the direction, its SH and the pair
+// kernel are computed once per pair and used NB times.  Sources are visited in slot order (the
+// same spatially compact order as the destinations); each 64-source tile (coefficients of all NB
+// right-hand sides and the exact integer coordinates) is staged in shared memory.  Sums: FP32 over
+// one tile in registers, FP32 across tiles in shared memory, FP64 across the split-K chunks in
+// the epilogue.  STORED reads the precomputed pair kernel K[source slot][destination slot] (FP32);
+// otherwise the path integral is walked in FP32.
+template <int LA, bool TABLE, bool STORED, int NB>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
+  constexpr int TS = RTE_PAIR_TS;
+  constexpr int T = RTE_PAIR_THREADS;
   typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
-  __shared__ float sW[RTE_PAIR_TS * C];
-  extern __shared__ double sAcc[];  // [C][RTE_PAIR_THREADS]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sP = reinterpret_cast<float4*>(smem_raw);            // [TS] source (x, y, z) as exact floats
+  float* sW = reinterpret_cast<float*>(sP + TS);                // [TS][NB][C]
+  float* sAcc = sW + TS * NB * C;                               // [NB*C][T]
   const int tid = threadIdx.x;
-  const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
+  const int slot = blockIdx.x * T + tid;
   const bool act = slot < a.N;
   const int r = act ? a.perm[slot] : 0;
   const int plane = a.nx * a.ny;
   const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  const float fk = (float)k, fj = (float)j, fi = (float)i;
   const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
   const float kscalef = (float)a.kscale;
   const float thr = (float)a.prop_thresh;
+  const int vstride = NB * a.Cfull;
 #pragma unroll
-  for (int c = 0; c < C; ++c) sAcc[c * RTE_PAIR_THREADS + tid] = 0.0;
-  float acc[C];
+  for (int q = 0; q < NB * C; ++q) sAcc[q * T + tid] = 0.f;
+  float acc[NB][C];
   const int sb = blockIdx.y * a.chunk;
   const int se = min(a.N, sb + a.chunk);
-  for (int s0 = sb; s0 < se; s0 += RTE_PAIR_TS) {
-    const int ns = min(RTE_PAIR_TS, se - s0);
+  for (int s0 = sb; s0 < se; s0 += TS) {
+    const int ns = min(TS, se - s0);
     __syncthreads();
-    for (int q = tid; q < ns * C; q += RTE_PAIR_THREADS) {
-      const int sv = q / C, c = q - sv * C;
-      sW[q] = a.Winf[(size_t)(s0 + sv) * a.Cfull + c];
+    for (int q = tid; q < ns; q += T) {
+      const int v = a.perm[s0 + q];
+      sP[q] = make_float4((float)(v % a.nx), (float)((v / a.nx) % a.ny), (float)(v / plane), 0.f);
+    }
+    for (int q = tid; q < ns * NB * C; q += T) {
+      const int sv = q / (NB * C), e = q - sv * (NB * C);
+      const int b = e / C, c = e - b * C;
+      sW[q] = a.Winf[(size_t)a.perm[s0 + sv] * vstride + b * a.Cfull + c];
     }
     __syncthreads();
     if (!act) continue;
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[c] = 0.f;
-    int kp = s0 % a.nx, jp = (s0 / a.nx) % a.ny, ip = s0 / plane;
-    const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.N + slot : nullptr;
-    float knext = STORED ? __ldg(Kcol) : 0.f;
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[b][c] = 0.f;
+    const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.Kld + slot : nullptr;
+    float k0 = 0.f, k1 = 0.f;
+    if (STORED) {
+      k0 = __ldg(Kcol);
+      if (ns > 1) k1 = __ldg(Kcol + a.Kld);
+    }
     for (int sv = 0; sv < ns; ++sv) {
-      float kk;
+      float kk = 0.f;
       if (STORED) {
-        kk = knext;
-        if (sv + 1 < ns) knext = __ldg(Kcol + (size_t)(sv + 1) * a.N);
+        kk = k0;
+        k0 = k1;
+        if (sv + 2 < ns) k1 = __ldg(Kcol + (size_t)(sv + 2) * a.Kld);
       }
-      const float ddx = (float)(k - kp) * dxf, ddy = (float)(j - jp) * dyf, ddz = (float)(i - ip) * dzf;
-      const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      const float4 q = sP[sv];
+      const float ddx = (fk - q.x) * dxf, ddy = (fj - q.y) * dyf, ddz = (fi - q.z) * dzf;
+      const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
       bool live;
       float dist = 0.f;
       if (STORED) {
         live = kk != 0.f;
       } else {
         dist = sqrtf(d2);
-        live = (s0 + sv != r) && dist < thr;
+        live = d2 > 0.f && dist < thr;
       }
       if (live) {
         ShT R[C];
         if (TABLE) {
-          const double ex = (double)(k - kp) * a.dx, ey = (double)(j - jp) * a.dy, ez = (double)(i - ip) * a.dz;
+          const double ex = (double)(k - (int)q.x) * a.dx, ey = (double)(j - (int)q.y) * a.dy,
+                       ez = (double)(i - (int)q.z) * a.dz;
           double ux, uy, uz;
           table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
           sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
@@ -287,67 +312,97 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
           const float inv = rsqrtf(d2);
           sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
         }
-        float S = 0.f;
-#pragma unroll
-        for (int c = 0; c < C; ++c) S = fmaf((float)R[c], sW[sv * C + c], S);
         if (!STORED) {
           int Q;
-          const float ps = path_sum<float, float>(i, j, k, ip, jp, kp, a.mutf, a.nx, plane, Q);
-          const float tau = ps * dist / (float)Q;
-          kk = __expf(-tau) * kscalef / d2;
+          const float ps = path_sum<float, float>(i, j, k, (int)q.z, (int)q.y, (int)q.x, a.mutf, a.nx, plane, Q);
+          kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
         }
-        const float t = kk * S;
+        const float* w = sW + sv * (NB * C);
 #pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] = fmaf((float)R[c], t, acc[c]);
-      }
-      if (++kp == a.nx) {
-        kp = 0;
-        if (++jp == a.ny) {
-          jp = 0;
-          ++ip;
+        for (int b = 0; b < NB; ++b) {
+          float S = 0.f;
+#pragma unroll
+          for (int c = 0; c < C; ++c) S = fmaf((float)R[c], w[b * C + c], S);
+          const float t = kk * S;
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[b][c] = fmaf((float)R[c], t, acc[b][c]);
         }
       }
     }
 #pragma unroll
-    for (int c = 0; c < C; ++c) sAcc[c * RTE_PAIR_THREADS + tid] += (double)acc[c];
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < C; ++c) sAcc[(b * C + c) * T + tid] += acc[b][c];
   }
   if (act) {
-    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * a.Cfull;
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * vstride;
 #pragma unroll
-    for (int c = 0; c < C; ++c) o[c] = sAcc[c * RTE_PAIR_THREADS + tid];
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < C; ++c) o[b * a.Cfull + c] = (double)sAcc[(b * C + c) * T + tid];
   }
 }
 
-// Precompute of the pair kernel k[r'][slot] = exp(-tau) dV/(cm d^2) (0 for r' == r or beyond
-// propThresh), path sums in FP64, stored as FP32.  Coalesced over destination slots.
-__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_store_kernel(PairArgs a) {
-  const int slot = blockIdx.x * RTE_PAIR_THREADS + threadIdx.x;
-  if (slot >= a.N) return;
-  const int r = a.perm[slot];
+// Pair-kernel precompute K[s][d] = exp(-tau) dV/(cm |r_d - r_s|^2) over destination slots d and
+// source slots s (0 on the diagonal and beyond propThresh), path sums in FP32.  K is symmetric: one
+// CTA computes a 64x64 tile with source tile index <= destination tile index into shared memory
+// and writes it and its transpose with coalesced stores (a diagonal tile once).
+#define RTE_KT 64
+__global__ void __launch_bounds__(RTE_KT) k_store_kernel(PairArgs a) {
+  __shared__ float tile[RTE_KT][RTE_KT + 1];
+  __shared__ int sxyz[RTE_KT][3];
+  const int ntile = (a.N + RTE_KT - 1) / RTE_KT;
+  // linear CTA index -> (bs, bd) with bs <= bd, row-major over the upper triangle
+  long long t = blockIdx.x;
+  int bd = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
+  while ((long long)(bd + 1) * (bd + 2) / 2 <= t) ++bd;
+  while ((long long)bd * (bd + 1) / 2 > t) --bd;
+  const int bs = (int)(t - (long long)bd * (bd + 1) / 2);
+  if (bd >= ntile) return;
+  const int tid = threadIdx.x;
   const int plane = a.nx * a.ny;
-  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
-  const int sb = blockIdx.y * a.chunk;
-  const int se = min(a.N, sb + a.chunk);
-  int kp = sb % a.nx, jp = (sb / a.nx) % a.ny, ip = sb / plane;
-  for (int rp = sb; rp < se; ++rp) {
-    float kk = 0.f;
-    if (rp != r) {
-      const double ddx = (double)(k - kp) * a.dx, ddy = (double)(j - jp) * a.dy, ddz = (double)(i - ip) * a.dz;
-      const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-      const double dist = sqrt(d2);
-      if (dist < a.prop_thresh) {
-        int Q;
-        const double ps = path_sum<double, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q);
-        kk = (float)(exp(-ps * dist / (double)Q) * a.kscale / d2);
+  const int s0 = bs * RTE_KT, d0 = bd * RTE_KT;
+  {
+    const int sl = s0 + tid;
+    const int v = sl < a.N ? a.perm[sl] : 0;
+    sxyz[tid][0] = v % a.nx;
+    sxyz[tid][1] = (v / a.nx) % a.ny;
+    sxyz[tid][2] = v / plane;
+  }
+  __syncthreads();
+  const int d = d0 + tid;
+  if (d < a.N) {
+    const int r = a.perm[d];
+    const int k = r % a.nx, j = (r / a.nx) % a.ny, i = r / plane;
+    const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
+    const float kscalef = (float)a.kscale, thr = (float)a.prop_thresh;
+    for (int q = 0; q < RTE_KT; ++q) {
+      float kk = 0.f;
+      if (s0 + q < a.N) {
+        const int kp = sxyz[q][0], jp = sxyz[q][1], ip = sxyz[q][2];
+        const float ddx = (float)(k - kp) * dxf, ddy = (float)(j - jp) * dyf, ddz = (float)(i - ip) * dzf;
+        const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+        const float dist = sqrtf(d2);
+        if (d2 > 0.f && dist < thr) {
+          int Q;
+          const float ps = path_sum<float, float>(i, j, k, ip, jp, kp, a.mutf, a.nx, plane, Q);
+          kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
+        }
       }
+      tile[tid][q] = kk;  // [destination][source]
     }
-    a.Kmat[(size_t)rp * a.N + slot] = kk;
-    if (++kp == a.nx) {
-      kp = 0;
-      if (++jp == a.ny) {
-        jp = 0;
-        ++ip;
-      }
+  }
+  __syncthreads();
+  // K[s][d]: row = source slot, contiguous over destination slots
+  for (int q = 0; q < RTE_KT; ++q) {
+    const int sl = s0 + q;
+    if (sl < a.N && d0 + tid < a.N) a.Kmat[(size_t)sl * a.Kld + d0 + tid] = tile[tid][q];
+  }
+  if (bs != bd) {
+    // K[d][s]: row = destination slot of this tile, now acting as the source
+    for (int q = 0; q < RTE_KT; ++q) {
+      const int dl = d0 + q;
+      if (dl < a.N && s0 + tid < a.N) a.Kmat[(size_t)dl * a.Kld + s0 + tid] = tile[q][tid];
     }
   }
 }
@@ -361,63 +416,47 @@ __global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double w2 = 0.0, s2 = 0.0, lw = 0.0, ls = 0.0;
+  const int nb = a.nb > 0 ? a.nb : 1;
+  const int vstride = nb * a.Cfull;
   if (r < a.N) {
-    double v[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) v[c] = 0.0;
-    for (int s = 0; s < a.S; ++s) {
-      const double* p = a.part + ((size_t)s * a.N + r) * a.Cfull;
-#pragma unroll
-      for (int c = 0; c < C; ++c) v[c] += p[c];
-    }
-    const double mu = a.mut[r];
-    if (a.K > 0 && !(a.air_no_self && mu == 0.0)) {
-      double w[C];
-#pragma unroll
-      for (int c = 0; c < C; ++c) w[c] = a.Win[(size_t)r * a.Cfull + c];
-      double selfv[C];
-      // Horner in mu per output coefficient: u = sum_k mu^k (M_k w)_c
-      for (int c = 0; c < C; ++c) {
-        double u = 0.0;
-        for (int kk = a.K - 1; kk >= 0; --kk) {
-          const double* Mrow = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
-          double t = 0.0;
-#pragma unroll
-          for (int cp = 0; cp < C; ++cp) t = fma(__ldg(Mrow + cp), w[cp], t);
-          u = fma(mu, u, t);
-        }
-        selfv[c] = u;
-      }
-#pragma unroll
-      for (int c = 0; c < C; ++c) v[c] = fma(a.self_scale, selfv[c], v[c]);
-    }
-    if (a.flag_scat) {
-      const double ms = a.mus[r];
-#pragma unroll
-      for (int l = 0; l <= LA; ++l)
-#pragma unroll
-        for (int m = -l; m <= l; ++m) v[l * l + l + m] *= a.scat[l] * ms;
-    }
     const bool stop_layer = (r / (a.nx * a.ny)) == a.nz - 1;
-    for (int c = 0; c < a.Cfull; ++c) {
-      const double x = c < C ? v[c] : 0.0;
-      a.Wout[(size_t)r * a.Cfull + c] = x;
-      if (a.Woutf) a.Woutf[(size_t)r * a.Cfull + c] = (float)x;
-      w2 += x * x;
-      double sv = 0.0;
-      if (a.sum) {
-        sv = a.sum[(size_t)r * a.Cfull + c] + x;
-        a.sum[(size_t)r * a.Cfull + c] = sv;
-        s2 += sv * sv;
+    for (int b = 0; b < nb; ++b) {
+      const size_t base = (size_t)r * vstride + (size_t)b * a.Cfull;
+      double v[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[c] = a.selfp ? a.selfp[base + c] : 0.0;
+      for (int s = 0; s < a.S; ++s) {
+        const double* p = a.part + (size_t)s * a.N * vstride + base;
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] += p[c];
       }
-      if (stop_layer) {
-        // sum of Re(w_lm) over m in the complex basis = R_l0 + sqrt2 * R_l,m for even m > 0
-        int l = 0;
-        while ((l + 1) * (l + 1) <= c) ++l;
-        const int m = c - l * l - l;
-        const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
-        lw += wgt * x;
-        ls += wgt * sv;
+      if (a.flag_scat) {
+        const double ms = a.mus[r];
+#pragma unroll
+        for (int l = 0; l <= LA; ++l)
+#pragma unroll
+          for (int m = -l; m <= l; ++m) v[l * l + l + m] *= a.scat[l] * ms;
+      }
+      for (int c = 0; c < a.Cfull; ++c) {
+        const double x = c < C ? v[c] : 0.0;
+        a.Wout[base + c] = x;
+        if (a.Woutf) a.Woutf[base + c] = (float)x;
+        w2 += x * x;
+        double sv = 0.0;
+        if (a.sum) {
+          sv = a.sum[base + c] + x;
+          a.sum[base + c] = sv;
+          s2 += sv * sv;
+        }
+        if (stop_layer) {
+          // sum of Re(w_lm) over m in the complex basis = R_l0 + sqrt2 * R_l,m for even m > 0
+          int l = 0;
+          while ((l + 1) * (l + 1) <= c) ++l;
+          const int m = c - l * l - l;
+          const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
+          lw += wgt * x;
+          ls += wgt * sv;
+        }
       }
     }
   }
@@ -437,6 +476,38 @@ __global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += red[threadIdx.x][w];
     atomicAdd(a.red + threadIdx.x, x);
   }
+}
+
+// Self-voxel term (compute_diagonal_abs, FisherInfo_IO/src/kernels.cu:151-178, and its dV scale)
+// for every voxel, right-hand side and output coefficient (one thread each):
+//   out[r][b][c] = scale * sum_c' D(mu_t(r))[c][c'] W[r][b][c'],
+// D from a table of the medium's distinct mu_t values (lut/idx), else by the power series
+// D(mu) = sum_k mu^k M_k (Horner).  FIM model: voxels with mu_t == 0 (tissue 0) get nothing.
+__global__ void k_self(SelfArgs a) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)a.N * a.nb * a.Cact;
+  if (t >= total) return;
+  const int c = (int)(t % a.Cact);
+  const int b = (int)((t / a.Cact) % a.nb);
+  const int r = (int)(t / ((long long)a.Cact * a.nb));
+  const size_t base = (size_t)r * a.nb * a.Cfull + (size_t)b * a.Cfull;
+  const double mu = a.mut[r];
+  double u = 0.0;
+  if (!(a.air_no_self && mu == 0.0)) {
+    const double* w = a.W + base;
+    if (a.idx) {
+      const double* D = a.lut + ((size_t)a.idx[r] * a.Cfull + c) * a.Cfull;
+      for (int cp = 0; cp < a.Cact; ++cp) u = fma(__ldg(D + cp), __ldg(w + cp), u);
+    } else {
+      for (int kk = a.K - 1; kk >= 0; --kk) {
+        const double* M = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
+        double tk = 0.0;
+        for (int cp = 0; cp < a.Cact; ++cp) tk = fma(__ldg(M + cp), __ldg(w + cp), tk);
+        u = fma(mu, u, tk);
+      }
+    }
+  }
+  a.out[base + c] = a.scale * u;
 }
 
 // Exitance images of the z = nZ-1 and z = 0 faces from the m = 0 coefficients
@@ -642,46 +713,77 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 
 // ---------------------------------------------------------------------------------------------
 // launchers
-template <int LA>
-static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, int stored, cudaStream_t st) {
-  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+template <int LA, bool TABLE, bool STORED, int NB>
+static size_t mixed_smem() {
   constexpr int C = (LA + 1) * (LA + 1);
-  if (precision == 0) {
-    if (table)
-      k_pair_fp64<LA, true><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
-    else
-      k_pair_fp64<LA, false><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
-    return cudaGetLastError();
-  }
-  const size_t smem = (size_t)C * RTE_PAIR_THREADS * sizeof(double);
-  void (*kern)(PairArgs);
-  if (table)
-    kern = stored ? k_pair_mixed<LA, true, true> : k_pair_mixed<LA, true, false>;
-  else
-    kern = stored ? k_pair_mixed<LA, false, true> : k_pair_mixed<LA, false, false>;
+  return sizeof(float4) * RTE_PAIR_TS + sizeof(float) * (RTE_PAIR_TS * NB * C + NB * C * RTE_PAIR_THREADS);
+}
+
+template <int LA, bool TABLE, bool STORED, int NB>
+static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
+  const size_t smem = mixed_smem<LA, TABLE, STORED, NB>();
+  void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
+  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
   kern<<<grid, RTE_PAIR_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st) {
-  switch (LA) {
-    case 0: return launch_pair_LA<0>(a, precision, table, stored, st);
-    case 1: return launch_pair_LA<1>(a, precision, table, stored, st);
-    case 2: return launch_pair_LA<2>(a, precision, table, stored, st);
-    case 3: return launch_pair_LA<3>(a, precision, table, stored, st);
-    case 4: return launch_pair_LA<4>(a, precision, table, stored, st);
-    case 5: return launch_pair_LA<5>(a, precision, table, stored, st);
-    case 6: return launch_pair_LA<6>(a, precision, table, stored, st);
-    case 7: return launch_pair_LA<7>(a, precision, table, stored, st);
+template <int LA, int NB>
+static cudaError_t launch_mixed_nb(const PairArgs& a, int table, int stored, cudaStream_t st, int* occ) {
+  if (table)
+    return stored ? launch_mixed<LA, true, true, NB>(a, st, occ) : launch_mixed<LA, true, false, NB>(a, st, occ);
+  return stored ? launch_mixed<LA, false, true, NB>(a, st, occ) : launch_mixed<LA, false, false, NB>(a, st, occ);
+}
+
+template <int LA>
+static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, int stored, int nb, cudaStream_t st,
+                                  int* occ) {
+  if (precision == 0) {
+    void (*kern)(PairArgs) = table ? k_pair_fp64<LA, true> : k_pair_fp64<LA, false>;
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, 0);
+    dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+    kern<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  switch (nb) {
+    case 1: return launch_mixed_nb<LA, 1>(a, table, stored, st, occ);
+    case 2: return launch_mixed_nb<LA, 2>(a, table, stored, st, occ);
+    case 4: return launch_mixed_nb<LA, 4>(a, table, stored, st, occ);
   }
   return cudaErrorInvalidValue;
 }
 
+static cudaError_t pair_dispatch(const PairArgs& a, int LA, int precision, int table, int stored, int nb,
+                                 cudaStream_t st, int* occ) {
+  switch (LA) {
+    case 0: return launch_pair_LA<0>(a, precision, table, stored, nb, st, occ);
+    case 1: return launch_pair_LA<1>(a, precision, table, stored, nb, st, occ);
+    case 2: return launch_pair_LA<2>(a, precision, table, stored, nb, st, occ);
+    case 3: return launch_pair_LA<3>(a, precision, table, stored, nb, st, occ);
+    case 4: return launch_pair_LA<4>(a, precision, table, stored, nb, st, occ);
+    case 5: return launch_pair_LA<5>(a, precision, table, stored, nb, st, occ);
+    case 6: return launch_pair_LA<6>(a, precision, table, stored, nb, st, occ);
+    case 7: return launch_pair_LA<7>(a, precision, table, stored, nb, st, occ);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st) {
+  return pair_dispatch(a, LA, precision, table, stored, a.nb > 0 ? a.nb : 1, st, nullptr);
+}
+
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int* blocks_per_sm) {
+  PairArgs dummy;
+  memset(&dummy, 0, sizeof dummy);
+  return pair_dispatch(dummy, LA, precision, table, stored, nb, nullptr, blocks_per_sm);
+}
+
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st) {
-  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
-  k_store_kernel<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+  const long long nt = (a.N + RTE_KT - 1) / RTE_KT;
+  k_store_kernel<<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -698,6 +800,12 @@ cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st) {
     case 7: k_epilogue<7><<<blocks, 128, 0, st>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st) {
+  const long long total = (long long)a.N * a.nb * a.Cact;
+  k_self<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 

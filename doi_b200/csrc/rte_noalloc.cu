@@ -163,11 +163,10 @@ extern "C" int rte_attenuate_noalloc(int nx, int ny, int nz, double dx, double d
     ep.nz = nz;
     ep.Cfull = (int)C;
     ep.S = S;
+    ep.nb = 1;
     ep.part = part;
-    ep.Win = a.Win;
-    ep.mut = d_mut;
+    ep.selfp = nullptr;
     ep.mus = d_mut;
-    ep.K = 0;
     ep.Wout = part_k ? o2 : o1;
     ep.red = red;
     e = rte_launch_epilogue(ep, nL, st);

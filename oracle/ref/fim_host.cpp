@@ -4,7 +4,7 @@
 // (kernels.cu lines 1-418 -- the device functions and kernels, no host launch
 // code --, dist.cu, sph_harm.cu, inits.cu, neumann.cu, rte.cu with main renamed,
 // iniparser.cu, dictionary.cu) are compiled as host C++ under fim_emu.h by
-// oracle/Makefile, straight from where they lie in the reference tree.  This file
+// oracle/build.sh, straight from where they lie in the reference tree.  This file
 // replaces only the one function that needs a GPU: prop_abs()
 // (FisherInfo_IO/src/kernels.cu:704-811), re-enacted here launch by launch: the
 // same grid (nX/10, nY/10), blocks of 10x10x5, the same four kernels in the same
@@ -16,6 +16,8 @@
 //       <prefix>_trans.bin, <prefix>_ref.bin (complex images), <prefix>_meta.txt
 //   fim_host apply <file.par> <in.bin> <flag> <flag_scat> <out.bin>
 //       one prop_abs pass over all slabs (flag = all-L, flag_scat = scatter)
+//   fim_host diag <file.par> <out.bin>
+//       the self-voxel table diag_terms_host (MAX_TISS_NUM*MAX_NL^4 complex, dist.cu:362-533)
 #include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -169,6 +171,10 @@ int main(int argc, char** argv) {
             g_prop_abs_calls / NUM_DEVICES - 1, (double)geom->prop_thresh, (double)info_stat_host->cm,
             geom->delX, geom->delY, geom->delZ);
     fclose(f);
+    return 0;
+  }
+  if (!strcmp(argv[1], "diag")) {
+    write_dist(argv[3], diag_terms_host, (size_t)MAX_TISS_NUM * MAX_NL * MAX_NL * MAX_NL * MAX_NL);
     return 0;
   }
   if (!strcmp(argv[1], "apply") && argc >= 7) {

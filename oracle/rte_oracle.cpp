@@ -412,12 +412,12 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
         cd v = acc[c] * dV;
         if (flag_scat) {
           if (p->mode == 1) {
-            if (p->g != 0.0) {
+            if (flag) {  // prop_scat_dev receives the same flag as the other kernels
               float cmf = (float)cm;
               double gi = (double)(int)p->g;  // __int2double_rn(int) truncation, kernels.cu:409
               v = (double)cmf * pow(gi, (double)l) * v * mus[r];
             } else {
-              v = v * mus[r];  // kernels.cu:412 (flag = 0 when g == 0, neumann.cu:74-79)
+              v = v * mus[r];  // kernels.cu:412 (Neumann passes flag = 0 when g == 0, neumann.cu:74-79)
             }
           } else {
             v = cm * pow(p->g, (double)l) * mus[r] * v;

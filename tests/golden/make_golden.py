@@ -1,0 +1,183 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference's own code.
+
+The reference ships no tests or golden outputs.  This script builds (oracle/build.sh) and runs:
+  * oracle/_ref/fim_host -- the FisherInfo_IO sources compiled as host C++, its GPU kernels
+    (kernels.cu:151-418) executed once per emulated CUDA thread, its own Neumann()/StopIteration,
+    source, diag-term and image code;
+  * oracle/_ref/rte_cpu  -- the CPU package built from its own sources;
+on small inputs (.par files written below; tissue maps generated with a fixed seed, plus the two
+20^3 maps shipped in `GPU package/utility/`), and stores the outputs as .npz files.  It needs the
+reference tree (default /root/reference, or $RTE_REFERENCE_DIR); the fixtures it writes are
+committed so the tests run without it.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("RTE_REFERENCE_DIR", "/root/reference")
+
+FIM_PAR = """[Runtime]
+TransFile = trans.out
+ReflectFile = ref.out
+PhaseFile = phase.out
+[Algorithm]
+nL = {nL}
+nTerms = 5
+[Geometry]
+nX = {nx}
+nY = {ny}
+nZ = {nz}
+xMin = {xmin}
+xMax = {xmax}
+yMin = {ymin}
+yMax = {ymax}
+zMin = 0
+zMax = {zmax}
+propThresh = {prop}
+selfsubVox = 1
+[Phantom]
+NoTiss = {ntiss}
+TissMapFile = {tiss}
+{tissue_lines}
+g = {g}
+n = {n}
+[Source]
+posX = 0
+posY = 0
+magnitude = {mag}
+"""
+
+CPU_PAR = """[Runtime]
+TransFile = trans.out
+ReflectFile = ref.out
+PhaseFile = phase.out
+[Algorithm]
+nL = {nL}
+nTerms = 30
+[Geometry]
+nX = {n}
+nY = {n}
+nZ = {n}
+xMin = {lo}
+xMax = {hi}
+yMin = {lo}
+yMax = {hi}
+zMin = 0
+zMax = {zmax}
+propThresh = 10
+[Phantom]
+mua = {mua}
+mus = {mus}
+g = {g}
+n = 1.0
+c = 1.0
+[Source]
+posX = 0
+posY = 0
+diam = {diam}
+magnitude = 1.0
+"""
+
+
+def run(cmd, cwd):
+    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{cmd} failed:\n{r.stdout[-2000:]}")
+    return r.stdout
+
+
+def fim_case(name, nx, ny, nz, nL, tiss, mua_t, mus_t, g=0.8, n=1.0, prop=10.0, mag=1.0, apply_seed=None):
+    d = tempfile.mkdtemp(prefix="golden_")
+    tiss.astype(np.uint8).tofile(os.path.join(d, "tiss.bin"))
+    lines = "\n".join(f"TissAbs{t} = {mua_t[t]!r}\nTissSc{t} = {mus_t[t]!r}" for t in range(1, len(mua_t)))
+    par = FIM_PAR.format(nL=nL, nx=nx, ny=ny, nz=nz, xmin=-nx * 0.05, xmax=nx * 0.05, ymin=-ny * 0.05,
+                         ymax=ny * 0.05, zmax=nz * 0.1, prop=prop, ntiss=len(mua_t) - 1, tiss="tiss.bin",
+                         tissue_lines=lines, g=g, n=n, mag=mag)
+    open(os.path.join(d, "t.par"), "w").write(par)
+    exe = os.path.join(ROOT, "oracle", "_ref", "fim_host")
+    N, C = nx * ny * nz, (nL + 1) ** 2
+    out = dict(nx=nx, ny=ny, nz=nz, nL=nL, g=g, n=n, prop=prop, mag=mag, tiss=tiss.astype(np.uint8),
+               mua_t=np.array(mua_t), mus_t=np.array(mus_t), par=par)
+    run([exe, "forward", "t.par", "res"], d)
+    rd = lambda f, k: np.fromfile(os.path.join(d, f), np.complex128).reshape(k)
+    out["src"] = rd("res_src.bin", (N, C))
+    out["out"] = rd("res_out.bin", (N, C))
+    out["trans"] = rd("res_trans.bin", (ny, nx))
+    out["ref"] = rd("res_ref.bin", (ny, nx))
+    meta = dict(l.split() for l in open(os.path.join(d, "res_meta.txt")))
+    out["terms"] = int(meta["terms"])
+    out["cm"] = float(meta["cm"])
+    out["delX"] = float(meta["delX"])
+    run([exe, "diag", "t.par", "diag.bin"], d)
+    out["diag"] = np.fromfile(os.path.join(d, "diag.bin"), np.complex128).reshape(25, 25, 4)[:C, :C, :]
+    if apply_seed is not None:
+        rng = np.random.default_rng(apply_seed)
+        W = rng.standard_normal((N, C)) + 1j * rng.standard_normal((N, C))
+        W.tofile(os.path.join(d, "in.bin"))
+        for flag, fs in ((1, 1), (1, 0), (0, 1)):
+            run([exe, "apply", "t.par", "in.bin", str(flag), str(fs), f"o{flag}{fs}.bin"], d)
+            out[f"apply_{flag}{fs}"] = rd(f"o{flag}{fs}.bin", (N, C))
+        out["apply_seed"] = apply_seed
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name, "terms", out["terms"])
+
+
+def read_img(path):
+    b = open(path, "rb").read()
+    nx, ny = np.frombuffer(b[:8], np.int32)
+    v = np.frombuffer(b[8:], np.float64)
+    return (v[: nx * ny] + 1j * v[nx * ny: 2 * nx * ny]).reshape(ny, nx)
+
+
+def cpu_case(name, n, nL, mua, mus, g, diam):
+    d = tempfile.mkdtemp(prefix="golden_")
+    par = CPU_PAR.format(nL=nL, n=n, lo=-n * 0.05, hi=n * 0.05, zmax=n * 0.1, mua=mua, mus=mus, g=g, diam=diam)
+    open(os.path.join(d, "c.par"), "w").write(par)
+    log = run([os.path.join(ROOT, "oracle", "_ref", "rte_cpu"), "c.par"], d)
+    terms = int([l for l in log.splitlines() if l.startswith("Neumann series:")][-1].split()[-1]) - 1
+    photons = float([l for l in log.splitlines() if l.startswith("Number of photons total")][-1].split()[-1])
+    side = {}
+    for f in os.listdir(d):
+        if f.startswith("SideFace"):
+            b = open(os.path.join(d, f), "rb").read()
+            side[f.split(".")[0]] = np.frombuffer(b, np.uint8)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), n=n, nL=nL, mua=mua, mus=mus, g=g, diam=diam,
+                        trans=read_img(os.path.join(d, "trans.out")), ref=read_img(os.path.join(d, "ref.out")),
+                        terms=terms, photons=photons, par=par)
+    print("wrote", name, "terms", terms)
+
+
+def main():
+    if not os.path.isdir(REF):
+        sys.exit(f"reference tree {REF} not found")
+    subprocess.run(["bash", os.path.join(ROOT, "oracle", "build.sh")], check=True)
+    rng = np.random.default_rng(2024)
+    # 1. uniform medium, 10x10x20, L=2, the reference stop rule (FIM forward)
+    fim_case("fim_uniform_10x10x20_L2", 10, 10, 20, 2, np.ones(2000, np.uint8), [0.0, 0.01], [0.0, 1.0],
+             apply_seed=1)
+    # 2. three tissues at random plus 5% air voxels (never on the source column: mu_s/mu_t of air is
+    #    0/0 in the source term), L=2, g = 0.9, n = 1.4 (cm = float(1/n)), magnitude 2
+    tiss = rng.integers(1, 4, 2000).astype(np.uint8)
+    air = rng.random(2000) < 0.05
+    col = (np.arange(2000) % 10 == 5) & ((np.arange(2000) // 10) % 10 == 5)
+    tiss[air & ~col] = 0
+    fim_case("fim_tissues_10x10x20_L2", 10, 10, 20, 2, tiss, [0.0, 0.01, 0.05, 0.02], [0.0, 1.0, 1.5, 0.7],
+             g=0.9, n=1.4, prop=1.5, mag=2.0, apply_seed=2)
+    # 3. the shipped non-uniform 20^3 tissue map, L=1
+    shipped = np.fromfile(os.path.join(REF, "GPU package", "utility", "tiss_map_nonuni.bin"), np.uint8)
+    fim_case("fim_shipped_nonuni_20_L1", 20, 20, 20, 1, shipped, [0.0, 0.01, 0.02, 0.03], [0.0, 1.0, 1.2, 0.8])
+    # 4. the CPU package on the 11^3, L=3 configuration (uniform, g = 0.8)
+    cpu_case("cpu_uniform_11_L3", 11, 3, 0.01, 1.0, 0.8, 0.1)
+    # 5. the CPU package, isotropic scattering (g = 0: only l = 0 propagated), 9^3, L=2
+    cpu_case("cpu_isotropic_9_L2", 9, 2, 0.05, 2.0, 0.0, 0.1)
+
+
+if __name__ == "__main__":
+    main()

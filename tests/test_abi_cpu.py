@@ -1,0 +1,59 @@
+"""The C-ABI library without a GPU: it loads, exports every function include/rte_b200.h declares, and
+fails with a status code and a message (never a crash, never a CPU fallback) when no device exists."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "rte_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(rte_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_parses():
+    names = _declared()
+    assert "rte_neumann" in names and "rte_prop_abs" in names and "rte_attenuate_noalloc" in names
+
+
+def test_library_exports_every_declared_symbol(rte):
+    lib = rte.load_library()
+    missing = [n for n in _declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(rte.rte.EXPORTS) <= set(_declared())
+
+
+def test_create_without_device_fails_loudly(rte):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(rte.RteError) as e:
+        rte.Context(5, 5, 5, nL=2)
+    assert "rte_create failed" in str(e.value)
+
+
+def test_bad_config_rejected(rte):
+    lib = rte.load_library()
+    from doi_b200.rte import _Config
+    h = ctypes.c_void_p()
+    cfg = _Config(0, 5, 5, -1, 1, -1, 1, 0, 1, 3, 10.0, 1, 0.8, 1.0, 1.0, 0, 0, 0, 0)
+    assert lib.rte_create(ctypes.byref(cfg), ctypes.byref(h)) == 1  # RTE_ERR_ARG
+    assert b"grid" in lib.rte_last_error(None)
+    cfg = _Config(5, 5, 5, -1, 1, -1, 1, 0, 1, 9, 10.0, 1, 0.8, 1.0, 1.0, 0, 0, 0, 0)
+    assert lib.rte_create(ctypes.byref(cfg), ctypes.byref(h)) == 6  # RTE_ERR_UNSUPPORTED (nL > 7)
+
+
+def test_noalloc_rejects_bad_arguments_without_device(rte):
+    lib = rte.load_library()
+    f = lib.rte_attenuate_noalloc
+    f.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                                 ctypes.c_void_p]
+    assert f(0, 4, 4, 0.1, 0.1, 0.1, 2, 1.0, 1.0, None, None, None, None) == 1
+    # too large for the built-in scratch: rejected before any device work
+    assert f(128, 128, 128, 0.1, 0.1, 0.1, 7, 1.0, 1.0, 1, 1, 1, None) == 6
+    assert b"scratch" in lib.rte_last_error(None)

@@ -1,0 +1,83 @@
+"""The FP64 oracle against golden outputs of the reference's own code (tests/golden/make_golden.py).
+
+FIM fixtures: the FisherInfo_IO kernels and host code run on the CPU (oracle/_ref/fim_host); the
+oracle's FIM mode must reproduce them to rounding (1e-12 relative L2), including the term count of
+the reference stop rule, the source, the self-voxel table and both exitance images.
+CPU fixtures: the CPU package (oracle/_ref/rte_cpu) images and term count; oracle CPU mode.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIM_CASES = ["fim_uniform_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_shipped_nonuni_20_L1"]
+CPU_CASES = ["cpu_uniform_11_L3", "cpu_isotropic_9_L2"]
+
+
+def _fim_params(O, g):
+    nx, ny, nz, L = (int(g[k]) for k in ("nx", "ny", "nz", "nL"))
+    dx = float(g["delX"])
+    # Geometry extents are floats in the reference; delX (written by the run) already carries that
+    return O.params(nx, ny, nz, dx, dx, dx, L, float(g["g"]), float(g["cm"]), float(np.float32(g["prop"])),
+                    mode=O.MODE_FIM, ssv=1, x_min=-nx * 0.05, y_min=-ny * 0.05)
+
+
+@pytest.mark.parametrize("case", FIM_CASES)
+def test_fim_forward(oracle, case):
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    p = _fim_params(oracle, g)
+    tiss = g["tiss"]
+    mua, mus = g["mua_t"][tiss], g["mus_t"][tiss]
+    src = oracle.source(p, mua, mus, kind=oracle.SRC_FIM)
+    assert rel(src, g["src"]) < 1e-13
+    out, _, nt = oracle.neumann(p, mua, mus, src, src, 1, oracle.STOP_REFERENCE, n0=2)
+    assert nt == int(g["terms"])
+    assert rel(out, g["out"]) < 1e-12
+    tr, rf = oracle.images(p, mua, mus, out, 1, mag=float(g["mag"]))
+    assert rel(tr, g["trans"]) < 1e-12
+    assert rel(rf, g["ref"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", FIM_CASES[:2])
+def test_fim_single_pass(oracle, case):
+    """One prop_abs pass of the reference kernels on a random complex input."""
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    p = _fim_params(oracle, g)
+    tiss = g["tiss"]
+    mua, mus = g["mua_t"][tiss], g["mus_t"][tiss]
+    N, C = tiss.size, (int(g["nL"]) + 1) ** 2
+    rng = np.random.default_rng(int(g["apply_seed"]))
+    W = rng.standard_normal((N, C)) + 1j * rng.standard_normal((N, C))
+    for flag, fs in ((1, 1), (1, 0), (0, 1)):
+        got = oracle.apply(p, mua, mus, W, flag, fs)
+        ref = g[f"apply_{flag}{fs}"]
+        assert rel(got, ref) < 1e-12, (flag, fs)
+
+
+@pytest.mark.parametrize("case", FIM_CASES)
+def test_fim_self_voxel_table(oracle, case):
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    L = int(g["nL"])
+    dx = float(g["delX"])
+    for t in range(1, len(g["mua_t"])):
+        mut = float(g["mua_t"][t] + g["mus_t"][t])
+        D = oracle.self_matrix(0, L, 1, mut, dx, dx, dx)
+        assert rel(D, g["diag"][:, :, t]) < 1e-13
+
+
+@pytest.mark.parametrize("case", CPU_CASES)
+def test_cpu_package_forward(oracle, case):
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    n, L = int(g["n"]), int(g["nL"])
+    N = n ** 3
+    p = oracle.params(n, n, n, 0.1, 0.1, 0.1, L, float(g["g"]), 1.0, 10.0, mode=oracle.MODE_CPU,
+                      x_min=-n * 0.05, y_min=-n * 0.05)
+    mua, mus = np.full(N, float(g["mua"])), np.full(N, float(g["mus"]))
+    r = oracle.forward(p, mua, mus, src_kind=oracle.SRC_CPU, img_mode=2, stop_rule=oracle.STOP_REFERENCE, n0=1,
+                       diam=float(g["diam"]))
+    assert r["terms"] == int(g["terms"])
+    assert rel(r["trans"], g["trans"]) < 1e-12
+    assert rel(r["ref"], g["ref"]) < 1e-12
