@@ -46,8 +46,8 @@ def algorithmic_counts(n=N_SIDE, Lo=L):
     # sum over ordered pairs of |di| for one axis = n^2 * n^2 * sum_{a,b} |a-b| = n^4 * (n^3 - n)/3
     s1 = (n ** 4) * (n ** 3 - n) / 3.0
     steps = 3 * s1
-    # FLOP per launch of the pair-apply kernel: 7C (SH recurrence 3C + two C-length MACs 4C) + 10
-    # (direction) per coupled pair; the precompute: 2 per Siddon step + 25 (geometry, exp, scale).
+    # FLOP per launch of the one-source pair-apply kernel: 7C (SH recurrence 3C + two C-length MACs
+    # 4C) + 10 (direction) per coupled pair; the precompute: 2 per Siddon step + 25 (geometry, exp).
     apply_flop = pairs * (7 * C + 10)
     store_flop = 2 * steps + 25 * pairs
     # canonical per-solve count (flops_term = pairs(7C + 2S + 25) + N(2C^2 + 4C), (terms+1) terms)
@@ -189,6 +189,12 @@ def run_ours(args):
                     device=dev)
     src = R.Source(pos_x=0.0, pos_y=0.0, kind=R.SRC_COLUMN)
     stop = R.Stop(R.STOP_FIXED, TERMS)
+    # batched form: B of the four collimated z=0 sources at (+-0.825, +-0.825) cm of the adjoint
+    # configuration, solved together on each phantom (B = 2 by default: the best throughput of the
+    # kernel instantiations; B = 4 runs out of registers)
+    B = args.batch
+    srcs = [R.Source(pos_x=x, pos_y=y, kind=R.SRC_COLUMN) for x, y in
+            ((-0.825, -0.825), (0.825, -0.825), (-0.825, 0.825), (0.825, 0.825))][:B] if B > 1 else [src]
     nsteps = args.steps + args.warmup
     seeds = [1000 * rank + s for s in range(nsteps)]
     media = [phantom(s) for s in seeds]
@@ -202,6 +208,8 @@ def run_ours(args):
     def step(k):
         a, b = dmedia[k]
         ctx.set_medium_device(a.data_ptr(), b.data_ptr())
+        if B > 1:
+            return ctx.forward_batch(srcs, stop, want_W=False, want_images=True)
         return ctx.forward(src, stop, want_W=False, want_images=True)
 
     for k in range(args.warmup):
@@ -227,43 +235,51 @@ def run_ours(args):
     if ws > 1:
         ms = max_over_ranks(ms, f"cuda:{dev}")
         torch.distributed.barrier()
-    value = throughput(ws, args.steps, ms)
+    value = throughput(ws, args.steps * B, ms)
 
     # e2e through the C ABI with host buffers (medium H2D, distribution + images D2H)
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     h2d = 2 * counts["N"] * 8
-    d2h = counts["N"] * counts["C"] * 16 + 2 * N_SIDE * N_SIDE * 16
+    d2h = B * (counts["N"] * counts["C"] * 16 + 2 * N_SIDE * N_SIDE * 16)
     torch.cuda.synchronize(dev)
     e2.record(stream)
     for k in range(args.warmup, nsteps):
         ctx.set_medium_voxel(*media[k])
-        ctx.forward(src, stop, want_W=True, want_images=True)
+        if B > 1:
+            ctx.forward_batch(srcs, stop, want_W=True, want_images=True)
+        else:
+            ctx.forward(src, stop, want_W=True, want_images=True)
     e3.record(stream)
     e3.synchronize()
     ms_e2e = e2.elapsed_time(e3)
     if ws > 1:
         ms_e2e = max_over_ranks(ms_e2e, f"cuda:{dev}")
-    e2e = throughput(ws, args.steps, ms_e2e)
+    e2e = throughput(ws, args.steps * B, ms_e2e)
 
     out = None
     if rank == 0:
         # accuracy of this precision against the plain FP64 method (itself held to the oracle by the
         # parity tests) on the first timed phantom, and the plain method's own speed
         ctx.set_medium_voxel(*media[args.warmup])
-        r_mixed = ctx.forward(src, stop, want_W=True)
+        r_mixed = ctx.forward_batch(srcs, stop, want_W=True) if B > 1 else ctx.forward(src, stop, want_W=True)
+        if B > 1:
+            r_mixed = {k: r_mixed[k][0] for k in ("W", "trans", "ref")}
         ref_err, plain = None, None
         if prec == R.PREC_MIXED and not args.skip_fp64_check:
             c64 = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_FP64, device=dev)
             c64.set_medium_voxel(*media[args.warmup])
-            r64 = c64.forward(src, stop, want_W=True)
+            r64 = c64.forward(srcs[0], stop, want_W=True)
             rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
             ref_err = {"W": rel(r_mixed["W"], r64["W"]), "trans": rel(r_mixed["trans"], r64["trans"]),
                        "ref": rel(r_mixed["ref"], r64["ref"])}
             plain = 1e3 / r64["ms_device"]
             c64.close()
         avg_pair_ms = st["ms_pair"] / max(st["n_pair"], 1)
-        achieved = counts["apply_flop"] / (avg_pair_ms * 1e-3) / 1e12
+        nbk = 1 if B == 1 else (2 if B <= 2 else 4)  # right-hand sides per launch
+        # algorithmic FLOP per launch: per coupled pair 3C (SH) + 4C per right-hand side + 10 (direction)
+        apply_flop = counts["pairs"] * (3 * counts["C"] + 4 * counts["C"] * B + 10)
+        achieved = apply_flop / (avg_pair_ms * 1e-3) / 1e12
         peak = peak32 if prec == R.PREC_MIXED else peak64
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
@@ -273,8 +289,11 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64acc" if prec == R.PREC_MIXED else "f64", "data": "synthetic",
-            "config": {"workload": "33^3 voxels (0.1 cm), L=5, 3-sphere seeded phantom per step, collimated "
-                                   "centre source, 20 Neumann terms + final A, z-face images",
+            "config": {"workload": (f"33^3 voxels (0.1 cm), L=5, 3-sphere seeded phantom per step, {B} collimated "
+                                    "z=0 sources from (+-0.825, +-0.825) cm solved as one batch" if B > 1 else
+                                    "33^3 voxels (0.1 cm), L=5, 3-sphere seeded phantom per step, collimated "
+                                    "centre source") + ", 20 Neumann terms + final A, z-face images",
+                       "batch": B,
                        "precision": args.precision, "pair_kernel": "stored FP32 (recomputed per solve)"
                        if prec == R.PREC_MIXED else "recomputed per term",
                        "grid": N_SIDE, "L": L, "terms": TERMS,
@@ -284,7 +303,7 @@ def run_ours(args):
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic, "kernel": "k_pair_mixed<5,stored>" if prec == R.PREC_MIXED
                          else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
-                         "flop_per_launch": counts["apply_flop"],
+                         "flop_per_launch": apply_flop, "rhs_per_launch": nbk,
                          "peak_source": "measured by rte_measure_fma_peak (8-chain FMA probe) in this run"},
             "cpu_baseline": None,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -294,7 +313,7 @@ def run_ours(args):
             "plain_fp64_solves_per_s": plain,
             "kernel_ms_per_step": {"pair": st["ms_pair"] / args.steps, "store": st["ms_store"] / args.steps,
                                    "epilogue": st["ms_epi"] / args.steps},
-            "solve_tflops_canonical": counts["solve_flop"] / (ms / args.steps / 1e3) / 1e12,
+            "solve_tflops_canonical": B * counts["solve_flop"] / (ms / args.steps / 1e3) / 1e12,
             "peaks_tflops": {"fp32": peak32, "fp64": peak64},
         }
         if ws == 1 and not args.skip_cpu:
@@ -320,6 +339,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64-check", action="store_true")
     ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
+    ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
+                    help="sources per phantom solved together (1 = one source per solve)")
     args = ap.parse_args()
     global N_SIDE
     N_SIDE = args.n

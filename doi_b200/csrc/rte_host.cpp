@@ -323,6 +323,22 @@ struct rte_ctx {
   bool self_lut_ok = false;
   size_t lut_cap = 0;
   std::vector<double> h_mom;    // host copy of the moments [K][C][C]
+  int* d_islot = nullptr;       // voxel -> slot
+  float4* d_slot_xyz = nullptr; // slot -> (x, y, z, voxel)
+  int* d_err = nullptr;         // bounded-wait failure flag of the pair kernels
+  int cpad = 0;                 // FP32 source row length (nb = 1)
+  int cstride = 0;              // FP32 stride of one right-hand side within a row (even)
+  // batched solves (several sources on one medium): buffers for up to bcap right-hand sides
+  int bcap = 0;
+  double *d_bW = nullptr, *d_bWn = nullptr, *d_bsum = nullptr, *d_bres = nullptr, *d_bball = nullptr;
+  float* d_bWf = nullptr;
+  size_t part_cap = 0, selfp_cap = 0;
+  // detectors and gradient
+  double* d_h = nullptr;        // [6][C] face flux weights
+  double *d_S = nullptr, *d_out = nullptr, *d_e = nullptr, *d_lam = nullptr, *d_y = nullptr;
+  double *d_gt = nullptr, *d_gs = nullptr, *d_J = nullptr, *d_rho = nullptr, *d_dlut = nullptr;
+  std::vector<double> h_h;      // host copy of the face weights
+  size_t dlut_cap = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
   // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
@@ -407,7 +423,9 @@ static void free_all(rte_ctx* c) {
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   void* ps[] = {c->d_perm, c->d_mut, c->d_mus, c->d_mutf, c->d_W, c->d_Wn, c->d_sum, c->d_part, c->d_mom,
                 c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img,
-                c->d_selfp, c->d_self_idx, c->d_self_lut};
+                c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
+                c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
+                c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -509,14 +527,37 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(dalloc(c, &c->d_aux4, NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_part, NC * c->max_split), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_selfp, NC), "alloc");
+  c->part_cap = NC * c->max_split;
+  c->selfp_cap = NC;
   if (rc == RTE_OK) cu(dalloc(c, &c->d_self_idx, c->N), "alloc");
-  if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, NC), "alloc");
+  c->cstride = (c->C + 1) / 2 * 2;
+  c->cpad = (c->cstride + 3) / 4 * 4;
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, (size_t)c->N * c->cpad), "alloc");
+  if (rc == RTE_OK) cu(cudaMemset(c->d_Wf, 0, sizeof(float) * (size_t)c->N * c->cpad), "memset");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_islot, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_slot_xyz, c->N), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_err, 1), "alloc");
+  if (rc == RTE_OK) cu(cudaMemset(c->d_err, 0, sizeof(int)), "memset");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_cplx, 2 * NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_red, 8), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 5 * (size_t)c->nx * c->ny), "alloc");  // trans, ref (complex), ballistic
   if (rc == RTE_OK) {
     std::vector<int> p = morton_perm(c->nx, c->ny, c->nz);
+    std::vector<int> inv(c->N);
+    std::vector<float4> xyz(c->N);
+    for (int q = 0; q < c->N; q++) {
+      const int v = p[q];
+      inv[v] = q;
+      int bits;
+      memcpy(&bits, &v, sizeof bits);
+      float w;
+      memcpy(&w, &bits, sizeof w);
+      xyz[q] = make_float4((float)(v % c->nx), (float)((v / c->nx) % c->ny), (float)(v / (c->nx * c->ny)), w);
+    }
     cu(cudaMemcpy(c->d_perm, p.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice), "perm upload");
+    if (rc == RTE_OK) cu(cudaMemcpy(c->d_islot, inv.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice), "upload");
+    if (rc == RTE_OK)
+      cu(cudaMemcpy(c->d_slot_xyz, xyz.data(), sizeof(float4) * c->N, cudaMemcpyHostToDevice), "upload");
   }
   if (rc != RTE_OK) {
     free_all(c);
@@ -595,11 +636,28 @@ static int build_self_lut(rte_ctx* c) {
     idx[r] = it->second;
   }
   const int C = c->C, K = c->K;
-  std::vector<double> lut(vals.size() * C * C, 0.0);
+  std::vector<double> lut(vals.size() * C * C, 0.0), dlut(vals.size() * C * C, 0.0);
   for (size_t q = 0; q < vals.size(); q++) {
     double* D = &lut[q * C * C];
+    double* dD = &dlut[q * C * C];
     for (int k = K - 1; k >= 0; k--)  // Horner in mu
       for (int e = 0; e < C * C; e++) D[e] = D[e] * vals[q] + c->h_mom[(size_t)k * C * C + e];
+    for (int k = K - 1; k >= 1; k--)  // d/dmu
+      for (int e = 0; e < C * C; e++) dD[e] = dD[e] * vals[q] + (double)k * c->h_mom[(size_t)k * C * C + e];
+  }
+  {
+    int rc = 0;
+    if (dlut.size() > c->dlut_cap) {
+      if (c->d_dlut) {
+        cudaFree(c->d_dlut);
+        c->bytes -= c->dlut_cap * sizeof(double);
+        c->d_dlut = nullptr;
+      }
+      CUDA_TRY(c, dalloc(c, &c->d_dlut, dlut.size()));
+      c->dlut_cap = dlut.size();
+    }
+    (void)rc;
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_dlut, dlut.data(), sizeof(double) * dlut.size(), cudaMemcpyHostToDevice, c->st));
   }
   if (lut.size() > c->lut_cap) {
     if (c->d_self_lut) {
@@ -735,7 +793,8 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
       return RTE_OK;
     }
   int occ = 0;
-  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored, nb, &occ));
+  const int cpad = (nb * ((c->C + 1) / 2 * 2) + 3) / 4 * 4;
+  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored, nb, cpad, &occ));
   int sms = 0;
   CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
   const long long slots = (long long)std::max(occ, 1) * sms;
@@ -799,6 +858,10 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   a.chunk = chunk;
   a.nsplit = S;
   a.nb = nb;
+  a.slot_xyz = c->d_slot_xyz;
+  a.cstride = (c->C + 1) / 2 * 2;
+  a.cpad = (nb * a.cstride + 3) / 4 * 4;
+  a.err = c->d_err;
   {
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
@@ -839,12 +902,27 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   scatter_factors(c, flag, e.scat);
   e.Wout = out;
   e.Woutf = out32;
+  e.islot = c->d_islot;
+  e.cstride = (c->C + 1) / 2 * 2;
+  e.cpad = (nb * e.cstride + 3) / 4 * 4;
   e.sum = sum;
   e.red = c->d_red;
   CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
   {
     ProfScope ps(c, 2);
     CUDA_TRY(c, rte_launch_epilogue(e, LA, c->st));
+  }
+  return RTE_OK;
+}
+
+// A pair kernel whose bounded wait ran out leaves its result invalid and raises d_err.
+static int check_kernel_err(rte_ctx* c) {
+  int h = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  if (h) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    return fail(c, RTE_ERR_TIMEOUT, "a pair kernel's wait for its shared-memory tile ran out");
   }
   return RTE_OK;
 }
@@ -861,7 +939,7 @@ static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* 
   double rel = 0.0;
   if (flag) {
     CUDA_TRY(c, cudaMemcpyAsync(c->d_W, W0, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_W, c->d_Wf, NC, c->st)));
+    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_W, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C, c->cstride, c->st)));
     const int flag_l = c->cfg.g != 0.0 ? 1 : 0;  // neumann.cu:74-79
     const int rule = force_terms >= 0 ? RTE_STOP_FIXED : stop->rule;
     const int maxt = force_terms >= 0 ? force_terms : (rule == RTE_STOP_REFERENCE ? 10000 : stop->max_terms);
@@ -909,10 +987,12 @@ static int neumann_real(rte_ctx* c, const double* W0, const double* S0, double* 
   // final A on the running sum (no scatter), neumann.cu:95-118
   float* in32 = nullptr;
   if (mixed) {
-    CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_sum, c->d_Wf, NC, c->st)));
+    CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_sum, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C, c->cstride, c->st)));
     in32 = c->d_Wf;
   }
   int rc = apply_term(c, c->d_sum, in32, res, nullptr, nullptr, 1, 0);
+  if (rc) return rc;
+  rc = check_kernel_err(c);
   if (rc) return rc;
   if (nterms) *nterms = terms;
   if (last_rel) *last_rel = rel;
@@ -951,14 +1031,16 @@ extern "C" int rte_prop_abs(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int f
   const size_t NC = (size_t)c->N * c->C;
   const bool mixed = c->precision == RTE_PREC_MIXED;
   // part 1 -> d_W, part 2 -> d_sum (both scratch here)
-  if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_aux1, c->d_Wf, NC, c->st)));
+  if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_aux1, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C, c->cstride, c->st)));
   rc = apply_term(c, c->d_aux1, c->d_Wf, c->d_W, nullptr, nullptr, flag, flag_scat);
   if (rc) return rc;
   if (has2) {
-    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_f64_to_f32(c->d_aux2, c->d_Wf, NC, c->st)));
+    if (mixed) CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_aux2, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C, c->cstride, c->st)));
     rc = apply_term(c, c->d_aux2, c->d_Wf, c->d_sum, nullptr, nullptr, flag, flag_scat);
     if (rc) return rc;
   }
+  rc = check_kernel_err(c);
+  if (rc) return rc;
   return download_cplx(c, c->d_W, has2 ? c->d_sum : nullptr, out);
 }
 
@@ -1023,15 +1105,16 @@ static int source_columns(const rte_ctx* c, const rte_source* s, std::vector<int
 
 // xi = D A xi_beam on the pencil columns, built on the device into d_dst (real basis), with the
 // ballistic transmission per column in d_ball (dist.cu:66-101; Dist.c:1077-1128 for RTE_SRC_CPU).
-static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst) {
+static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vstride = 0, double* d_ball = nullptr,
+                         bool zero = true) {
   if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
   std::vector<int> cols;
   double scale;
   if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d", s->kind);
   if ((int)cols.size() > RTE_MAX_SRC_COLS) return fail(c, RTE_ERR_UNSUPPORTED, "beam covers more than %d columns", RTE_MAX_SRC_COLS);
-  const size_t NC = (size_t)c->N * c->C;
-  double* d_ball = c->d_img + 4 * (size_t)c->nx * c->ny;
-  CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, NC * sizeof(double), c->st));
+  if (vstride <= 0) vstride = c->C;
+  if (!d_ball) d_ball = c->d_img + 4 * (size_t)c->nx * c->ny;
+  if (zero) CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, (size_t)c->N * vstride * sizeof(double), c->st));
   CUDA_TRY(c, cudaMemsetAsync(d_ball, 0, (size_t)c->nx * c->ny * sizeof(double), c->st));
   if (cols.empty()) return RTE_OK;
   SrcArgs a;
@@ -1050,6 +1133,7 @@ static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst) {
   a.dz = c->dz;
   a.dV = c->dV;
   a.z_min = c->cfg.z_min;
+  a.vstride = vstride;
   a.mut = c->d_mut;
   a.mus = c->d_mus;
   a.W = d_dst;
@@ -1106,7 +1190,7 @@ static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a) {
 // images of a real-basis distribution on the device; with_ball adds the ballistic term left in
 // d_ball by the last launch_source.
 static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool with_ball, rte_cplx* trans,
-                      rte_cplx* ref) {
+                      rte_cplx* ref, int vstride = 0, const double* d_ball = nullptr) {
   ImgArgs a;
   memset(&a, 0, sizeof a);
   a.nx = c->nx;
@@ -1114,11 +1198,12 @@ static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool
   a.nz = c->nz;
   a.Cfull = c->C;
   a.L = c->L;
+  a.vstride = vstride > 0 ? vstride : c->C;
   a.out = d_out;
   int rc = image_weights(c, s, a);
   if (rc) return rc;
   const size_t np = (size_t)c->nx * c->ny;
-  a.ball = with_ball ? c->d_img + 4 * np : nullptr;
+  a.ball = with_ball ? (d_ball ? d_ball : c->d_img + 4 * np) : nullptr;
   a.trans = c->d_img;
   a.ref = c->d_img + 2 * np;
   CUDA_TRY(c, (c->launches++, rte_launch_images(a, c->st)));
@@ -1208,16 +1293,19 @@ extern "C" int rte_measure_fma_peak(int device, int fp64, double* tflops) {
   cudaEventCreate(&e1);
   const int blocks = sms * 8, iters = fp64 ? 20000 : 40000;
   double best = 0;
-  for (int rep = 0; rep < 4; rep++) {
-    cudaEventRecord(e0, 0);
-    rte_launch_fma_peak(fp64, iters, sink, 0, blocks);
-    cudaEventRecord(e1, 0);
-    cudaEventSynchronize(e1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    const double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0;
-    if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
-  }
+  // FP32: the faster of scalar and packed (f32x2) FMA streams
+  const int variants[2] = {fp64 ? 1 : 0, fp64 ? 1 : 2};
+  for (int v = 0; v < (fp64 ? 1 : 2); v++)
+    for (int rep = 0; rep < 4; rep++) {
+      cudaEventRecord(e0, 0);
+      rte_launch_fma_peak(variants[v], iters, sink, 0, blocks);
+      cudaEventRecord(e1, 0);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0 * (variants[v] == 2 ? 2.0 : 1.0);
+      if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
   cudaError_t e = cudaGetLastError();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1260,5 +1348,486 @@ extern "C" int rte_get_stats(rte_ctx* c, rte_stats* out) {
     c->ms_acc[k] = 0;
     c->n_acc[k] = 0;
   }
+  return RTE_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched forward solves: nsrc sources on one medium propagated together (the pair kernels reuse
+// each pair's direction, SH and kernel value for every source).
+static const int kMaxBatch = 4;
+
+template <class T>
+static int grow(rte_ctx* c, T** p, size_t& cap, size_t n) {
+  if (n <= cap) return RTE_OK;
+  if (*p) {
+    cudaFree(*p);
+    c->bytes -= cap * sizeof(T);
+    *p = nullptr;
+  }
+  CUDA_TRY(c, dalloc(c, p, n));
+  cap = n;
+  return RTE_OK;
+}
+
+static int ensure_batch(rte_ctx* c, int nb) {
+  const size_t NC = (size_t)c->N * c->C;
+  int rc = grow(c, &c->d_part, c->part_cap, NC * nb * c->max_split);
+  if (!rc) rc = grow(c, &c->d_selfp, c->selfp_cap, NC * nb);
+  if (rc || nb <= c->bcap) return rc;
+  double** bufs[] = {&c->d_bW, &c->d_bWn, &c->d_bsum, &c->d_bres};
+  for (double** b : bufs) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+    CUDA_TRY(c, dalloc(c, b, NC * nb));
+  }
+  if (c->d_bball) cudaFree(c->d_bball);
+  c->d_bball = nullptr;
+  CUDA_TRY(c, dalloc(c, &c->d_bball, (size_t)nb * c->nx * c->ny));
+  if (c->d_bWf) cudaFree(c->d_bWf);
+  c->d_bWf = nullptr;
+  const int cp = (nb * c->cstride + 3) / 4 * 4;
+  CUDA_TRY(c, dalloc(c, &c->d_bWf, (size_t)c->N * cp));
+  CUDA_TRY(c, cudaMemset(c->d_bWf, 0, sizeof(float) * (size_t)c->N * cp));
+  c->bcap = nb;
+  return RTE_OK;
+}
+
+extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                                 rte_cplx* W_out, rte_cplx* trans, rte_cplx* ref, rte_report* rep) {
+  if (!c || !srcs || !stop || nsrc < 1) return fail(c, RTE_ERR_ARG, "bad argument");
+  if (nsrc > kMaxBatch) return fail(c, RTE_ERR_UNSUPPORTED, "at most %d sources per batch", kMaxBatch);
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (stop->rule == RTE_STOP_REFERENCE)
+    return fail(c, RTE_ERR_UNSUPPORTED, "batched solves take a fixed or relative-L2 stop rule");
+  const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  if (c->precision != RTE_PREC_MIXED || nsrc == 1) {  // one source at a time
+    double ms = 0;
+    rte_report r1;
+    for (int b = 0; b < nsrc; b++) {
+      int rc = rte_forward(c, &srcs[b], stop, W_out ? W_out + b * NC : nullptr, trans ? trans + b * np : nullptr,
+                           ref ? ref + b * np : nullptr, &r1);
+      if (rc) return rc;
+      ms += r1.ms_device;
+    }
+    if (rep) {
+      *rep = r1;
+      rep->ms_device = ms;
+    }
+    return RTE_OK;
+  }
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  const int nb = nsrc <= 2 ? 2 : 4;  // kernel instantiations; extra right-hand sides stay zero
+  int rc = ensure_batch(c, nb);
+  if (rc) return rc;
+  const int vs = nb * c->C;
+  const int cp = (nb * c->cstride + 3) / 4 * 4;
+  cudaEvent_t t0, t1;
+  CUDA_TRY(c, cudaEventCreate(&t0));
+  CUDA_TRY(c, cudaEventCreate(&t1));
+  CUDA_TRY(c, cudaEventRecord(t0, c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bW, 0, NC * nb * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bball, 0, np * nb * sizeof(double), c->st));
+  for (int b = 0; b < nsrc && !rc; b++)
+    rc = launch_source(c, &srcs[b], c->d_bW + b * c->C, vs, c->d_bball + b * np, false);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_bsum, c->d_bW, NC * nb * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
+  const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
+  int terms = 0;
+  double rel = 0.0;
+  while (terms < stop->max_terms) {
+    rc = apply_term(c, c->d_bW, c->d_bWf, c->d_bWn, c->d_bWf, c->d_bsum, flag_l, 1, nb);
+    if (rc) return rc;
+    std::swap(c->d_bW, c->d_bWn);
+    terms++;
+    if (stop->rule == RTE_STOP_REL_L2) {
+      double hred[4];
+      CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+      rel = hred[1] > 0 ? sqrt(hred[0] / hred[1]) : 0.0;
+      if (rel < stop->tol) break;
+    }
+  }
+  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bsum, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
+  rc = apply_term(c, c->d_bsum, c->d_bWf, c->d_bres, nullptr, nullptr, 1, 0, nb);
+  if (!rc) rc = check_kernel_err(c);
+  for (int b = 0; b < nsrc && !rc && (trans || ref); b++)
+    rc = run_images(c, c->d_bres + b * c->C, &srcs[b], true, trans ? trans + b * np : nullptr,
+                    ref ? ref + b * np : nullptr, vs, c->d_bball + b * np);
+  if (!rc) CUDA_TRY(c, cudaEventRecord(t1, c->st));
+  for (int b = 0; b < nsrc && !rc && W_out; b++) {
+    CUDA_TRY(c, (c->launches++, rte_launch_to_cplx(c->d_bres + b * c->C, nullptr, c->d_cplx, c->N, c->L, c->st, vs)));
+    CUDA_TRY(c, cudaMemcpyAsync(W_out + b * NC, c->d_cplx, NC * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  }
+  float ms = 0;
+  if (!rc) {
+    CUDA_TRY(c, cudaStreamSynchronize(c->st));
+    cudaEventElapsedTime(&ms, t0, t1);
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (rc) return rc;
+  if (rep) {
+    rep->terms = terms;
+    rep->last_rel = rel;
+    rep->ms_device = ms;
+    rep->ms_setup = c->last_setup_ms;
+  }
+  return RTE_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Detectors: exitant flux through the six faces, binned; the adjoint gradient of a binned-flux misfit.
+// Face order: z- (z = 0), z+ (z = nZ-1), y-, y+, x-, x+.
+
+// h_f[c] = cm * (pixel area) * int_{w.n > 0} R_c(w) (w.n) dw, by Gauss-Legendre in w.n and a
+// uniform rule around n (exact for the polynomial integrand up to the order used).
+static void face_weights(rte_ctx* c) {
+  const int C = c->C;
+  c->h_h.assign(6 * C, 0.0);
+  std::vector<double> mu, wmu;
+  gauss01(24, mu, wmu);
+  const int M = 64;
+  const double nrm[6][3] = {{0, 0, -1}, {0, 0, 1}, {0, -1, 0}, {0, 1, 0}, {-1, 0, 0}, {1, 0, 0}};
+  const double area[6] = {c->dx * c->dy, c->dx * c->dy, c->dx * c->dz, c->dx * c->dz, c->dy * c->dz, c->dy * c->dz};
+  std::vector<double> R(C);
+  for (int f = 0; f < 6; f++) {
+    const double* n = nrm[f];
+    double e1[3], e2[3];
+    if (fabs(n[2]) > 0.5) {
+      e1[0] = 1; e1[1] = 0; e1[2] = 0;
+    } else {
+      e1[0] = 0; e1[1] = 0; e1[2] = 1;
+    }
+    e2[0] = n[1] * e1[2] - n[2] * e1[1];
+    e2[1] = n[2] * e1[0] - n[0] * e1[2];
+    e2[2] = n[0] * e1[1] - n[1] * e1[0];
+    for (size_t a = 0; a < mu.size(); a++) {
+      const double m = mu[a], s = sqrt(1.0 - m * m);
+      for (int b = 0; b < M; b++) {
+        const double ps = 2.0 * M_PI * (b + 0.5) / M;
+        const double cp = cos(ps), sp = sin(ps);
+        double w[3];
+        for (int d = 0; d < 3; d++) w[d] = m * n[d] + s * (cp * e1[d] + sp * e2[d]);
+        sh_real_host(c->sh, c->L, w[0], w[1], w[2], R.data());
+        const double wt = wmu[a] * (2.0 * M_PI / M) * m;
+        for (int q = 0; q < C; q++) c->h_h[f * C + q] += wt * R[q];
+      }
+    }
+    for (int q = 0; q < C; q++) c->h_h[f * C + q] *= c->cm * area[f];
+  }
+}
+
+static int ensure_detector_buffers(rte_ctx* c) {
+  if (c->d_h) return RTE_OK;
+  const size_t NC = (size_t)c->N * c->C;
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  face_weights(c);
+  CUDA_TRY(c, dalloc(c, &c->d_h, c->h_h.size()));
+  CUDA_TRY(c, cudaMemcpy(c->d_h, c->h_h.data(), sizeof(double) * c->h_h.size(), cudaMemcpyHostToDevice));
+  double** bufs[] = {&c->d_S, &c->d_out, &c->d_e, &c->d_lam, &c->d_y};
+  for (double** b : bufs) CUDA_TRY(c, dalloc(c, b, NC));
+  CUDA_TRY(c, dalloc(c, &c->d_gt, c->N));
+  CUDA_TRY(c, dalloc(c, &c->d_gs, c->N));
+  CUDA_TRY(c, dalloc(c, &c->d_J, npix));
+  CUDA_TRY(c, dalloc(c, &c->d_rho, npix));
+  return RTE_OK;
+}
+
+// face geometry: rows x cols of pixels and offset of each face in the concatenated pixel array
+static void face_dims(const rte_ctx* c, int f, int& P, int& Q, size_t& off) {
+  const size_t a0 = (size_t)c->nx * c->ny, a1 = (size_t)c->nz * c->nx, a2 = (size_t)c->nz * c->ny;
+  const size_t offs[6] = {0, a0, 2 * a0, 2 * a0 + a1, 2 * a0 + 2 * a1, 2 * a0 + 2 * a1 + a2};
+  off = offs[f];
+  if (f < 2) {
+    P = c->ny;
+    Q = c->nx;
+  } else if (f < 4) {
+    P = c->nz;
+    Q = c->nx;
+  } else {
+    P = c->nz;
+    Q = c->ny;
+  }
+}
+
+// fraction of pixel p (of P along an edge) inside bin a (of nb)
+static inline double overlap(int p, int P, int a, int nb) {
+  const double lo = std::max((double)p / P, (double)a / nb), hi = std::min((double)(p + 1) / P, (double)(a + 1) / nb);
+  return hi > lo ? (hi - lo) * P : 0.0;
+}
+
+// bins[f][a][b] = sum over the face's pixels of overlap x overlap x J
+static void bin_faces(const rte_ctx* c, const rte_detector* d, const std::vector<double>& J, double* bins) {
+  const int nb = d->nbins;
+  for (int f = 0; f < 6; f++) {
+    double* B = bins + (size_t)f * nb * nb;
+    for (int q = 0; q < nb * nb; q++) B[q] = 0.0;
+    if (!((d->faces >> f) & 1)) continue;
+    int P, Q;
+    size_t off;
+    face_dims(c, f, P, Q, off);
+    for (int p = 0; p < P; p++)
+      for (int a = 0; a < nb; a++) {
+        const double wa = overlap(p, P, a, nb);
+        if (wa == 0.0) continue;
+        for (int q = 0; q < Q; q++)
+          for (int b = 0; b < nb; b++) {
+            const double wb = overlap(q, Q, b, nb);
+            if (wb != 0.0) B[a * nb + b] += wa * wb * J[off + (size_t)p * Q + q];
+          }
+      }
+  }
+}
+
+// rho(pixel) = sum over bins of dL/dbin x (pixel's weight in the bin)
+static void unbin_faces(const rte_ctx* c, const rte_detector* d, const double* dbins, std::vector<double>& rho) {
+  const int nb = d->nbins;
+  std::fill(rho.begin(), rho.end(), 0.0);
+  for (int f = 0; f < 6; f++) {
+    if (!((d->faces >> f) & 1)) continue;
+    const double* B = dbins + (size_t)f * nb * nb;
+    int P, Q;
+    size_t off;
+    face_dims(c, f, P, Q, off);
+    for (int p = 0; p < P; p++)
+      for (int a = 0; a < nb; a++) {
+        const double wa = overlap(p, P, a, nb);
+        if (wa == 0.0) continue;
+        for (int q = 0; q < Q; q++)
+          for (int b = 0; b < nb; b++) {
+            const double wb = overlap(q, Q, b, nb);
+            if (wb != 0.0) rho[off + (size_t)p * Q + q] += wa * wb * B[a * nb + b];
+          }
+      }
+  }
+}
+
+// forward solve of one source leaving S (running sum) in d_S and out = A S in d_out; fluxes of
+// all face pixels (ballistic included) in J.
+static int forward_with_flux(rte_ctx* c, const rte_source* s, const rte_stop* stop, std::vector<double>& J, int* terms) {
+  const size_t NC = (size_t)c->N * c->C;
+  int rc = launch_source(c, s, c->d_aux1);
+  if (rc) return rc;
+  rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_out, 1, stop, -1, terms, nullptr);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_S, c->d_sum, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  FaceArgs fa;
+  memset(&fa, 0, sizeof fa);
+  fa.nx = c->nx;
+  fa.ny = c->ny;
+  fa.nz = c->nz;
+  fa.Cfull = c->C;
+  fa.vstride = c->C;
+  fa.out = c->d_out;
+  fa.h = c->d_h;
+  fa.ball = c->d_img + 4 * (size_t)c->nx * c->ny;
+  fa.J = c->d_J;
+  CUDA_TRY(c, (c->launches++, rte_launch_face_flux(fa, c->st)));
+  CUDA_TRY(c, cudaMemcpyAsync(J.data(), c->d_J, J.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  return RTE_OK;
+}
+
+static int check_detector(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* d) {
+  if (!srcs || !stop || !d || nsrc < 1) return fail(c, RTE_ERR_ARG, "null argument");
+  if (d->nbins < 1 || d->nbins > 1024 || d->faces <= 0 || d->faces > 63) return fail(c, RTE_ERR_ARG, "bad detector");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (stop->rule == RTE_STOP_REFERENCE) return fail(c, RTE_ERR_UNSUPPORTED, "detectors take a fixed or relative-L2 stop rule");
+  for (int q = 0; q < nsrc; q++)
+    if (srcs[q].kind == RTE_SRC_CPU) return fail(c, RTE_ERR_UNSUPPORTED, "detectors support single-column sources");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  return ensure_detector_buffers(c);
+}
+
+extern "C" int rte_detector_flux(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                                 const rte_detector* d, double* flux) {
+  if (!c) return RTE_ERR_ARG;
+  int rc = check_detector(c, nsrc, srcs, stop, d);
+  if (rc) return rc;
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  std::vector<double> J(npix);
+  for (int q = 0; q < nsrc; q++) {
+    int terms = 0;
+    rc = forward_with_flux(c, &srcs[q], stop, J, &terms);
+    if (rc) return rc;
+    bin_faces(c, d, J, flux + (size_t)q * 6 * d->nbins * d->nbins);
+  }
+  return RTE_OK;
+}
+
+// Gradient of L = sum_{sources, bins} (F - target)^2 with respect to per-voxel mu_a and mu_s by the
+// adjoint method.  With S = sum_k (DA)^k xi, out = A S and e = dL/dout:
+//   lambda = (I - (DA)^T)^-1 A^T e, computed as P A (P e + sum_k (DA)^k D A P e), P = (-1)^l;
+//   y = e + D lambda;
+//   dL/dmu_t(v) = -sum_{pairs} len(v) k (y.R)(R.S) + (dV/cm) y_v . dDself/dmu S_v;
+//   dL/dmu_s(v) += lambda_v . scat_l (A S)_v;   plus the source column and ballistic terms.
+extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                            const rte_detector* d, const double* target, double* loss, double* g_mua,
+                            double* g_mus) {
+  if (!c || !target || !g_mua || !g_mus) return fail(c, RTE_ERR_ARG, "null argument");
+  int rc = check_detector(c, nsrc, srcs, stop, d);
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  const int nb = d->nbins;
+  const bool mixed = c->precision == RTE_PREC_MIXED;
+  std::vector<double> J(npix), rho(npix), bins(6 * nb * nb), dbins(6 * nb * nb);
+  std::vector<double> ga(c->N, 0.0), gsum(c->N, 0.0);
+  CUDA_TRY(c, cudaMemsetAsync(c->d_gt, 0, sizeof(double) * c->N, c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_gs, 0, sizeof(double) * c->N, c->st));
+  double L2 = 0.0;
+  double scat[RTE_MAX_L + 1];
+  scatter_factors(c, 1, scat);
+  std::vector<double> mut(c->N), mus(c->N);
+  CUDA_TRY(c, cudaMemcpy(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(mus.data(), c->d_mus, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  for (int sidx = 0; sidx < nsrc; sidx++) {
+    const rte_source* s = &srcs[sidx];
+    int terms = 0;
+    rc = forward_with_flux(c, s, stop, J, &terms);
+    if (rc) return rc;
+    bin_faces(c, d, J, bins.data());
+    const double* T = target + (size_t)sidx * 6 * nb * nb;
+    for (int f = 0; f < 6; f++)
+      for (int q = 0; q < nb * nb; q++) {
+        const size_t i = (size_t)f * nb * nb + q;
+        const double r = ((d->faces >> f) & 1) ? bins[i] - T[i] : 0.0;
+        L2 += r * r;
+        dbins[i] = 2.0 * r;
+      }
+    unbin_faces(c, d, dbins.data(), rho);
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_rho, rho.data(), npix * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_e, 0, NC * sizeof(double), c->st));
+    FaceArgs fa;
+    memset(&fa, 0, sizeof fa);
+    fa.nx = c->nx;
+    fa.ny = c->ny;
+    fa.nz = c->nz;
+    fa.Cfull = c->C;
+    fa.vstride = c->C;
+    fa.h = c->d_h;
+    fa.rho = c->d_rho;
+    fa.e = c->d_e;
+    CUDA_TRY(c, (c->launches++, rte_launch_adjoint_seed(fa, c->st)));
+    // adjoint series
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_aux3, c->d_e, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_aux3, c->N, c->L, c->C, c->st)));
+    if (mixed)
+      CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_aux3, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C,
+                                                          c->cstride, c->st)));
+    rc = apply_term(c, c->d_aux3, c->d_Wf, c->d_aux4, nullptr, nullptr, 1, 1);
+    if (rc) return rc;
+    CUDA_TRY(c, (c->launches++, rte_launch_axpy(c->d_aux3, c->d_aux4, 1.0, NC, c->st)));
+    rc = neumann_real(c, c->d_aux4, c->d_aux3, c->d_lam, 1, stop, std::max(terms - 1, 0), nullptr, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_lam, c->N, c->L, c->C, c->st)));
+    CUDA_TRY(c, (c->launches++, rte_launch_y_field(c->d_y, c->d_e, c->d_lam, c->d_mus, scat, c->N, c->L, c->C, c->st)));
+    // back-projection through exp(-tau)
+    BpArgs bp;
+    memset(&bp, 0, sizeof bp);
+    bp.N = c->N;
+    bp.nx = c->nx;
+    bp.ny = c->ny;
+    bp.nz = c->nz;
+    bp.Cfull = c->C;
+    bp.dx = c->dx;
+    bp.dy = c->dy;
+    bp.dz = c->dz;
+    bp.prop_thresh = c->prop_thresh;
+    bp.kscale = c->dV / c->cm;
+    bp.perm = c->d_perm;
+    bp.islot = c->d_islot;
+    bp.mut = c->d_mut;
+    bp.mutf = c->d_mutf;
+    bp.y = c->d_y;
+    bp.S = c->d_S;
+    bool stored = false;
+    rc = ensure_pair_kernel(c, &stored);
+    if (rc) return rc;
+    bp.Kmat = stored ? c->d_K : nullptr;
+    bp.Kld = c->Kld;
+    bp.g = c->d_gt;
+    const size_t accb = (size_t)c->N * (mixed ? sizeof(float) : sizeof(double));
+    bp.use_smem = accb <= 200 * 1024 ? 1 : 0;
+    const int tiles = (c->N + RTE_BP_THREADS - 1) / RTE_BP_THREADS;
+    int S = std::max(1, std::min(16, (4 * 148 + tiles - 1) / tiles));
+    bp.chunk = (c->N + S - 1) / S;
+    bp.nsplit = (c->N + bp.chunk - 1) / bp.chunk;
+    {
+      ProfScope ps(c, 0);
+      CUDA_TRY(c, rte_launch_backproject(bp, c->L, mixed ? 0 : 1, c->st));
+    }
+    GradLocalArgs gl;
+    memset(&gl, 0, sizeof gl);
+    gl.N = c->N;
+    gl.Cfull = c->C;
+    gl.Cact = c->C;
+    gl.y = c->d_y;
+    gl.lam = c->d_lam;
+    gl.S = c->d_S;
+    gl.out = c->d_out;
+    gl.mus = c->d_mus;
+    gl.mut = c->d_mut;
+    gl.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
+    gl.dlut = c->d_dlut;
+    gl.mom = c->d_mom;
+    gl.K = c->K;
+    gl.scale = c->dV / c->cm;
+    gl.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
+    for (int l = 0; l <= RTE_MAX_L; l++) gl.scat[l] = scat[l];
+    gl.gt = c->d_gt;
+    gl.gs = c->d_gs;
+    CUDA_TRY(c, (c->launches++, rte_launch_grad_local(gl, c->st)));
+    // source column and ballistic transmission (host; nz voxels)
+    std::vector<int> cols;
+    double scale;
+    if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source");
+    for (int col : cols) {
+      const int nz = c->nz, plane = c->nx * c->ny;
+      std::vector<double> lamc((size_t)nz * c->C);
+      for (int i = 0; i < nz; i++)
+        CUDA_TRY(c, cudaMemcpyAsync(&lamc[(size_t)i * c->C], c->d_lam + ((size_t)i * plane + col) * c->C,
+                                    c->C * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+      std::vector<double> X(nz), Lam(nz), Tt(nz), E(nz);
+      double att = 1.0;
+      for (int i = 0; i < nz; i++) {
+        const int r = i * plane + col;
+        E[i] = exp(-mut[r] * c->dz);
+        Tt[i] = att;
+        att *= E[i];
+        double lam = 0.0, gl2 = 1.0;
+        for (int l = 0; l <= c->L; l++) {
+          lam += lamc[(size_t)i * c->C + l * l + l] * scale * gl2 * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) / c->dV;
+          gl2 *= c->cfg.g;
+        }
+        Lam[i] = lam;
+        X[i] = (mus[r] / mut[r]) * Tt[i] * (1 - E[i]);
+      }
+      double tail = 0.0;  // sum_{i' > i} Lam X
+      const double ball = s->mag * att;
+      const double rho_b = rho[np + (size_t)col];  // z+ face pixel of this column
+      for (int i = nz - 1; i >= 0; i--) {
+        const int r = i * plane + col;
+        const double mt = mut[r], ms = mus[r], ma = mt - ms;
+        const double common = (ms / mt) * Tt[i] * c->dz * E[i];
+        ga[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (-ms / (mt * mt)) + common) - c->dz * tail - rho_b * ball * c->dz;
+        gsum[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (ma / (mt * mt)) + common) - c->dz * tail - rho_b * ball * c->dz;
+        tail += Lam[i] * X[i];
+      }
+    }
+  }
+  std::vector<double> gt(c->N), gs(c->N);
+  CUDA_TRY(c, cudaMemcpyAsync(gt.data(), c->d_gt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(gs.data(), c->d_gs, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  rc = check_kernel_err(c);
+  if (rc) return rc;
+  for (int r = 0; r < c->N; r++) {
+    g_mua[r] = gt[r] + ga[r];
+    g_mus[r] = gt[r] + gs[r] + gsum[r];
+  }
+  if (loss) *loss = L2;
   return RTE_OK;
 }

@@ -8,6 +8,7 @@
 #define RTE_PAIR_THREADS 128  // destination voxels per CTA (one per thread)
 #define RTE_PAIR_TS 64        // source voxels staged in shared memory per step
 #define RTE_MAX_MOM 48        // self-term power-series terms
+#define RTE_BP_THREADS 256    // destination voxels per CTA of the back-projection
 
 struct PairArgs {
   int N, nx, ny, nz, Cfull;
@@ -25,6 +26,10 @@ struct PairArgs {
   int chunk;            // source voxels per blockIdx.y
   int nsplit;           // S
   int nb;               // right-hand sides sharing the medium (mixed kernels), layout [N][nb][Cfull]
+  const float4* slot_xyz;  // per slot: (x, y, z) voxel coordinates as exact floats, w = voxel index
+  int cpad;             // FP32 source row length in floats: nb*cstride rounded up to a multiple of 4
+  int cstride;          // FP32 row stride of one right-hand side: Cfull rounded up to even
+  int* err;             // set to 1 when a bounded wait runs out (kernel result invalid)
 };
 
 struct EpiArgs {
@@ -35,7 +40,9 @@ struct EpiArgs {
   int flag_scat;
   double scat[RTE_MAX_L + 1];  // per-l scatter factor (times mu_s of the voxel)
   double* Wout;         // FP64 result (may alias nothing else)
-  float* Woutf;         // FP32 copy (may be null)
+  float* Woutf;         // FP32 copy in slot order, rows of cpad floats (may be null)
+  const int* islot;     // voxel -> slot
+  int cpad, cstride;
   double* sum;          // running sum (null = do not accumulate)
   double* red;          // [0] ||Wout||^2 [1] ||sum||^2 [2] stop-layer sum of Wout [3] of sum
 };
@@ -53,7 +60,7 @@ struct SelfArgs {
 };
 
 struct ImgArgs {
-  int nx, ny, nz, Cfull, L;
+  int nx, ny, nz, Cfull, L, vstride;
   const double* out;
   double wt[RTE_MAX_L + 1];  // transmission weights per l (m = 0 coefficient)
   double wr[RTE_MAX_L + 1];  // reflection weights per l
@@ -74,13 +81,68 @@ struct SrcArgs {
   int nx, ny, nz, Cfull, L, kind, ncols;
   int cols[RTE_MAX_SRC_COLS];
   double scale, mag, g, dz, dV, z_min;
+  int vstride;   // elements between consecutive voxels of W (Cfull for one right-hand side)
   const double* mut;
   const double* mus;
-  double* W;     // N x Cfull, zeroed by the caller
+  double* W;     // N x vstride, zeroed by the caller
   double* ball;  // nx*ny ballistic transmission, zeroed by the caller
 };
 
+// detector faces and the adjoint gradient
+struct FaceArgs {
+  int nx, ny, nz, Cfull, vstride;
+  const double* out;   // real basis [N][vstride]
+  const double* h;     // [6][Cfull] exitant-flux weights of each face (area and cm included)
+  const double* ball;  // nx*ny ballistic transmission of the z = nZ-1 face (may be null)
+  double* J;           // fluxes of all face pixels (z-, z+, y-, y+, x-, x+ concatenated)
+  const double* rho;   // adjoint seed: dL/dJ per face pixel
+  double* e;           // adjoint seed field [N][Cfull]
+};
+
+struct BpArgs {
+  int N, nx, ny, nz, Cfull;
+  double dx, dy, dz, prop_thresh, kscale;
+  const int* perm;
+  const int* islot;
+  const double* mut;
+  const float* mutf;
+  const double* y;     // destination-side field [N][Cfull] (voxel order)
+  const double* S;     // source-side field [N][Cfull] (voxel order)
+  const float* Kmat;   // stored pair kernel (null: recompute the path integral)
+  size_t Kld;
+  double* g;           // gradient w.r.t. mu_t, accumulated [N]
+  int chunk, nsplit;
+  int use_smem;        // per-CTA private accumulator of N entries in shared memory
+};
+
+struct GradLocalArgs {
+  int N, Cfull, Cact;
+  const double* y;      // e + D lambda
+  const double* lam;    // adjoint field
+  const double* S;      // forward running sum
+  const double* out;    // A S
+  const double* mus;
+  const double* mut;
+  const int* idx;       // voxel -> distinct mu_t (null: power series)
+  const double* dlut;   // d Dself / d mu_t per distinct value [nd][C][C]
+  const double* mom;
+  int K;
+  double scale;         // dV / cm
+  int air_no_self;
+  double scat[RTE_MAX_L + 1];
+  double* gt;           // += self-term part of dL/dmu_t
+  double* gs;           // += scatter part of dL/dmu_s
+};
+
 extern "C++" {
+cudaError_t rte_launch_face_flux(const FaceArgs& a, cudaStream_t st);
+cudaError_t rte_launch_adjoint_seed(const FaceArgs& a, cudaStream_t st);
+cudaError_t rte_launch_parity(double* x, int N, int L, int vstride, cudaStream_t st);
+cudaError_t rte_launch_axpy(double* y, const double* x, double alpha, size_t n, cudaStream_t st);
+cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, const double* mus, const double* scat,
+                               int N, int L, int Cfull, cudaStream_t st);
+cudaError_t rte_launch_backproject(const BpArgs& a, int LA, int fp64, cudaStream_t st);
+cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st);
 // message returned by rte_last_error(NULL) on this thread
 __attribute__((visibility("hidden"))) void rte_set_global_error(const char* msg);
 cudaError_t rte_launch_source(const SrcArgs& a, cudaStream_t st);
@@ -90,15 +152,18 @@ cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t s
 cudaError_t rte_upload_sh_tables(const ShTables& t);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
-cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int* blocks_per_sm);
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm);
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);
 cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st);
 cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st);
 cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
                                cudaStream_t st);
 cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L,
-                               cudaStream_t st);
+                               cudaStream_t st, int ustride = 0);
 cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
                                   double* red, cudaStream_t st);
 cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
+// FP64 [N][vstride] (voxel order) -> FP32 [slot][cpad] (slot order)
+cudaError_t rte_launch_to_f32_slots(const double* a, float* b, const int* islot, int N, int vstride, int cpad,
+                                    int Cfull, int cstride, cudaStream_t st);
 }

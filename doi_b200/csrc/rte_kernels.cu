@@ -27,6 +27,26 @@
 
 #include "rte_internal.h"
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two FP32 FMAs per instruction.
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+struct ScatTab {
+  double v[RTE_MAX_L + 1];
+};
+
 __constant__ ShTables c_sh;
 __constant__ float c_shAf[64];
 __constant__ float c_shBf[64];
@@ -56,22 +76,60 @@ template <> __device__ __forceinline__ float shA<float>(int i) { return c_shAf[i
 template <> __device__ __forceinline__ float shB<float>(int i) { return c_shBf[i]; }
 template <> __device__ __forceinline__ float shQ0<float>(int i) { return c_shQ0f[i]; }
 
+// Compile-time copies of the SH recurrence coefficients (the same formulas as the host tables in
+// rte_host.cpp), so the unrolled FP32 recurrence multiplies by immediates and the l = m+1 steps
+// carry no B term.
+struct ShConstTab {
+  double A[64], B[64], Q0[RTE_MAX_L + 1];
+};
+constexpr double c_sqrt(double x) {
+  double r = x > 1.0 ? x : 1.0;
+  for (int i = 0; i < 80; ++i) r = 0.5 * (r + x / r);
+  return r;
+}
+constexpr double c_knorm(int l, int m) {
+  double f = 1.0;
+  for (int i = l - m + 1; i <= l + m; ++i) f *= (double)i;
+  const double k = c_sqrt((2.0 * l + 1.0) / (4.0 * 3.14159265358979323846) / f);
+  return m > 0 ? k * c_sqrt(2.0) : k;
+}
+constexpr ShConstTab make_sh_const() {
+  ShConstTab t{};
+  for (int m = 0; m <= RTE_MAX_L; ++m) {
+    double dfact = 1.0;
+    for (int i = 2 * m - 1; i > 0; i -= 2) dfact *= (double)i;
+    t.Q0[m] = c_knorm(m, m) * ((m & 1) ? -1.0 : 1.0) * dfact;
+    for (int l = m + 1; l <= RTE_MAX_L; ++l) {
+      const int id = l * (l + 1) / 2 + m;
+      t.A[id] = c_knorm(l, m) * (2.0 * l - 1.0) / ((double)(l - m) * c_knorm(l - 1, m));
+      t.B[id] = (l - 2 >= m) ? c_knorm(l, m) * (double)(l + m - 1) / ((double)(l - m) * c_knorm(l - 2, m)) : 0.0;
+    }
+  }
+  return t;
+}
+__device__ constexpr ShConstTab kShConst = make_sh_const();
+
 // Real orthonormal SH R_lm at the unit direction (x, y, z), index l*l + l + m.
 // R_l0 = q_l^0(z), R_l,+m = q_l^m(z) Re((x+iy)^m), R_l,-m = q_l^m(z) Im((x+iy)^m), with the
 // normalised associated-Legendre polynomials q (Condon-Shortley phase included) from the
-// upward recurrence in l.  No trigonometric calls.
+// upward recurrence in l.  No trigonometric calls.  FP64 reads the uploaded tables; FP32 uses
+// the compile-time copies.
 template <int L, typename T>
 __device__ __forceinline__ void sh_eval(T x, T y, T z, T* R) {
+  constexpr bool F32 = std::is_same<T, float>::value;
   T cmv = T(1), smv = T(0);
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
-    if (m > 0) {
+    if (m == 1) {
+      cmv = x;
+      smv = y;
+    } else if (m > 1) {
       T c2 = cmv * x - smv * y;
       T s2 = cmv * y + smv * x;
       cmv = c2;
       smv = s2;
     }
-    T q2 = T(0), q1 = shQ0<T>(m);
+    T q2 = T(0), q1 = F32 ? (T)kShConst.Q0[m] : shQ0<T>(m);
     if (m == 0) {
       R[0] = q1;
     } else {
@@ -81,7 +139,14 @@ __device__ __forceinline__ void sh_eval(T x, T y, T z, T* R) {
 #pragma unroll
     for (int l = m + 1; l <= L; ++l) {
       const int id = l * (l + 1) / 2 + m;
-      T q = shA<T>(id) * z * q1 - shB<T>(id) * q2;
+      const T A = F32 ? (T)kShConst.A[id] : shA<T>(id);
+      T q;
+      if (l == m + 1) {
+        q = (A * z) * q1;
+      } else {
+        const T B = F32 ? (T)kShConst.B[id] : shB<T>(id);
+        q = (A * z) * q1 - B * q2;
+      }
       q2 = q1;
       q1 = q;
       if (m == 0) {
@@ -227,114 +292,192 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
 // Mixed precision: path integrals, SH and projections in FP32 (SH in FP64 for l >= 7).  NB right-
 // hand sides that share the medium are propagated together: the direction, its SH and the pair
 // kernel are computed once per pair and used NB times.  Sources are visited in slot order (the
-// same spatially compact order as the destinations); each 64-source tile (coefficients of all NB
-// right-hand sides and the exact integer coordinates) is staged in shared memory.  Sums: FP32 over
-// one tile in registers, FP32 across tiles in shared memory, FP64 across the split-K chunks in
-// the epilogue.  STORED reads the precomputed pair kernel K[source slot][destination slot] (FP32);
-// otherwise the path integral is walked in FP32.
+// same spatially compact order as the destinations).  The FP32 source coefficients are kept in
+// slot order with rows of CP floats, so a 64-source tile (and its coordinates) is one contiguous
+// block: one thread issues two TMA bulk copies (cp.async.bulk, completion on an mbarrier) per tile
+// into a double buffer, overlapping the next tile's copy with this tile's arithmetic.  Sums: FP32
+// over one tile in registers (projections split over four accumulators), FP32 across tiles in
+// shared memory, FP64 across the split-K chunks in the epilogue.  STORED reads the precomputed
+// pair kernel K[source slot][destination slot] (FP32); otherwise the path is walked in FP32.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// bounded wait on an mbarrier phase; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// shared memory: [2][TS] float4 | [2][TS][cpad] float | [NB*C][T] float | 2 mbarriers
+struct MixedLayout {
+  size_t off_w, off_acc, off_bar, bytes;
+  __host__ __device__ MixedLayout(int cpad, int nbc) {
+    off_w = sizeof(float4) * 2 * RTE_PAIR_TS;
+    off_acc = off_w + sizeof(float) * 2 * RTE_PAIR_TS * (size_t)cpad;
+    off_bar = (off_acc + sizeof(float) * (size_t)nbc * RTE_PAIR_THREADS + 15) / 16 * 16;
+    bytes = off_bar + 2 * sizeof(uint64_t);
+  }
+};
+
 template <int LA, bool TABLE, bool STORED, int NB>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
-  constexpr int C = (LA + 1) * (LA + 1);
-  constexpr int TS = RTE_PAIR_TS;
-  constexpr int T = RTE_PAIR_THREADS;
+  constexpr int C = (LA + 1) * (LA + 1), TS = RTE_PAIR_TS, T = RTE_PAIR_THREADS;
+  const int CP = a.cpad;  // FP32 source row: nb * Cfull floats, padded to a multiple of 4
+  const MixedLayout Sh(CP, NB * C);
   typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* sP = reinterpret_cast<float4*>(smem_raw);            // [TS] source (x, y, z) as exact floats
-  float* sW = reinterpret_cast<float*>(sP + TS);                // [TS][NB][C]
-  float* sAcc = sW + TS * NB * C;                               // [NB*C][T]
+  float4* sP = reinterpret_cast<float4*>(smem_raw);
+  float* sW = reinterpret_cast<float*>(smem_raw + Sh.off_w);
+  float* sAcc = reinterpret_cast<float*>(smem_raw + Sh.off_acc);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Sh.off_bar);
   const int tid = threadIdx.x;
   const int slot = blockIdx.x * T + tid;
   const bool act = slot < a.N;
-  const int r = act ? a.perm[slot] : 0;
+  const float4 me = a.slot_xyz[act ? slot : 0];
+  const int r = __float_as_int(me.w);
   const int plane = a.nx * a.ny;
-  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
-  const float fk = (float)k, fj = (float)j, fi = (float)i;
+  const int i = (int)me.z, j = (int)me.y, k = (int)me.x;
   const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
   const float kscalef = (float)a.kscale;
   const float thr = (float)a.prop_thresh;
-  const int vstride = NB * a.Cfull;
 #pragma unroll
   for (int q = 0; q < NB * C; ++q) sAcc[q * T + tid] = 0.f;
-  float acc[NB][C];
   const int sb = blockIdx.y * a.chunk;
   const int se = min(a.N, sb + a.chunk);
-  for (int s0 = sb; s0 < se; s0 += TS) {
+  const int ntile = (se - sb + TS - 1) / TS;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int t) {  // tile t -> buffer t & 1 (one thread)
+    const int s0 = sb + t * TS;
     const int ns = min(TS, se - s0);
-    __syncthreads();
-    for (int q = tid; q < ns; q += T) {
-      const int v = a.perm[s0 + q];
-      sP[q] = make_float4((float)(v % a.nx), (float)((v / a.nx) % a.ny), (float)(v / plane), 0.f);
+    const int b = t & 1;
+    const uint32_t bw = (uint32_t)(ns * CP * sizeof(float)), bp = (uint32_t)(ns * sizeof(float4));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[b], bw + bp);
+    bulk_g2s(sW + b * TS * CP, a.Winf + (size_t)s0 * CP, bw, &bar[b]);
+    bulk_g2s(sP + b * TS, a.slot_xyz + s0, bp, &bar[b]);
+  };
+  if (tid == 0 && ntile > 0) issue(0);
+  constexpr int C2 = (C + 1) / 2;  // coefficient pairs (packed f32x2 arithmetic)
+  const int CS = a.cstride;        // FP32 row stride of one right-hand side (even)
+  f2_t acc[NB][C2];
+  for (int t = 0; t < ntile; ++t) {
+    if (tid == 0 && t + 1 < ntile) issue(t + 1);
+    const bool ok = mbar_wait(&bar[t & 1], (uint32_t)((t >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(a.err, 1);
+      return;
     }
-    for (int q = tid; q < ns * NB * C; q += T) {
-      const int sv = q / (NB * C), e = q - sv * (NB * C);
-      const int b = e / C, c = e - b * C;
-      sW[q] = a.Winf[(size_t)a.perm[s0 + sv] * vstride + b * a.Cfull + c];
-    }
-    __syncthreads();
-    if (!act) continue;
+    const int s0 = sb + t * TS;
+    const int ns = min(TS, se - s0);
+    const float4* P = sP + (t & 1) * TS;
+    const float* Wt = sW + (t & 1) * TS * CP;
+    if (act) {
 #pragma unroll
-    for (int b = 0; b < NB; ++b)
+      for (int b = 0; b < NB; ++b)
 #pragma unroll
-      for (int c = 0; c < C; ++c) acc[b][c] = 0.f;
-    const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.Kld + slot : nullptr;
-    float k0 = 0.f, k1 = 0.f;
-    if (STORED) {
-      k0 = __ldg(Kcol);
-      if (ns > 1) k1 = __ldg(Kcol + a.Kld);
-    }
-    for (int sv = 0; sv < ns; ++sv) {
-      float kk = 0.f;
+        for (int c = 0; c < C2; ++c) acc[b][c] = 0ull;
+      const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.Kld + slot : nullptr;
+      float k0 = 0.f, k1 = 0.f;
       if (STORED) {
-        kk = k0;
-        k0 = k1;
-        if (sv + 2 < ns) k1 = __ldg(Kcol + (size_t)(sv + 2) * a.Kld);
+        k0 = __ldg(Kcol);
+        if (ns > 1) k1 = __ldg(Kcol + a.Kld);
       }
-      const float4 q = sP[sv];
-      const float ddx = (fk - q.x) * dxf, ddy = (fj - q.y) * dyf, ddz = (fi - q.z) * dzf;
-      const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-      bool live;
-      float dist = 0.f;
-      if (STORED) {
-        live = kk != 0.f;
-      } else {
-        dist = sqrtf(d2);
-        live = d2 > 0.f && dist < thr;
-      }
-      if (live) {
-        ShT R[C];
-        if (TABLE) {
-          const double ex = (double)(k - (int)q.x) * a.dx, ey = (double)(j - (int)q.y) * a.dy,
-                       ez = (double)(i - (int)q.z) * a.dz;
-          double ux, uy, uz;
-          table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
-          sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
+      for (int sv = 0; sv < ns; ++sv) {
+        float kk = 0.f;
+        if (STORED) {
+          kk = k0;
+          k0 = k1;
+          if (sv + 2 < ns) k1 = __ldg(Kcol + (size_t)(sv + 2) * a.Kld);
+        }
+        const float4 q = P[sv];
+        const float ddx = (me.x - q.x) * dxf, ddy = (me.y - q.y) * dyf, ddz = (me.z - q.z) * dzf;
+        const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+        bool live;
+        float dist = 0.f;
+        if (STORED) {
+          live = kk != 0.f;
         } else {
-          const float inv = rsqrtf(d2);
-          sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+          dist = sqrtf(d2);
+          live = d2 > 0.f && dist < thr;
         }
-        if (!STORED) {
-          int Q;
-          const float ps = path_sum<float, float>(i, j, k, (int)q.z, (int)q.y, (int)q.x, a.mutf, a.nx, plane, Q);
-          kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
-        }
-        const float* w = sW + sv * (NB * C);
+        if (live) {
+          ShT R[C];
+          if (TABLE) {
+            const double ex = (double)(k - (int)q.x) * a.dx, ey = (double)(j - (int)q.y) * a.dy,
+                         ez = (double)(i - (int)q.z) * a.dz;
+            double ux, uy, uz;
+            table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
+            sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
+          } else {
+            const float inv = rsqrtf(d2);
+            sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+          }
+          if (!STORED) {
+            int Q;
+            const float ps = path_sum<float, float>(i, j, k, (int)q.z, (int)q.y, (int)q.x, a.mutf, a.nx, plane, Q);
+            kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
+          }
+          f2_t R2[C2];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-          float S = 0.f;
+          for (int c = 0; c < C2; ++c) R2[c] = f2_pack((float)R[2 * c], 2 * c + 1 < C ? (float)R[2 * c + 1] : 0.f);
 #pragma unroll
-          for (int c = 0; c < C; ++c) S = fmaf((float)R[c], w[b * C + c], S);
-          const float t = kk * S;
+          for (int b = 0; b < NB; ++b) {
+            const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+            f2_t Sa = 0ull, Sb = 0ull;
 #pragma unroll
-          for (int c = 0; c < C; ++c) acc[b][c] = fmaf((float)R[c], t, acc[b][c]);
+            for (int c = 0; c < C2; c += 2) {
+              Sa = f2_fma(R2[c], w[c], Sa);
+              if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+            }
+            float a0, a1, b0, b1;
+            f2_unpack(Sa, a0, a1);
+            f2_unpack(Sb, b0, b1);
+            const float tb = kk * ((a0 + a1) + (b0 + b1));
+            const f2_t T2 = f2_pack(tb, tb);
+#pragma unroll
+            for (int c = 0; c < C2; ++c) acc[b][c] = f2_fma(R2[c], T2, acc[b][c]);
+          }
         }
       }
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int c = 0; c < C2; ++c) {
+          float lo, hi;
+          f2_unpack(acc[b][c], lo, hi);
+          sAcc[(b * C + 2 * c) * T + tid] += lo;
+          if (2 * c + 1 < C) sAcc[(b * C + 2 * c + 1) * T + tid] += hi;
+        }
     }
-#pragma unroll
-    for (int b = 0; b < NB; ++b)
-#pragma unroll
-      for (int c = 0; c < C; ++c) sAcc[(b * C + c) * T + tid] += acc[b][c];
+    __syncthreads();  // buffer t & 1 is free for tile t + 2
   }
   if (act) {
+    const int vstride = NB * a.Cfull;
     double* o = a.part + ((size_t)blockIdx.y * a.N + r) * vstride;
 #pragma unroll
     for (int b = 0; b < NB; ++b)
@@ -440,7 +583,7 @@ __global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
       for (int c = 0; c < a.Cfull; ++c) {
         const double x = c < C ? v[c] : 0.0;
         a.Wout[base + c] = x;
-        if (a.Woutf) a.Woutf[base + c] = (float)x;
+        if (a.Woutf) a.Woutf[(size_t)a.islot[r] * a.cpad + (size_t)b * a.cstride + c] = (float)x;
         w2 += x * x;
         double sv = 0.0;
         if (a.sum) {
@@ -519,11 +662,11 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
   double t = 0.0, f = 0.0, ti = 0.0, fi = 0.0;
   for (int l = 0; l <= a.L; ++l) {
     const int c = l * l + l;
-    t += a.wt[l] * a.out[rt * a.Cfull + c];
-    f += a.wr[l] * a.out[rr * a.Cfull + c];
+    t += a.wt[l] * a.out[rt * a.vstride + c];
+    f += a.wr[l] * a.out[rr * a.vstride + c];
     if (out_im) {
-      ti += a.wt[l] * out_im[rt * a.Cfull + c];
-      fi += a.wr[l] * out_im[rr * a.Cfull + c];
+      ti += a.wt[l] * out_im[rt * a.vstride + c];
+      fi += a.wr[l] * out_im[rr * a.vstride + c];
     }
   }
   if (a.ball) t += a.ball[p];
@@ -561,7 +704,7 @@ __global__ void k_source(SrcArgs a) {
     att *= exp(-mt * a.dz);
     double gl = 1.0;
     for (int l = 0; l <= a.L; ++l) {
-      a.W[r * a.Cfull + l * l + l] = a.scale * gl * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / a.dV;
+      a.W[r * a.vstride + l * l + l] = a.scale * gl * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / a.dV;
       gl *= a.g;
     }
   }
@@ -590,7 +733,27 @@ __global__ void k_medium(const double* mua, const double* mus, double* mut, doub
 }
 
 // FMA throughput probe (roofline denominator for the CUDA-core-bound kernels): 8 independent FMA
-// chains per thread; the result is written so the work cannot be removed.
+// chains per thread; the result is written so the work cannot be removed.  k_fma2_peak does the
+// same with packed f32x2 FMAs (two FP32 FMAs per instruction).
+__global__ void k_fma2_peak(int iters, float* sink) {
+  f2_t a[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) a[q] = f2_pack((float)(threadIdx.x + q) * 1e-3f, (float)(threadIdx.x + 2 * q) * 1e-3f);
+  const f2_t b = f2_pack(0.999999f, 0.999998f), c = f2_pack(1e-7f, 2e-7f);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = f2_fma(a[q], b, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    float lo, hi;
+    f2_unpack(a[q], lo, hi);
+    s += lo + hi;
+  }
+  if (s == -1.2345f) sink[blockIdx.x] = s;
+}
+
 template <typename T>
 __global__ void k_fma_peak(int iters, float* sink) {
   T a[8];
@@ -605,6 +768,233 @@ __global__ void k_fma_peak(int iters, float* sink) {
 #pragma unroll
   for (int q = 0; q < 8; ++q) s += a[q];
   if (s == (T)-1.2345) sink[blockIdx.x] = (float)s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Detectors and the adjoint gradient.
+// Face pixels: z-(ny*nx) z+(ny*nx) y-(nz*nx) y+(nz*nx) x-(nz*ny) x+(nz*ny), row-major.
+__device__ __forceinline__ void face_pixel(int q, int nx, int ny, int nz, int& f, int& p, int& r) {
+  const int a0 = nx * ny, a1 = nz * nx, a2 = nz * ny;
+  const int off[6] = {0, a0, 2 * a0, 2 * a0 + a1, 2 * a0 + 2 * a1, 2 * a0 + 2 * a1 + a2};
+  f = 5;
+  for (int t = 1; t < 6; ++t)
+    if (q < off[t]) {
+      f = t - 1;
+      break;
+    }
+  p = q - off[f];
+  if (f < 2) {  // p = j*nx + k
+    const int i = f == 0 ? 0 : nz - 1;
+    r = i * nx * ny + p;
+  } else if (f < 4) {  // p = i*nx + k
+    const int i = p / nx, k = p % nx, j = f == 2 ? 0 : ny - 1;
+    r = (i * ny + j) * nx + k;
+  } else {  // p = i*ny + j
+    const int i = p / ny, j = p % ny, k = f == 4 ? 0 : nx - 1;
+    r = (i * ny + j) * nx + k;
+  }
+}
+
+__global__ void k_face_flux(FaceArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
+  if (q >= total) return;
+  int f, p, r;
+  face_pixel(q, a.nx, a.ny, a.nz, f, p, r);
+  const double* h = a.h + f * a.Cfull;
+  const double* o = a.out + (size_t)r * a.vstride;
+  double J = 0.0;
+  for (int c = 0; c < a.Cfull; ++c) J = fma(h[c], o[c], J);
+  if (f == 1 && a.ball) J += a.ball[p];
+  a.J[q] = J;
+}
+
+// e[r][c] += rho(pixel) h_f[c] for every face pixel (edge voxels belong to several faces)
+__global__ void k_adjoint_seed(FaceArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
+  if (q >= total) return;
+  const double rho = a.rho[q];
+  if (rho == 0.0) return;
+  int f, p, r;
+  face_pixel(q, a.nx, a.ny, a.nz, f, p, r);
+  for (int c = 0; c < a.Cfull; ++c) atomicAdd(a.e + (size_t)r * a.Cfull + c, rho * a.h[f * a.Cfull + c]);
+}
+
+// x *= (-1)^l: the parity of the real SH, R(-w) = (-1)^l R(w); the transpose of the pair operator
+// is P A P.
+__global__ void k_parity(double* x, int N, int L, int vstride) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = (L + 1) * (L + 1);
+  if (t >= (long long)N * C) return;
+  const int r = (int)(t / C), c = (int)(t % C);
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  if (l & 1) x[(size_t)r * vstride + c] = -x[(size_t)r * vstride + c];
+}
+
+__global__ void k_axpy(double* y, const double* x, double alpha, size_t n) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) y[t] = fma(alpha, x[t], y[t]);
+}
+
+// y = e + D lambda, D = scat_l mu_s(r)
+__global__ void k_y_field(double* y, const double* e, const double* lam, const double* mus, ScatTab sc, int N, int L,
+                          int Cfull) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * Cfull) return;
+  const int r = (int)(t / Cfull), c = (int)(t % Cfull);
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  y[t] = e[t] + (l <= L ? sc.v[l] : 0.0) * mus[r] * lam[t];
+}
+
+// Segments of the centre-to-centre path of path_sum, each length handed to `add(v, len * Q / dist)`.
+template <typename F>
+__device__ __forceinline__ void path_walk(int i, int j, int k, int ip, int jp, int kp, int nx, int plane, int& Q,
+                                          F add) {
+  const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
+  const int mz = max(Dz, 1), my = max(Dy, 1), mx = max(Dx, 1);
+  Q = 2 * mx * my * mz;
+  const int BIG = 0x3fffffff;
+  const int incz = 2 * mx * my, incy = 2 * mx * mz, incx = 2 * my * mz;
+  int Az = Dz ? mx * my : BIG, Ay = Dy ? mx * mz : BIG, Ax = Dx ? my * mz : BIG;
+  const int stz = ip > i ? plane : -plane, sty = jp > j ? nx : -nx, stx = kp > k ? 1 : -1;
+  int v = i * plane + j * nx + k;
+  int prev = 0;
+  const int steps = Dx + Dy + Dz;
+  for (int s = 0; s < steps; ++s) {
+    const int m = min(Az, min(Ay, Ax));
+    if (m > prev) add(v, m - prev);
+    prev = m;
+    const bool bz = Az == m;
+    const bool by = !bz && (Ay == m);
+    const bool bx = !bz && !by;
+    v += bz ? stz : (by ? sty : stx);
+    Az += bz ? incz : 0;
+    Ay += by ? incy : 0;
+    Ax += bx ? incx : 0;
+  }
+  add(v, Q - prev);
+}
+
+// Back-projection for the gradient w.r.t. mu_t:
+//   g(v) -= sum_{r != r'} len_rr'(v) k_rr' (y_r . R(w)) (R(w) . S_r'),   w = (r - r')/|r - r'|,
+// the derivative of y^T A S through exp(-tau).  One thread per destination voxel r (slot order),
+// sources of one split-K chunk in voxel order; k from the stored pair kernel (FP32) or recomputed
+// (FP64); each CTA accumulates into a private copy of g in shared memory when it fits, then adds
+// it to the global FP64 gradient.
+template <int LA, typename T>
+__global__ void __launch_bounds__(RTE_BP_THREADS) k_backproject(BpArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* gsh = reinterpret_cast<T*>(smem_raw);
+  const int tid = threadIdx.x;
+  if (a.use_smem) {
+    for (int v = tid; v < a.N; v += RTE_BP_THREADS) gsh[v] = T(0);
+    __syncthreads();
+  }
+  const int slot = blockIdx.x * RTE_BP_THREADS + tid;
+  const bool act = slot < a.N;
+  const int r = act ? a.perm[slot] : 0;
+  const int plane = a.nx * a.ny;
+  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  T y[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) y[c] = act ? (T)a.y[(size_t)r * a.Cfull + c] : T(0);
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  if (act) {
+    int kp = sb % a.nx, jp = (sb / a.nx) % a.ny, ip = sb / plane;
+    for (int rp = sb; rp < se; ++rp) {
+      if (rp != r) {
+        const T ddx = (T)(k - kp) * (T)a.dx, ddy = (T)(j - jp) * (T)a.dy, ddz = (T)(i - ip) * (T)a.dz;
+        const T d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        const T dist = sqrt(d2);
+        if (dist < (T)a.prop_thresh) {
+          T kk;
+          if (a.Kmat) {
+            kk = (T)__ldg(a.Kmat + (size_t)a.islot[rp] * a.Kld + slot);
+          } else {
+            int Q0;
+            const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q0);
+            kk = exp(-ps * dist / (T)Q0) * (T)a.kscale / d2;
+          }
+          const T inv = T(1) / dist;
+          T R[C];
+          sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
+          T yr = 0, sr = 0;
+          const double* Sp = a.S + (size_t)rp * a.Cfull;
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            yr = fma(y[c], R[c], yr);
+            sr = fma(R[c], (T)__ldg(Sp + c), sr);
+          }
+          const T q = kk * yr * sr;
+          if (q != T(0)) {
+            int Q = 1;
+            // lengths arrive scaled by Q/dist; coef restores them
+            const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
+            const T coef = -q * dist / (T)(2 * max(Dx, 1) * max(Dy, 1) * max(Dz, 1));
+            if (a.use_smem)
+              path_walk(i, j, k, ip, jp, kp, a.nx, plane, Q, [&](int v, int len) { atomicAdd(gsh + v, coef * (T)len); });
+            else
+              path_walk(i, j, k, ip, jp, kp, a.nx, plane, Q,
+                        [&](int v, int len) { atomicAdd(a.g + v, (double)(coef * (T)len)); });
+          }
+        }
+      }
+      if (++kp == a.nx) {
+        kp = 0;
+        if (++jp == a.ny) {
+          jp = 0;
+          ++ip;
+        }
+      }
+    }
+  }
+  if (a.use_smem) {
+    __syncthreads();
+    for (int v = tid; v < a.N; v += RTE_BP_THREADS) {
+      const T x = gsh[v];
+      if (x != T(0)) atomicAdd(a.g + v, (double)x);
+    }
+  }
+}
+
+// Per-voxel parts of the gradient: the scatter D (d/dmu_s: lambda . scat_l . (A S)) and the
+// self-voxel term (d/dmu_t: (dV/cm) y . dDself/dmu S).
+__global__ void k_grad_local(GradLocalArgs a) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.N) return;
+  const size_t b = (size_t)r * a.Cfull;
+  double gs = 0.0;
+  for (int c = 0; c < a.Cact; ++c) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= c) ++l;
+    gs = fma(a.lam[b + c] * a.scat[l], a.out[b + c], gs);
+  }
+  a.gs[r] += gs;
+  const double mu = a.mut[r];
+  if (a.air_no_self && mu == 0.0) return;
+  double gt = 0.0;
+  for (int c = 0; c < a.Cact; ++c) {
+    double u = 0.0;
+    if (a.idx) {
+      const double* D = a.dlut + ((size_t)a.idx[r] * a.Cfull + c) * a.Cfull;
+      for (int cp = 0; cp < a.Cact; ++cp) u = fma(D[cp], a.S[b + cp], u);
+    } else {
+      // d/dmu sum_k mu^k M_k = sum_{k>=1} k mu^(k-1) M_k
+      for (int kk = a.K - 1; kk >= 1; --kk) {
+        const double* M = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
+        double t = 0.0;
+        for (int cp = 0; cp < a.Cact; ++cp) t = fma(M[cp], a.S[b + cp], t);
+        u = fma(mu, u, (double)kk * t);
+      }
+    }
+    gt = fma(a.y[b + c], u, gt);
+  }
+  a.gt[r] += a.scale * gt;
 }
 
 // Complex reference basis <-> real basis.  w = w1 + i w2 with w1, w2 the coefficient sets of
@@ -647,10 +1037,14 @@ __global__ void k_to_real(const double* __restrict__ w, double* u1, double* u2, 
   }
 }
 
-__global__ void k_to_cplx(const double* __restrict__ u1, const double* __restrict__ u2, double* w, int N, int L) {
+__global__ void k_to_cplx(const double* __restrict__ u1, const double* __restrict__ u2, double* w, int N, int L,
+                          int ustride) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= N) return;
   const int C = (L + 1) * (L + 1);
+  // u1/u2 rows are ustride apart (several right-hand sides interleaved); w rows are C apart
+  u1 += (size_t)r * ustride - (size_t)r * C;
+  if (u2) u2 += (size_t)r * ustride - (size_t)r * C;
   const double is2 = 0.70710678118654752;
   for (int l = 0; l <= L; ++l) {
     const int c0 = l * l + l;
@@ -706,6 +1100,15 @@ __global__ void k_layer_sums(const double* W, const double* S, int N, int nx, in
   }
 }
 
+__global__ void k_to_f32_slots(const double* a, float* b, const int* islot, int N, int vstride, int cpad,
+                               int Cfull, int cstride) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * vstride) return;
+  const int r = (int)(t / vstride), e = (int)(t % vstride);
+  const int rhs = e / Cfull, c = e - rhs * Cfull;
+  b[(size_t)islot[r] * cpad + (size_t)rhs * cstride + c] = (float)a[t];
+}
+
 __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
@@ -714,14 +1117,8 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // ---------------------------------------------------------------------------------------------
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB>
-static size_t mixed_smem() {
-  constexpr int C = (LA + 1) * (LA + 1);
-  return sizeof(float4) * RTE_PAIR_TS + sizeof(float) * (RTE_PAIR_TS * NB * C + NB * C * RTE_PAIR_THREADS);
-}
-
-template <int LA, bool TABLE, bool STORED, int NB>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
-  const size_t smem = mixed_smem<LA, TABLE, STORED, NB>();
+  const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1)).bytes;
   void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -775,9 +1172,10 @@ cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table,
   return pair_dispatch(a, LA, precision, table, stored, a.nb > 0 ? a.nb : 1, st, nullptr);
 }
 
-cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int* blocks_per_sm) {
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm) {
   PairArgs dummy;
   memset(&dummy, 0, sizeof dummy);
+  dummy.cpad = cpad;
   return pair_dispatch(dummy, LA, precision, table, stored, nb, nullptr, blocks_per_sm);
 }
 
@@ -821,8 +1219,10 @@ cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N
   return cudaGetLastError();
 }
 
-cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L, cudaStream_t st) {
-  k_to_cplx<<<(N + 127) / 128, 128, 0, st>>>(u1, u2, cplx, N, L);
+cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L, cudaStream_t st,
+                               int ustride) {
+  const int C = (L + 1) * (L + 1);
+  k_to_cplx<<<(N + 127) / 128, 128, 0, st>>>(u1, u2, cplx, N, L, ustride > 0 ? ustride : C);
   return cudaGetLastError();
 }
 
@@ -845,14 +1245,89 @@ cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut,
 }
 
 cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks) {
-  if (fp64)
+  if (fp64 == 2)
+    k_fma2_peak<<<blocks, 256, 0, st>>>(iters, sink);
+  else if (fp64)
     k_fma_peak<double><<<blocks, 256, 0, st>>>(iters, sink);
   else
     k_fma_peak<float><<<blocks, 256, 0, st>>>(iters, sink);
   return cudaGetLastError();
 }
 
+cudaError_t rte_launch_to_f32_slots(const double* a, float* b, const int* islot, int N, int vstride, int cpad,
+                                    int Cfull, int cstride, cudaStream_t st) {
+  const long long n = (long long)N * vstride;
+  k_to_f32_slots<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, islot, N, vstride, cpad, Cfull, cstride);
+  return cudaGetLastError();
+}
+
 cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st) {
   k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_face_flux(const FaceArgs& a, cudaStream_t st) {
+  const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
+  k_face_flux<<<(total + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_adjoint_seed(const FaceArgs& a, cudaStream_t st) {
+  const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
+  k_adjoint_seed<<<(total + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_parity(double* x, int N, int L, int vstride, cudaStream_t st) {
+  const long long n = (long long)N * (L + 1) * (L + 1);
+  k_parity<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, N, L, vstride);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_axpy(double* y, const double* x, double alpha, size_t n, cudaStream_t st) {
+  k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(y, x, alpha, n);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, const double* mus, const double* scat,
+                               int N, int L, int Cfull, cudaStream_t st) {
+  ScatTab sc;
+  for (int l = 0; l <= RTE_MAX_L; ++l) sc.v[l] = scat[l];
+  const long long n = (long long)N * Cfull;
+  k_y_field<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(y, e, lam, mus, sc, N, L, Cfull);
+  return cudaGetLastError();
+}
+
+template <int LA, typename T>
+static cudaError_t launch_bp(const BpArgs& a, cudaStream_t st) {
+  const size_t smem = a.use_smem ? (size_t)a.N * sizeof(T) : 0;
+  cudaError_t e = cudaFuncSetAttribute(k_backproject<LA, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.N + RTE_BP_THREADS - 1) / RTE_BP_THREADS, a.nsplit);
+  k_backproject<LA, T><<<grid, RTE_BP_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int LA>
+static cudaError_t launch_bp_LA(const BpArgs& a, int fp64, cudaStream_t st) {
+  return fp64 ? launch_bp<LA, double>(a, st) : launch_bp<LA, float>(a, st);
+}
+
+cudaError_t rte_launch_backproject(const BpArgs& a, int LA, int fp64, cudaStream_t st) {
+  switch (LA) {
+    case 0: return launch_bp_LA<0>(a, fp64, st);
+    case 1: return launch_bp_LA<1>(a, fp64, st);
+    case 2: return launch_bp_LA<2>(a, fp64, st);
+    case 3: return launch_bp_LA<3>(a, fp64, st);
+    case 4: return launch_bp_LA<4>(a, fp64, st);
+    case 5: return launch_bp_LA<5>(a, fp64, st);
+    case 6: return launch_bp_LA<6>(a, fp64, st);
+    case 7: return launch_bp_LA<7>(a, fp64, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st) {
+  k_grad_local<<<(a.N + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -28,7 +28,8 @@ STOP_REFERENCE, STOP_FIXED, STOP_REL_L2 = 0, 1, 2
 # exported symbols of include/rte_b200.h (checked by the CPU tests)
 EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "rte_set_medium_tissue",
            "rte_set_medium_voxel", "rte_set_medium_device", "rte_source_beam", "rte_prop_abs", "rte_neumann",
-           "rte_images", "rte_forward", "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling",
+           "rte_images", "rte_forward", "rte_forward_batch", "rte_detector_flux", "rte_gradient",
+           "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling",
            "rte_get_stats")
 
 
@@ -55,6 +56,21 @@ class _Source(ctypes.Structure):
 
 class _Stop(ctypes.Structure):
     _fields_ = [("rule", ctypes.c_int), ("max_terms", ctypes.c_int), ("tol", ctypes.c_double)]
+
+
+class _Detector(ctypes.Structure):
+    _fields_ = [("nbins", ctypes.c_int), ("faces", ctypes.c_int)]
+
+
+@dataclass
+class Detector:
+    """nbins x nbins bins on each face in the `faces` bit mask (1 z=0, 2 z=nZ-1, 4 y=0, 8 y=nY-1,
+    16 x=0, 32 x=nX-1)."""
+    nbins: int = 8
+    faces: int = 63
+
+    def c(self):
+        return _Detector(self.nbins, self.faces)
 
 
 class _Stats(ctypes.Structure):
@@ -129,6 +145,12 @@ def load_library():
     L.rte_images.argtypes = [P, dp, ctypes.POINTER(_Source), dp, dp]
     L.rte_forward.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
                               ctypes.POINTER(_Report)]
+    L.rte_detector_flux.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop),
+                                    ctypes.POINTER(_Detector), dp]
+    L.rte_gradient.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop),
+                               ctypes.POINTER(_Detector), dp, ctypes.POINTER(ctypes.c_double), dp, dp]
+    L.rte_forward_batch.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
+                                    ctypes.POINTER(_Report)]
     _LIB = L
     return L
 
@@ -265,6 +287,49 @@ class Context:
         self._check(self.lib.rte_images(self.h, _ptr(out), ctypes.byref(s) if s is not None else None,
                                         _ptr(tr), _ptr(rf)), "rte_images")
         return tr.reshape(self.ny, self.nx), rf.reshape(self.ny, self.nx)
+
+    def detector_flux(self, srcs, stop, det):
+        """Binned exitant flux, shape (len(srcs), 6, nbins, nbins)."""
+        B = len(srcs)
+        out = np.zeros((B, 6, det.nbins, det.nbins))
+        arr = (_Source * B)(*[s.c() for s in srcs])
+        st, d = stop.c(), det.c()
+        self._check(self.lib.rte_detector_flux(self.h, B, arr, ctypes.byref(st), ctypes.byref(d), _ptr(out)),
+                    "rte_detector_flux")
+        return out
+
+    def gradient(self, srcs, stop, det, target):
+        """(loss, dL/dmu_a, dL/dmu_s) for loss = sum (flux - target)^2, by the adjoint method."""
+        B = len(srcs)
+        target = np.ascontiguousarray(target, np.float64).reshape(B, 6, det.nbins, det.nbins)
+        ga = np.zeros(self.N)
+        gs = np.zeros(self.N)
+        loss = ctypes.c_double(0.0)
+        arr = (_Source * B)(*[s.c() for s in srcs])
+        st, d = stop.c(), det.c()
+        self._check(self.lib.rte_gradient(self.h, B, arr, ctypes.byref(st), ctypes.byref(d), _ptr(target),
+                                          ctypes.byref(loss), _ptr(ga), _ptr(gs)), "rte_gradient")
+        return loss.value, ga, gs
+
+    def forward_batch(self, srcs, stop=None, want_W=True, want_images=True):
+        """Several sources on the current medium in one batched solve; returns the per-source results
+        stacked along a leading axis."""
+        stop = stop or Stop()
+        B = len(srcs)
+        W = np.zeros((B, self.N, self.C), np.complex128) if want_W else None
+        tr = np.zeros((B, self.ny, self.nx), np.complex128) if want_images else None
+        rf = np.zeros((B, self.ny, self.nx), np.complex128) if want_images else None
+        arr = (_Source * B)(*[s.c() for s in srcs])
+        rep = _Report()
+        st = stop.c()
+        self._check(self.lib.rte_forward_batch(self.h, B, arr, ctypes.byref(st), _ptr(W), _ptr(tr), _ptr(rf),
+                                               ctypes.byref(rep)), "rte_forward_batch")
+        res = dict(terms=rep.terms, last_rel=rep.last_rel, ms_device=rep.ms_device, ms_setup=rep.ms_setup)
+        if want_W:
+            res["W"] = W
+        if want_images:
+            res["trans"], res["ref"] = tr, rf
+        return res
 
     def forward(self, src, stop=None, want_W=True, want_images=True):
         stop = stop or Stop()

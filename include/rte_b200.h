@@ -142,6 +142,35 @@ int rte_images(rte_ctx* ctx, const rte_cplx* out, const rte_source* src, rte_cpl
 int rte_forward(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, rte_cplx* W_out,
                 rte_cplx* trans, rte_cplx* ref, rte_report* report);
 
+/* ---- detectors and derivatives (new entry points) -------------------------------- */
+typedef struct {
+  int nbins; /* bins per face edge: nbins x nbins bins per face (area-weighted pixel binning) */
+  int faces; /* bit mask of faces: 1 z=0, 2 z=nZ-1, 4 y=0, 8 y=nY-1, 16 x=0, 32 x=nX-1 */
+} rte_detector;
+
+/* Exitant flux per detector bin of each source: flux[src][6 faces][nbins][nbins] (faces outside
+ * the mask are 0).  Fluxes integrate the exitant radiance over the outward hemisphere of each
+ * face, with the ballistic beam on the z = nZ-1 face.  Single-column sources only. */
+int rte_detector_flux(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                      const rte_detector* det, double* flux);
+
+/* Adjoint gradient of loss = sum (flux - target)^2 (target laid out as rte_detector_flux's
+ * output) with respect to the per-voxel mu_a and mu_s of the current medium (N each).  One forward
+ * and one adjoint Neumann series per source plus one back-projection through the path integrals;
+ * exact for the discrete model when the series has converged (use RTE_STOP_REL_L2 with a small
+ * tolerance for derivative checks).  The reference computes region derivatives by forward
+ * sensitivity solves instead (FisherInfo_IO/src/compute_grad_rte.cu:273-385). */
+int rte_gradient(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                 const rte_detector* det, const double* target, double* loss, double* g_mua,
+                 double* g_mus);
+
+/* Batched forward solves (new): nsrc <= 4 sources on the current medium, propagated together so
+ * each voxel pair's direction, spherical harmonics and kernel value serve every source.  Outputs
+ * are the nsrc single-source results back to back (W_out nsrc*N*C, trans/ref nsrc*nX*nY, each may
+ * be NULL).  Stop rule RTE_STOP_FIXED or RTE_STOP_REL_L2 (norms over all sources). */
+int rte_forward_batch(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop,
+                      rte_cplx* W_out, rte_cplx* trans, rte_cplx* ref, rte_report* report);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ------------------
  * For callers that must not allocate device memory when they run the solver: work recorded
  * into a CUDA graph (cudaMalloc is illegal during stream capture), plug-ins whose host

@@ -134,3 +134,28 @@ def test_neumann_reference_stop_rule_fim(rte, oracle):
     otr, orf = oracle.images(p, mua, mus, ref_out, 1)
     assert rel(tr, otr) < 1e-6 and rel(rf, orf) < 1e-6
     ctx.close()
+
+
+def test_forward_batch_matches_single(rte, oracle):
+    """Four sources on one medium in one batched solve == four single solves (mixed precision), and
+    each within 1e-5 of the FP64 oracle."""
+    n, L = 9, 3
+    mua, mus, _ = rte.sphere_phantom(n, nspheres=2, seed=8, rmin=0.15, rmax=0.25)
+    srcs = [rte.Source(pos_x=x, pos_y=y) for x, y in ((-0.2, -0.2), (0.2, -0.2), (-0.2, 0.2), (0.0, 0.0))]
+    stop = rte.Stop(rte.STOP_FIXED, 12)
+    ctx, p = _ctx(rte, oracle, n, n, n, L, rte.MODEL_EXACT, rte.PREC_MIXED, kernel_mode=rte.KERNEL_STORE)
+    ctx.set_medium_voxel(mua, mus)
+    single = [ctx.forward(s, stop) for s in srcs]
+    rb4 = None
+    for nsrc in (4, 3, 2):
+        rb = ctx.forward_batch(srcs[:nsrc], stop)
+        rb4 = rb if nsrc == 4 else rb4
+        for b in range(nsrc):
+            assert rel(rb["W"][b], single[b]["W"]) < 1e-6
+            assert rel(rb["trans"][b], single[b]["trans"]) < 1e-6 and rel(rb["ref"][b], single[b]["ref"]) < 1e-6
+    for b, s in enumerate(srcs):
+        ref = oracle.forward(p, mua, mus, src_kind=oracle.SRC_COLUMN, img_mode=0, stop_rule=oracle.STOP_FIXED,
+                             max_terms=12, pos_x=s.pos_x, pos_y=s.pos_y)
+        assert rel(rb4["W"][b], ref["out"]) < 1e-5
+        assert rel(rb4["trans"][b], ref["trans"]) < 1e-5
+    ctx.close()
