@@ -172,6 +172,72 @@ def run_reference(args):
     return 0
 
 
+SERVE_GRIDS, SERVE_ORDERS = (17, 25, 33, 41), (3, 5, 7)
+
+
+def serve_requests(count, seed):
+    """The seeded request mix of the serving stream: grid from {17,25,33,41}^3 (0.1 cm), SH order from
+    {3,5,7}, background mu_a=0.01 / mu_s=1 plus 0-3 inclusions as in the phantom above, one source:
+    collimated beam or isotropic point on a random face at a uniform-random position."""
+    from doi_b200.phantoms import sphere_phantom
+    import doi_b200 as R
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        n = int(rng.choice(SERVE_GRIDS))
+        Lq = int(rng.choice(SERVE_ORDERS))
+        mua, mus, _ = sphere_phantom(n, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=int(rng.integers(0, 4)),
+                                     seed=seed * 100003 + q)
+        face = int(rng.integers(0, 6))
+        kind = R.SRC_BEAM if rng.random() < 0.5 else R.SRC_POINT
+        a, b = rng.uniform(-n * DX / 2, n * DX / 2, 2)
+        src = R.Source(pos_x=float(a), pos_y=float(b), pos_z=float(b + n * DX / 2), kind=kind, face=face)
+        out.append((n, Lq, mua, mus, src))
+    return out
+
+
+def run_serve(args, dev):
+    """Continuous-batching stream through rte_server_* with Poisson arrivals; latency from submit to
+    completion, throughput = completed requests / (first submit -> last completion)."""
+    import doi_b200 as R
+    reqs = serve_requests(args.serve_requests, seed=17)
+    rng = np.random.default_rng(23)
+    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
+    with R.Server(device=dev, workers=args.serve_workers) as srv:
+        # one request of every shape first (context creation, self-term tables, graph capture) so the
+        # stream measures steady-state serving; these are not counted
+        N0 = [(n, Lq) for n in SERVE_GRIDS for Lq in SERVE_ORDERS]
+        warm = [srv.submit(np.full(n ** 3, 0.01), np.full(n ** 3, 1.0), [R.Source(kind=R.SRC_BEAM)], n, dx=DX,
+                           nL=Lq, g=0.8, terms=TERMS) for n, Lq in N0]
+        for t in warm:
+            srv.wait(t, timeout=1800)
+        srv_stats0 = srv.stats()
+        t0 = time.perf_counter()
+        tickets, t_next = [], t0
+        for (n, Lq, mua, mus, src), gap in zip(reqs, gaps):
+            t_next += gap
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(mua, mus, [src], n, dx=DX, nL=Lq, g=0.8, terms=TERMS))
+        lat, dev_ms = [], 0.0
+        for t in tickets:
+            _, _, info = srv.wait(t, timeout=3600)
+            lat.append(info["latency_ms"])
+            dev_ms += info["device_ms"]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    lat = np.array(lat)
+    return {"requests": len(reqs), "arrival_rate_per_s": args.serve_rate, "workers": args.serve_workers,
+            "solves_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "wall_s": wall,
+            "device_ms_sum": dev_ms, "terms": TERMS, "precision": "mixed (stored FP32 pair kernel)",
+            "contexts": st["contexts"], "hbm_reserved_gb": st["hbm_reserved"] / 1e9,
+            "failed": st["failed"] - srv_stats0["failed"],
+            "mix": "grid {17,25,33,41}^3, L {3,5,7}, 0-3 inclusions, beam or isotropic point on a random "
+                   "face; warm-up: one uncounted request of every (grid, order) shape"}
+
+
 def run_ours(args):
     import torch
     import doi_b200 as R
@@ -318,6 +384,8 @@ def run_ours(args):
         }
         if ws == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(args.ref_seconds)
+        if args.serve_requests > 0:
+            line["serve"] = run_serve(args, dev)
         out = line
     ctx.close()
     if ws > 1:
@@ -341,6 +409,10 @@ def main():
     ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
     ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
                     help="sources per phantom solved together (1 = one source per solve)")
+    ap.add_argument("--serve-requests", type=int, default=64,
+                    help="requests in the serving stream (0 = skip; 2000 = the full stream)")
+    ap.add_argument("--serve-rate", type=float, default=3.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-workers", type=int, default=4, help="requests in flight at most")
     args = ap.parse_args()
     global N_SIDE
     N_SIDE = args.n

@@ -3,12 +3,12 @@
 The compute path is the CUDA library doi_b200/lib/librte_b200.so (C ABI in include/rte_b200.h);
 this package holds its build script, the ctypes binding and the phantom helpers.
 """
-from .rte import (Context, RteError, Source, Stop, Detector, load_library, MODEL_EXACT, MODEL_FIM, MODEL_CPU,
+from .rte import (Context, RteError, Server, Source, Stop, Detector, load_library, MODEL_EXACT, MODEL_FIM, MODEL_CPU,
                   PREC_FP64, PREC_MIXED, KERNEL_AUTO, KERNEL_STORE, KERNEL_RECOMPUTE, SRC_COLUMN, SRC_FIM,
-                  SRC_CPU, STOP_REFERENCE, STOP_FIXED, STOP_REL_L2)
+                  SRC_CPU, SRC_BEAM, SRC_POINT, STOP_REFERENCE, STOP_FIXED, STOP_REL_L2)
 from .phantoms import sphere_phantom, uniform_phantom
 
-__all__ = ["Context", "RteError", "Source", "Stop", "Detector", "load_library", "sphere_phantom", "uniform_phantom",
+__all__ = ["Context", "RteError", "Server", "Source", "Stop", "Detector", "load_library", "sphere_phantom", "uniform_phantom",
            "MODEL_EXACT", "MODEL_FIM", "MODEL_CPU", "PREC_FP64", "PREC_MIXED", "KERNEL_AUTO", "KERNEL_STORE",
-           "KERNEL_RECOMPUTE", "SRC_COLUMN", "SRC_FIM", "SRC_CPU", "STOP_REFERENCE", "STOP_FIXED",
+           "KERNEL_RECOMPUTE", "SRC_COLUMN", "SRC_FIM", "SRC_CPU", "SRC_BEAM", "SRC_POINT", "STOP_REFERENCE", "STOP_FIXED",
            "STOP_REL_L2"]

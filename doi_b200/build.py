@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librte_b200.so")
-SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp"]
+SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,10 +38,10 @@ def build(verbose=False, force=False, ptxas_verbose=False):
     objs = []
     for src in SOURCES:
         obj = os.path.join(LIBDIR, src + ".o")
-        cmd = [nvcc(), "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+        cmd = [nvcc()] + ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                "-I", os.path.join(HERE, "..", "include"), "-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cu"):
-            cmd[1:1] = ARCH + ["--expt-relaxed-constexpr"]
+            cmd[1:1] = ["--expt-relaxed-constexpr"]
             if ptxas_verbose:
                 cmd.insert(1, "-Xptxas=-v")
         if verbose:

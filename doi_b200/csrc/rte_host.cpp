@@ -339,6 +339,18 @@ struct rte_ctx {
   double *d_gt = nullptr, *d_gs = nullptr, *d_J = nullptr, *d_rho = nullptr, *d_dlut = nullptr;
   std::vector<double> h_h;      // host copy of the face weights
   size_t dlut_cap = 0;
+  double* d_fball = nullptr;    // ballistic flux per face pixel of the current single source
+  double* d_q = nullptr;        // point-source emission of the current single source [N][C]
+  bool has_point = false;
+  bool capturing = false;       // recording a CUDA graph: no host synchronisation allowed
+  bool capture_store = false;   // record the pair-kernel precompute into the graph being captured
+  // captured Neumann series per right-hand-side count (1, 2, 4) and terms
+  cudaGraphExec_t graph[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int graph_terms[5] = {0, 0, 0, 0, 0};
+  double* graph_w0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // buffers the graph reads W0 / S0 from
+  double* graph_s0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* d_bq = nullptr;       // batched point emissions [N][nb][C]
+  cudaEvent_t ev_graph[2] = {nullptr, nullptr};  // device time of one graph request
   size_t bytes = 0;
   double last_setup_ms = 0.0;
   // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
@@ -415,6 +427,10 @@ static cudaError_t dalloc(rte_ctx* c, T** p, size_t n) {
 }
 
 static void free_all(rte_ctx* c) {
+  for (int k = 0; k < 5; k++)
+    if (c->graph[k]) cudaGraphExecDestroy(c->graph[k]);
+  for (int k = 0; k < 2; k++)
+    if (c->ev_graph[k]) cudaEventDestroy(c->ev_graph[k]);
   for (int k = 0; k < 3; k++)
     for (auto& p : c->ev[k]) {
       cudaEventDestroy(p.first);
@@ -425,7 +441,7 @@ static void free_all(rte_ctx* c) {
                 c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img,
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
-                c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut};
+                c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -540,7 +556,10 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(cudaMemset(c->d_err, 0, sizeof(int)), "memset");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_cplx, 2 * NC), "alloc");
   if (rc == RTE_OK) cu(dalloc(c, &c->d_red, 8), "alloc");
-  if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 5 * (size_t)c->nx * c->ny), "alloc");  // trans, ref (complex), ballistic
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_img, 4 * (size_t)c->nx * c->ny), "alloc");  // trans, ref (complex)
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_fball, npix), "alloc");
+  if (rc == RTE_OK) cu(dalloc(c, &c->d_q, NC), "alloc");
   if (rc == RTE_OK) {
     std::vector<int> p = morton_perm(c->nx, c->ny, c->nz);
     std::vector<int> inv(c->N);
@@ -749,7 +768,7 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * ld));
     c->Kld = ld;
   }
-  if (!c->K_valid) {
+  if (!c->K_valid || c->capture_store) {
     PairArgs a;
     memset(&a, 0, sizeof a);
     a.N = c->N;
@@ -766,16 +785,20 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     a.mutf = c->d_mutf;
     a.Kmat = c->d_K;
     a.Kld = c->Kld;
-    CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
-    {
-      ProfScope ps(c, 1);
+    if (c->capturing) {
       CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+    } else {
+      CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
+      {
+        ProfScope ps(c, 1);
+        CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+      }
+      CUDA_TRY(c, cudaEventRecord(c->ev1, c->st));
+      CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+      c->last_setup_ms = ms;
     }
-    CUDA_TRY(c, cudaEventRecord(c->ev1, c->st));
-    CUDA_TRY(c, cudaEventSynchronize(c->ev1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    c->last_setup_ms = ms;
     c->K_valid = true;
   }
   *stored = true;
@@ -1075,6 +1098,21 @@ extern "C" int rte_neumann(rte_ctx* c, const rte_cplx* src, rte_cplx* out, int f
 
 // ---------------------------------------------------------------------------------------
 // Sources (real basis: the beam is m = 0 only, where both bases coincide).
+// In-face pixel of a face position: z faces (x, y) -> j*nx + k; y faces (x, z) -> i*nx + k;
+// x faces (y, z) -> i*ny + j.
+static int face_pixel_of(const rte_ctx* c, int face, double px, double py, double pz) {
+  auto idx = [](double p, double lo, double d, int n) {
+    int v = (int)floor((p - lo) / d);
+    return std::min(std::max(v, 0), n - 1);
+  };
+  const int k = idx(px, c->cfg.x_min, c->dx, c->nx), j = idx(py, c->cfg.y_min, c->dy, c->ny),
+            i = idx(pz, c->cfg.z_min, c->dz, c->nz);
+  if (face < 2) return j * c->nx + k;
+  if (face < 4) return i * c->nx + k;
+  return i * c->ny + j;
+}
+
+// Beam columns (entry-face pixels) and amplitude scale of a source.
 static int source_columns(const rte_ctx* c, const rte_source* s, std::vector<int>& cols, double& scale) {
   cols.clear();
   scale = 1.0;
@@ -1094,29 +1132,63 @@ static int source_columns(const rte_ctx* c, const rte_source* s, std::vector<int
     if (!cols.empty()) scale = s->mag / (double)cols.size();
     return RTE_OK;
   }
-  if (s->kind != RTE_SRC_COLUMN) return RTE_ERR_ARG;
-  int cx = (int)floor((s->pos_x - c->cfg.x_min) / c->dx), cy = (int)floor((s->pos_y - c->cfg.y_min) / c->dy);
-  cx = std::min(std::max(cx, 0), c->nx - 1);
-  cy = std::min(std::max(cy, 0), c->ny - 1);
-  cols.push_back(cy * c->nx + cx);
-  scale = s->mag;
-  return RTE_OK;
+  if (s->kind == RTE_SRC_COLUMN) {
+    cols.push_back(face_pixel_of(c, 0, s->pos_x, s->pos_y, s->pos_z));
+    scale = s->mag;
+    return RTE_OK;
+  }
+  if (s->kind == RTE_SRC_BEAM || s->kind == RTE_SRC_POINT) {
+    if (s->face < 0 || s->face > 5) return RTE_ERR_ARG;
+    cols.push_back(face_pixel_of(c, s->face, s->pos_x, s->pos_y, s->pos_z));
+    scale = s->mag;
+    return RTE_OK;
+  }
+  return RTE_ERR_ARG;
 }
 
-// xi = D A xi_beam on the pencil columns, built on the device into d_dst (real basis), with the
-// ballistic transmission per column in d_ball (dist.cu:66-101; Dist.c:1077-1128 for RTE_SRC_CPU).
-static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vstride = 0, double* d_ball = nullptr,
-                         bool zero = true) {
+static inline int source_face(const rte_source* s) {
+  return (s->kind == RTE_SRC_BEAM || s->kind == RTE_SRC_POINT) ? s->face : 0;
+}
+
+// voxel of face pixel p at depth t behind face f
+static int face_voxel(const rte_ctx* c, int f, int p, int t) {
+  const int plane = c->nx * c->ny;
+  if (f < 2) return (f == 0 ? t : c->nz - 1 - t) * plane + p;
+  if (f < 4) {
+    const int i = p / c->nx, k = p % c->nx, j = f == 2 ? t : c->ny - 1 - t;
+    return i * plane + j * c->nx + k;
+  }
+  const int i = p / c->ny, j = p % c->ny, k = f == 4 ? t : c->nx - 1 - t;
+  return i * plane + j * c->nx + k;
+}
+
+// Source terms of one right-hand side, built on the device into d_dst (real basis, rows vstride
+// apart): beams put xi = D A xi_beam on their column (dist.cu:66-101; Dist.c:1077-1128 for
+// RTE_SRC_CPU) and their ballistic exitant flux in d_fball; a point source puts its isotropic
+// emission q into d_q (its uncollided and scattered orders follow from the series).
+static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vstride = 0, double* d_fball = nullptr,
+                         bool zero = true, double* d_q = nullptr) {
   if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
   std::vector<int> cols;
   double scale;
-  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d", s->kind);
+  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d / face %d", s->kind, s->face);
   if ((int)cols.size() > RTE_MAX_SRC_COLS) return fail(c, RTE_ERR_UNSUPPORTED, "beam covers more than %d columns", RTE_MAX_SRC_COLS);
   if (vstride <= 0) vstride = c->C;
-  if (!d_ball) d_ball = c->d_img + 4 * (size_t)c->nx * c->ny;
-  if (zero) CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, (size_t)c->N * vstride * sizeof(double), c->st));
-  CUDA_TRY(c, cudaMemsetAsync(d_ball, 0, (size_t)c->nx * c->ny * sizeof(double), c->st));
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  if (!d_fball) d_fball = c->d_fball;
+  if (zero) {
+    CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, (size_t)c->N * vstride * sizeof(double), c->st));
+    CUDA_TRY(c, cudaMemsetAsync(d_fball, 0, npix * sizeof(double), c->st));
+  }
   if (cols.empty()) return RTE_OK;
+  if (s->kind == RTE_SRC_POINT) {
+    if (!d_q) return fail(c, RTE_ERR_UNSUPPORTED, "point sources are not available in this call");
+    const int r0 = face_voxel(c, s->face, cols[0], 0);
+    const double q = s->mag / (sqrt(4.0 * M_PI) * c->dV);  // isotropic: w_00 = I sqrt(4 pi), I = mag/(4 pi dV)
+    CUDA_TRY(c, cudaMemcpyAsync(d_q + (size_t)r0 * vstride, &q, sizeof(double), cudaMemcpyHostToDevice, c->st));
+    c->has_point = true;
+    return RTE_OK;
+  }
   SrcArgs a;
   memset(&a, 0, sizeof a);
   a.nx = c->nx;
@@ -1125,19 +1197,30 @@ static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vst
   a.Cfull = c->C;
   a.L = c->L;
   a.kind = s->kind;
+  a.face = source_face(s);
   a.ncols = (int)cols.size();
   for (size_t q = 0; q < cols.size(); q++) a.cols[q] = cols[q];
+  // HG scatter of the beam direction: coefficient g^l R_lm(d) (d = inward normal of the face)
+  const double dirs[6][3] = {{0, 0, 1}, {0, 0, -1}, {0, 1, 0}, {0, -1, 0}, {1, 0, 0}, {-1, 0, 0}};
+  std::vector<double> R(c->C);
+  sh_real_host(c->sh, c->L, dirs[a.face][0], dirs[a.face][1], dirs[a.face][2], R.data());
+  for (int l = 0, q = 0; l <= c->L; l++)
+    for (int m = -l; m <= l; m++, q++) {
+      double v = scale * pow(c->cfg.g, (double)l) * R[q];
+      if (m == 0 && a.face == 0) v = scale * pow(c->cfg.g, (double)l) * sqrt((2.0 * l + 1.0) / (4.0 * M_PI));
+      a.coef[q] = fabs(v) < 1e-300 ? 0.0 : v;
+    }
   a.scale = scale;
   a.mag = s->mag;
-  a.g = c->cfg.g;
-  a.dz = c->dz;
+  a.dlen = a.face < 2 ? c->dz : (a.face < 4 ? c->dy : c->dx);
   a.dV = c->dV;
   a.z_min = c->cfg.z_min;
+  a.dz = c->dz;
   a.vstride = vstride;
   a.mut = c->d_mut;
   a.mus = c->d_mus;
   a.W = d_dst;
-  a.ball = d_ball;
+  a.fball = d_fball;
   CUDA_TRY(c, (c->launches++, rte_launch_source(a, c->st)));
   return RTE_OK;
 }
@@ -1190,7 +1273,7 @@ static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a) {
 // images of a real-basis distribution on the device; with_ball adds the ballistic term left in
 // d_ball by the last launch_source.
 static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool with_ball, rte_cplx* trans,
-                      rte_cplx* ref, int vstride = 0, const double* d_ball = nullptr) {
+                      rte_cplx* ref, int vstride = 0, const double* d_fball = nullptr) {
   ImgArgs a;
   memset(&a, 0, sizeof a);
   a.nx = c->nx;
@@ -1203,7 +1286,7 @@ static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool
   int rc = image_weights(c, s, a);
   if (rc) return rc;
   const size_t np = (size_t)c->nx * c->ny;
-  a.ball = with_ball ? (d_ball ? d_ball : c->d_img + 4 * np) : nullptr;
+  a.fball = with_ball ? (d_fball ? d_fball : c->d_fball) : nullptr;
   a.trans = c->d_img;
   a.ref = c->d_img + 2 * np;
   CUDA_TRY(c, (c->launches++, rte_launch_images(a, c->st)));
@@ -1228,7 +1311,7 @@ extern "C" int rte_images(rte_ctx* c, const rte_cplx* out, const rte_source* s, 
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   int rc;
   if (s) {  // ballistic term of this source (the source itself goes to scratch)
-    rc = launch_source(c, s, c->d_aux3);
+    rc = launch_source(c, s, c->d_aux3, 0, nullptr, true, c->d_aux4);
     if (rc) return rc;
   }
   bool has2 = false;
@@ -1248,6 +1331,26 @@ extern "C" int rte_images(rte_ctx* c, const rte_cplx* out, const rte_source* s, 
   return RTE_OK;
 }
 
+// First term and initial running sum of the series for beams (xi) and point sources (q):
+// W0 = xi + D A q, S0 = xi + q + D A q (the point's uncollided field enters through the final A).
+// xi (in d_xi) becomes S0; W0 goes to d_w0.  nb right-hand sides interleaved ([N][nb][C]).
+static int series_start(rte_ctx* c, double* d_xi, double* d_q, double* d_w0, int nb, float* d_f32, int cpad) {
+  const size_t n = (size_t)c->N * nb * c->C;
+  if (!c->has_point) {
+    CUDA_TRY(c, cudaMemcpyAsync(d_w0, d_xi, n * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    return RTE_OK;
+  }
+  if (c->precision == RTE_PREC_MIXED)
+    CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(d_q, d_f32, c->d_islot, c->N, nb * c->C, cpad, c->C,
+                                                        c->cstride, c->st)));
+  int rc = apply_term(c, d_q, d_f32, d_w0, nullptr, nullptr, 1, 1, nb);
+  if (rc) return rc;
+  CUDA_TRY(c, (c->launches++, rte_launch_axpy(d_w0, d_xi, 1.0, n, c->st)));  // W0 = xi + DAq
+  CUDA_TRY(c, cudaMemcpyAsync(d_xi, d_w0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_axpy(d_xi, d_q, 1.0, n, c->st)));   // S0 = W0 + q
+  return RTE_OK;
+}
+
 extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop, rte_cplx* W_out, rte_cplx* trans,
                            rte_cplx* ref, rte_report* rep) {
   if (!c || !s || !stop) return fail(c, RTE_ERR_ARG, "null argument");
@@ -1259,8 +1362,12 @@ extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop
   CUDA_TRY(c, cudaEventRecord(t0, c->st));
   int terms = 0;
   double rel = 0;
-  int rc = launch_source(c, s, c->d_aux1);
-  if (!rc) rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, &terms, &rel);
+  c->has_point = false;
+  int rc = RTE_OK;
+  if (s->kind == RTE_SRC_POINT) CUDA_TRY(c, cudaMemsetAsync(c->d_q, 0, (size_t)c->N * c->C * sizeof(double), c->st));
+  rc = launch_source(c, s, c->d_aux1, 0, nullptr, true, c->d_q);
+  if (!rc) rc = series_start(c, c->d_aux1, c->d_q, c->d_aux3, 1, c->d_Wf, c->cpad);
+  if (!rc) rc = neumann_real(c, c->d_aux3, c->d_aux1, c->d_aux2, 1, stop, -1, &terms, &rel);
   if (!rc && (trans || ref)) rc = run_images(c, c->d_aux2, s, true, trans, ref);
   if (!rc) CUDA_TRY(c, cudaEventRecord(t1, c->st));
   if (!rc && W_out) rc = download_cplx(c, c->d_aux2, nullptr, W_out);
@@ -1380,9 +1487,13 @@ static int ensure_batch(rte_ctx* c, int nb) {
     *b = nullptr;
     CUDA_TRY(c, dalloc(c, b, NC * nb));
   }
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
   if (c->d_bball) cudaFree(c->d_bball);
   c->d_bball = nullptr;
-  CUDA_TRY(c, dalloc(c, &c->d_bball, (size_t)nb * c->nx * c->ny));
+  CUDA_TRY(c, dalloc(c, &c->d_bball, (size_t)nb * npix));
+  if (c->d_bq) cudaFree(c->d_bq);
+  c->d_bq = nullptr;
+  CUDA_TRY(c, dalloc(c, &c->d_bq, NC * nb));
   if (c->d_bWf) cudaFree(c->d_bWf);
   c->d_bWf = nullptr;
   const int cp = (nb * c->cstride + 3) / 4 * 4;
@@ -1425,12 +1536,17 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   CUDA_TRY(c, cudaEventCreate(&t0));
   CUDA_TRY(c, cudaEventCreate(&t1));
   CUDA_TRY(c, cudaEventRecord(t0, c->st));
-  CUDA_TRY(c, cudaMemsetAsync(c->d_bW, 0, NC * nb * sizeof(double), c->st));
-  CUDA_TRY(c, cudaMemsetAsync(c->d_bball, 0, np * nb * sizeof(double), c->st));
+  const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bsum, 0, NC * nb * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bq, 0, NC * nb * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bball, 0, npix * nb * sizeof(double), c->st));
+  c->has_point = false;
   for (int b = 0; b < nsrc && !rc; b++)
-    rc = launch_source(c, &srcs[b], c->d_bW + b * c->C, vs, c->d_bball + b * np, false);
+    rc = launch_source(c, &srcs[b], c->d_bsum + b * c->C, vs, c->d_bball + b * npix, false, c->d_bq + b * c->C);
   if (rc) return rc;
-  CUDA_TRY(c, cudaMemcpyAsync(c->d_bsum, c->d_bW, NC * nb * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  // W0 -> d_bW, S0 -> d_bsum
+  rc = series_start(c, c->d_bsum, c->d_bq, c->d_bW, nb, c->d_bWf, cp);
+  if (rc) return rc;
   CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
   const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
   int terms = 0;
@@ -1453,7 +1569,7 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   if (!rc) rc = check_kernel_err(c);
   for (int b = 0; b < nsrc && !rc && (trans || ref); b++)
     rc = run_images(c, c->d_bres + b * c->C, &srcs[b], true, trans ? trans + b * np : nullptr,
-                    ref ? ref + b * np : nullptr, vs, c->d_bball + b * np);
+                    ref ? ref + b * np : nullptr, vs, c->d_bball + b * npix);
   if (!rc) CUDA_TRY(c, cudaEventRecord(t1, c->st));
   for (int b = 0; b < nsrc && !rc && W_out; b++) {
     CUDA_TRY(c, (c->launches++, rte_launch_to_cplx(c->d_bres + b * c->C, nullptr, c->d_cplx, c->N, c->L, c->st, vs)));
@@ -1607,9 +1723,12 @@ static void unbin_faces(const rte_ctx* c, const rte_detector* d, const double* d
 // all face pixels (ballistic included) in J.
 static int forward_with_flux(rte_ctx* c, const rte_source* s, const rte_stop* stop, std::vector<double>& J, int* terms) {
   const size_t NC = (size_t)c->N * c->C;
-  int rc = launch_source(c, s, c->d_aux1);
+  c->has_point = false;
+  if (s->kind == RTE_SRC_POINT) CUDA_TRY(c, cudaMemsetAsync(c->d_q, 0, NC * sizeof(double), c->st));
+  int rc = launch_source(c, s, c->d_aux1, 0, nullptr, true, c->d_q);
+  if (!rc) rc = series_start(c, c->d_aux1, c->d_q, c->d_aux3, 1, c->d_Wf, c->cpad);
   if (rc) return rc;
-  rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_out, 1, stop, -1, terms, nullptr);
+  rc = neumann_real(c, c->d_aux3, c->d_aux1, c->d_out, 1, stop, -1, terms, nullptr);
   if (rc) return rc;
   CUDA_TRY(c, cudaMemcpyAsync(c->d_S, c->d_sum, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
   FaceArgs fa;
@@ -1621,7 +1740,7 @@ static int forward_with_flux(rte_ctx* c, const rte_source* s, const rte_stop* st
   fa.vstride = c->C;
   fa.out = c->d_out;
   fa.h = c->d_h;
-  fa.ball = c->d_img + 4 * (size_t)c->nx * c->ny;
+  fa.fball = c->d_fball;
   fa.J = c->d_J;
   CUDA_TRY(c, (c->launches++, rte_launch_face_flux(fa, c->st)));
   CUDA_TRY(c, cudaMemcpyAsync(J.data(), c->d_J, J.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -1636,6 +1755,7 @@ static int check_detector(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   if (stop->rule == RTE_STOP_REFERENCE) return fail(c, RTE_ERR_UNSUPPORTED, "detectors take a fixed or relative-L2 stop rule");
   for (int q = 0; q < nsrc; q++)
     if (srcs[q].kind == RTE_SRC_CPU) return fail(c, RTE_ERR_UNSUPPORTED, "detectors support single-column sources");
+  (void)0;
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   return ensure_detector_buffers(c);
 }
@@ -1666,6 +1786,10 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
                             const rte_detector* d, const double* target, double* loss, double* g_mua,
                             double* g_mus) {
   if (!c || !target || !g_mua || !g_mus) return fail(c, RTE_ERR_ARG, "null argument");
+  for (int q = 0; q < nsrc && srcs; q++)
+    if (srcs[q].kind != RTE_SRC_COLUMN && srcs[q].kind != RTE_SRC_FIM &&
+        !(srcs[q].kind == RTE_SRC_BEAM && srcs[q].face == 0))
+      return fail(c, RTE_ERR_UNSUPPORTED, "the gradient takes collimated sources on the z = 0 face");
   int rc = check_detector(c, nsrc, srcs, stop, d);
   if (rc) return rc;
   const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
@@ -1829,5 +1953,159 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
     g_mus[r] = gt[r] + gs[r] + gsum[r];
   }
   if (loss) *loss = L2;
+  return RTE_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Fixed-term Neumann series of nb right-hand sides as one CUDA graph per context: the pair-kernel
+// precompute (for the medium set before the replay), nterms x (pair, self, epilogue) and the final
+// attenuation, recorded once and replayed for every request of this shape.  W0 and S0 must be in
+// graph_w0 / graph_s0 before the replay; the result lands in d_bres (nb > 1) or d_aux2 (nb = 1).
+static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
+  const int gi = nb;
+  const size_t NC = (size_t)c->N * c->C;
+  const int vs = nb * c->C;
+  const int cp = (nb * c->cstride + 3) / 4 * 4;
+  double* W = nb == 1 ? c->d_W : c->d_bW;
+  double* Wn = nb == 1 ? c->d_Wn : c->d_bWn;
+  double* sum = nb == 1 ? c->d_sum : c->d_bsum;
+  double* res = nb == 1 ? c->d_aux2 : c->d_bres;
+  float* Wf = nb == 1 ? c->d_Wf : c->d_bWf;
+  const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
+  if (!c->graph[gi] || c->graph_terms[gi] != nterms) {
+    if (c->graph[gi]) {
+      cudaGraphExecDestroy(c->graph[gi]);
+      c->graph[gi] = nullptr;
+    }
+    // everything that may allocate or synchronise happens before the capture
+    bool stored = false;
+    int rc = ensure_pair_kernel(c, &stored);
+    if (rc) return rc;
+    int S, chunk;
+    rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
+    if (!rc) rc = plan_split(c, c->L, stored ? 1 : 0, nb, &S, &chunk);
+    if (!rc && flag_l == 0) rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
+    if (rc) return rc;
+    c->graph_w0[gi] = W;
+    c->graph_s0[gi] = sum;
+    const bool prof = c->profiling;
+    c->profiling = false;
+    c->capturing = true;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    if (stored) {  // the precompute for whatever medium is set when the graph is replayed
+      c->capture_store = true;
+      rc = ensure_pair_kernel(c, &stored);
+      c->capture_store = false;
+    }
+    cudaError_t e = rte_launch_to_f32_slots(W, Wf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st);
+    if (e == cudaSuccess) {
+      double *w = W, *wn = Wn;
+      for (int t = 0; t < nterms && !rc; t++) {
+        rc = apply_term(c, w, Wf, wn, Wf, sum, flag_l, 1, nb);
+        std::swap(w, wn);
+      }
+      if (!rc) e = rte_launch_to_f32_slots(sum, Wf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st);
+      if (!rc && e == cudaSuccess) rc = apply_term(c, sum, Wf, res, nullptr, nullptr, 1, 0, nb);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(c->st, &g);
+    c->capturing = false;
+    c->profiling = prof;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess || e2 != cudaSuccess)
+      return fail(c, RTE_ERR_DEVICE, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    cudaError_t e3 = cudaGraphInstantiate(&c->graph[gi], g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "graph instantiate: %s", cudaGetErrorString(e3));
+    c->graph_terms[gi] = nterms;
+  }
+  (void)NC;
+  c->launches += 4 * nterms + 4;
+  CUDA_TRY(c, cudaGraphLaunch(c->graph[gi], c->st));
+  c->K_valid = true;
+  *d_res = res;
+  return RTE_OK;
+}
+
+// One request through the graph path: sources (nsrc <= 4 on the current medium), the captured
+// series, images.  trans/ref: nsrc * nx * ny complex (may be null).
+static int forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, int nterms, rte_cplx* trans, rte_cplx* ref,
+                         float* ms_out) {
+  if (nsrc > 1 && c->precision != RTE_PREC_MIXED) {  // FP64 keeps one right-hand side per series
+    float tot = 0;
+    const size_t np = (size_t)c->nx * c->ny;
+    for (int b = 0; b < nsrc; b++) {
+      float ms = 0;
+      int rc = forward_graph(c, 1, srcs + b, nterms, trans ? trans + b * np : nullptr, ref ? ref + b * np : nullptr, &ms);
+      if (rc) return rc;
+      tot += ms;
+    }
+    if (ms_out) *ms_out = tot;
+    return RTE_OK;
+  }
+  const int nb = nsrc == 1 ? 1 : (nsrc <= 2 ? 2 : 4);
+  int rc = nb > 1 ? ensure_batch(c, nb) : RTE_OK;
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  const int vs = nb * c->C;
+  const int cp = (nb * c->cstride + 3) / 4 * 4;
+  if (!c->ev_graph[0]) {
+    CUDA_TRY(c, cudaEventCreate(&c->ev_graph[0]));
+    CUDA_TRY(c, cudaEventCreate(&c->ev_graph[1]));
+  }
+  cudaEvent_t t0 = c->ev_graph[0], t1 = c->ev_graph[1];
+  CUDA_TRY(c, cudaEventRecord(t0, c->st));
+  double* dres = nullptr;
+  if (!c->graph[nb] || c->graph_terms[nb] != nterms) {
+    // first request of this shape: record the graph on zero inputs, then run the real one
+    double* w = nb == 1 ? c->d_W : c->d_bW;
+    double* sm = nb == 1 ? c->d_sum : c->d_bsum;
+    CUDA_TRY(c, cudaMemsetAsync(w, 0, NC * nb * sizeof(double), c->st));
+    CUDA_TRY(c, cudaMemsetAsync(sm, 0, NC * nb * sizeof(double), c->st));
+    rc = run_series_graph(c, nb, nterms, &dres);
+    if (rc) return rc;
+  }
+  double* W0 = c->graph_w0[nb];
+  double* S0 = c->graph_s0[nb];
+  double* q = nb == 1 ? c->d_q : c->d_bq;
+  double* fb = nb == 1 ? c->d_fball : c->d_bball;
+  CUDA_TRY(c, cudaMemsetAsync(S0, 0, NC * nb * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(q, 0, NC * nb * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(fb, 0, npix * nb * sizeof(double), c->st));
+  c->has_point = false;
+  for (int b = 0; b < nsrc && !rc; b++)
+    rc = launch_source(c, &srcs[b], S0 + b * c->C, vs, fb + b * npix, false, q + b * c->C);
+  if (!rc) rc = series_start(c, S0, q, W0, nb, nb == 1 ? c->d_Wf : c->d_bWf, cp);
+  if (!rc) rc = run_series_graph(c, nb, nterms, &dres);
+  for (int b = 0; b < nsrc && !rc && (trans || ref); b++)
+    rc = run_images(c, dres + b * c->C, &srcs[b], true, trans ? trans + b * np : nullptr,
+                    ref ? ref + b * np : nullptr, vs, fb + b * npix);
+  if (!rc) CUDA_TRY(c, cudaEventRecord(t1, c->st));
+  if (!rc) CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  if (!rc) rc = check_kernel_err(c);
+  float ms = 0;
+  if (!rc) cudaEventElapsedTime(&ms, t0, t1);
+  if (ms_out) *ms_out = ms;
+  return rc;
+}
+
+extern "C" int rte_forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, int nterms, rte_cplx* trans,
+                                 rte_cplx* ref, rte_report* rep) {
+  if (!c || !srcs || nsrc < 1 || nsrc > kMaxBatch || nterms < 0) return fail(c, RTE_ERR_ARG, "bad argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  float ms = 0;
+  int rc = forward_graph(c, nsrc, srcs, nterms, trans, ref, &ms);
+  if (rc) return rc;
+  if (rep) {
+    rep->terms = nterms;
+    rep->last_rel = 0;
+    rep->ms_device = ms;
+    rep->ms_setup = 0;
+  }
   return RTE_OK;
 }

@@ -64,7 +64,7 @@ struct ImgArgs {
   const double* out;
   double wt[RTE_MAX_L + 1];  // transmission weights per l (m = 0 coefficient)
   double wr[RTE_MAX_L + 1];  // reflection weights per l
-  const double* ball;        // nx*ny ballistic transmission added to trans (may be null)
+  const double* fball;       // ballistic flux per face pixel (z- first, z+ next); may be null
   double* trans;  // nx*ny complex (re, im)
   double* ref;
 };
@@ -79,13 +79,15 @@ struct ShTables {
 
 struct SrcArgs {
   int nx, ny, nz, Cfull, L, kind, ncols;
-  int cols[RTE_MAX_SRC_COLS];
-  double scale, mag, g, dz, dV, z_min;
+  int face;                   // entry face (detector order: z-, z+, y-, y+, x-, x+)
+  int cols[RTE_MAX_SRC_COLS]; // pixels of the entry face (row-major in the face) hit by the beam
+  double coef[64];            // per real coefficient: scale * g^l * R_lm(beam direction)
+  double scale, mag, dlen, dV, z_min, dz;
   int vstride;   // elements between consecutive voxels of W (Cfull for one right-hand side)
   const double* mut;
   const double* mus;
   double* W;     // N x vstride, zeroed by the caller
-  double* ball;  // nx*ny ballistic transmission, zeroed by the caller
+  double* fball; // ballistic exitant flux per face pixel (all six faces), zeroed by the caller
 };
 
 // detector faces and the adjoint gradient
@@ -93,7 +95,7 @@ struct FaceArgs {
   int nx, ny, nz, Cfull, vstride;
   const double* out;   // real basis [N][vstride]
   const double* h;     // [6][Cfull] exitant-flux weights of each face (area and cm included)
-  const double* ball;  // nx*ny ballistic transmission of the z = nZ-1 face (may be null)
+  const double* fball; // ballistic flux per face pixel, same layout as J (may be null)
   double* J;           // fluxes of all face pixels (z-, z+, y-, y+, x-, x+ concatenated)
   const double* rho;   // adjoint seed: dL/dJ per face pixel
   double* e;           // adjoint seed field [N][Cfull]

@@ -669,7 +669,10 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
       fi += a.wr[l] * out_im[rr * a.vstride + c];
     }
   }
-  if (a.ball) t += a.ball[p];
+  if (a.fball) {
+    t += a.fball[(size_t)a.nx * a.ny + p];
+    f += a.fball[p];
+  }
   if (a.trans) {
     a.trans[2 * p] = t;
     a.trans[2 * p + 1] = ti;
@@ -687,32 +690,54 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
 __global__ void k_source(SrcArgs a) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= a.ncols) return;
-  const int col = a.cols[q];
+  const int p = a.cols[q];
   const int plane = a.nx * a.ny;
+  const int axis = a.face / 2;  // 0: along z, 1: along y, 2: along x
+  const bool up = (a.face & 1) == 0;
+  int n, base, stride, row, col;
+  if (axis == 0) {
+    n = a.nz;
+    base = p;
+    stride = plane;
+  } else if (axis == 1) {
+    n = a.ny;
+    row = p / a.nx;  // i
+    col = p % a.nx;  // k
+    base = row * plane + col;
+    stride = a.nx;
+  } else {
+    n = a.nx;
+    row = p / a.ny;  // i
+    col = p % a.ny;  // j
+    base = row * plane + col * a.nx;
+    stride = 1;
+  }
   double att = 1.0, mt = 0.0;
-  for (int i = 0; i < a.nz; ++i) {
-    const size_t r = (size_t)i * plane + col;
+  for (int t = 0; t < n; ++t) {
+    const size_t r = (size_t)base + (size_t)(up ? t : n - 1 - t) * stride;
     mt = a.mut[r];
     const double ms = a.mus[r];
     double v;
-    if (a.kind == 2) {
-      const double tz = (double)i * a.dz + a.z_min + a.dz / 2.0 - a.dz / 2.0;
+    if (a.kind == 2) {  // absolute depth of the voxel top (z- entry only)
+      const double tz = (double)t * a.dz + a.z_min + a.dz / 2.0 - a.dz / 2.0;
       v = exp(-mt * tz) - exp(-mt * (tz + a.dz));
     } else {
-      v = att * (1 - exp(-mt * a.dz));
+      v = att * (1 - exp(-mt * a.dlen));
     }
-    att *= exp(-mt * a.dz);
-    double gl = 1.0;
-    for (int l = 0; l <= a.L; ++l) {
-      a.W[r * a.vstride + l * l + l] = a.scale * gl * ms / mt * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) * v / a.dV;
-      gl *= a.g;
-    }
+    att *= exp(-mt * a.dlen);
+    const double amp = ms / mt * v / a.dV;
+    for (int c = 0; c < a.Cfull; ++c)
+      if (a.coef[c] != 0.0) a.W[r * a.vstride + c] += amp * a.coef[c];
   }
+  // exit face = the opposite face, same in-face pixel
+  const int ef = a.face ^ 1;
+  const size_t a0 = (size_t)a.nx * a.ny, a1 = (size_t)a.nz * a.nx, a2 = (size_t)a.nz * a.ny;
+  const size_t off[6] = {0, a0, 2 * a0, 2 * a0 + a1, 2 * a0 + 2 * a1, 2 * a0 + 2 * a1 + a2};
   if (a.kind == 2) {
     const double zs = (double)(a.nz - 1) * a.dz + a.z_min + a.dz / 2.0;
-    a.ball[col] = a.scale * exp(-mt * (zs + a.dz / 2.0));
+    a.fball[off[ef] + p] = a.scale * exp(-mt * (zs + a.dz / 2.0));
   } else {
-    a.ball[col] = a.mag * att;
+    a.fball[off[ef] + p] = a.mag * att;
   }
 }
 
@@ -805,7 +830,7 @@ __global__ void k_face_flux(FaceArgs a) {
   const double* o = a.out + (size_t)r * a.vstride;
   double J = 0.0;
   for (int c = 0; c < a.Cfull; ++c) J = fma(h[c], o[c], J);
-  if (f == 1 && a.ball) J += a.ball[p];
+  if (a.fball) J += a.fball[q];
   a.J[q] = J;
 }
 

@@ -22,15 +22,16 @@ LIB_PATH = os.path.join(_HERE, "lib", "librte_b200.so")
 MODEL_EXACT, MODEL_FIM, MODEL_CPU = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 KERNEL_AUTO, KERNEL_STORE, KERNEL_RECOMPUTE = 0, 1, 2
-SRC_COLUMN, SRC_FIM, SRC_CPU = 0, 1, 2
+SRC_COLUMN, SRC_FIM, SRC_CPU, SRC_BEAM, SRC_POINT = 0, 1, 2, 3, 4
 STOP_REFERENCE, STOP_FIXED, STOP_REL_L2 = 0, 1, 2
 
 # exported symbols of include/rte_b200.h (checked by the CPU tests)
 EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "rte_set_medium_tissue",
            "rte_set_medium_voxel", "rte_set_medium_device", "rte_source_beam", "rte_prop_abs", "rte_neumann",
            "rte_images", "rte_forward", "rte_forward_batch", "rte_detector_flux", "rte_gradient",
-           "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling",
-           "rte_get_stats")
+           "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling", "rte_get_stats", "rte_forward_graph",
+           "rte_server_create", "rte_server_submit", "rte_server_wait", "rte_server_cancel", "rte_server_stats",
+           "rte_server_destroy")
 
 
 class RteError(RuntimeError):
@@ -51,7 +52,8 @@ class _Config(ctypes.Structure):
 class _Source(ctypes.Structure):
     _fields_ = [("pos_x", ctypes.c_double), ("pos_y", ctypes.c_double), ("pos_z", ctypes.c_double),
                 ("diam", ctypes.c_double), ("theta", ctypes.c_double), ("phi", ctypes.c_double),
-                ("mag", ctypes.c_double), ("modulation", ctypes.c_double), ("kind", ctypes.c_int)]
+                ("mag", ctypes.c_double), ("modulation", ctypes.c_double), ("kind", ctypes.c_int),
+                ("face", ctypes.c_int)]
 
 
 class _Stop(ctypes.Structure):
@@ -95,10 +97,11 @@ class Source:
     mag: float = 1.0
     modulation: float = 0.0
     kind: int = SRC_COLUMN
+    face: int = 0
 
     def c(self):
         return _Source(self.pos_x, self.pos_y, self.pos_z, self.diam, self.theta, self.phi, self.mag,
-                       self.modulation, self.kind)
+                       self.modulation, self.kind, self.face)
 
 
 @dataclass
@@ -109,6 +112,24 @@ class Stop:
 
     def c(self):
         return _Stop(self.rule, self.max_terms, self.tol)
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("dx", ctypes.c_double), ("nL", ctypes.c_int), ("g", ctypes.c_double),
+                ("n_index", ctypes.c_double), ("precision", ctypes.c_int), ("terms", ctypes.c_int),
+                ("nsrc", ctypes.c_int), ("src", _Source * 4), ("mua", ctypes.c_void_p), ("mus", ctypes.c_void_p)]
+
+
+class _ResultInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("service_ms", ctypes.c_double), ("device_ms", ctypes.c_double)]
+
+
+class _ServerInfo(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("cancelled", ctypes.c_longlong), ("inflight", ctypes.c_longlong), ("pending", ctypes.c_longlong),
+                ("contexts", ctypes.c_int), ("hbm_reserved", ctypes.c_size_t), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("wall_s", ctypes.c_double)]
 
 
 _LIB = None
@@ -151,6 +172,15 @@ def load_library():
                                ctypes.POINTER(_Detector), dp, ctypes.POINTER(ctypes.c_double), dp, dp]
     L.rte_forward_batch.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
                                     ctypes.POINTER(_Report)]
+    L.rte_forward_graph.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.c_int, dp, dp,
+                                    ctypes.POINTER(_Report)]
+    L.rte_server_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.rte_server_submit.argtypes = [P, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_longlong)]
+    L.rte_server_wait.argtypes = [P, ctypes.c_longlong, ctypes.c_double, dp, dp, ctypes.POINTER(_ResultInfo)]
+    L.rte_server_cancel.argtypes = [P, ctypes.c_longlong]
+    L.rte_server_stats.argtypes = [P, ctypes.POINTER(_ServerInfo)]
+    L.rte_server_destroy.argtypes = [P]
+    L.rte_server_destroy.restype = None
     _LIB = L
     return L
 
@@ -331,6 +361,18 @@ class Context:
             res["trans"], res["ref"] = tr, rf
         return res
 
+    def forward_graph(self, srcs, nterms):
+        """Fixed-term forward solve of up to 4 sources, replayed from a CUDA graph recorded on the
+        first call; returns (trans, ref) stacked per source and the device time in ms."""
+        B = len(srcs)
+        tr = np.zeros((B, self.ny, self.nx), np.complex128)
+        rf = np.zeros((B, self.ny, self.nx), np.complex128)
+        arr = (_Source * B)(*[s.c() for s in srcs])
+        rep = _Report()
+        self._check(self.lib.rte_forward_graph(self.h, B, arr, int(nterms), _ptr(tr), _ptr(rf), ctypes.byref(rep)),
+                    "rte_forward_graph")
+        return tr, rf, rep.ms_device
+
     def forward(self, src, stop=None, want_W=True, want_images=True):
         stop = stop or Stop()
         W = np.zeros((self.N, self.C), np.complex128) if want_W else None
@@ -347,3 +389,78 @@ class Context:
             res["trans"] = tr.reshape(self.ny, self.nx)
             res["ref"] = rf.reshape(self.ny, self.nx)
         return res
+
+
+class Server:
+    """Continuous-batching forward-solve server on one GPU (rte_server_*).
+
+    submit() copies the request and returns a ticket at once; requests of any grid / order / medium
+    run concurrently as HBM and worker slots allow; wait() returns (trans, ref, info)."""
+
+    def __init__(self, device=0, hbm_budget_gb=0.0, workers=4):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.rte_server_create(device, float(hbm_budget_gb), int(workers), ctypes.byref(h))
+        if rc != 0:
+            raise RteError(f"rte_server_create failed ({rc})")
+        self.h = h
+        self._shape = {}
+
+    def submit(self, mua, mus, srcs, n, dx=0.1, nL=3, g=0.8, n_index=1.0, precision=PREC_MIXED, terms=12):
+        mua = np.ascontiguousarray(mua, np.float64).ravel()
+        mus = np.ascontiguousarray(mus, np.float64).ravel()
+        if mua.size != n ** 3 or mus.size != n ** 3:
+            raise RteError("medium arrays must have n^3 entries")
+        if not 1 <= len(srcs) <= 4:
+            raise RteError("1 to 4 sources per request")
+        rq = _Request()
+        rq.n, rq.dx, rq.nL, rq.g, rq.n_index = n, dx, nL, g, n_index
+        rq.precision, rq.terms, rq.nsrc = precision, terms, len(srcs)
+        for i, s in enumerate(srcs):
+            rq.src[i] = s.c()
+        rq.mua, rq.mus = mua.ctypes.data, mus.ctypes.data
+        t = ctypes.c_longlong(0)
+        rc = self.lib.rte_server_submit(self.h, ctypes.byref(rq), ctypes.byref(t))
+        if rc != 0:
+            raise RteError(f"rte_server_submit failed ({rc})")
+        self._shape[t.value] = (len(srcs), n)
+        return t.value
+
+    def wait(self, ticket, timeout=600.0):
+        B, n = self._shape[ticket]
+        tr = np.zeros((B, n, n), np.complex128)
+        rf = np.zeros((B, n, n), np.complex128)
+        info = _ResultInfo()
+        rc = self.lib.rte_server_wait(self.h, ticket, float(timeout), _ptr(tr), _ptr(rf), ctypes.byref(info))
+        if rc == 7:  # RTE_ERR_TIMEOUT: the ticket stays valid
+            raise TimeoutError(f"request {ticket} still running")
+        del self._shape[ticket]
+        if rc != 0:
+            raise RteError(f"request {ticket} failed ({rc})")
+        return tr, rf, {k: getattr(info, k) for k, _ in _ResultInfo._fields_}
+
+    def cancel(self, ticket):
+        return self.lib.rte_server_cancel(self.h, ticket) == 0
+
+    def stats(self):
+        st = _ServerInfo()
+        if self.lib.rte_server_stats(self.h, ctypes.byref(st)) != 0:
+            raise RteError("rte_server_stats failed")
+        return {k: getattr(st, k) for k, _ in _ServerInfo._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rte_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

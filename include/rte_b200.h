@@ -31,6 +31,7 @@ extern "C" {
 #define RTE_ERR_IO 5          /* file could not be read or written */
 #define RTE_ERR_UNSUPPORTED 6 /* feature outside this build's limits */
 #define RTE_ERR_TIMEOUT 7     /* a bounded device wait ran out */
+#define RTE_ERR_CANCELLED 8   /* the request was cancelled before it ran */
 
 /* ---- discretisation models (which reference the numbers follow) ------------------- */
 #define RTE_MODEL_EXACT 0 /* exact Y_lm, exact path integral, 200x200 self term, exact exitance */
@@ -47,6 +48,8 @@ extern "C" {
 #define RTE_SRC_COLUMN 0 /* collimated pencil on the z=0 face, column containing (pos_x,pos_y) */
 #define RTE_SRC_FIM 1    /* FisherInfo_IO rule: column x == nX/2.0 && y == nY/2.0 (even grids only) */
 #define RTE_SRC_CPU 2    /* CPU package rule: columns within diam/2, normalised by column count */
+#define RTE_SRC_BEAM 3   /* collimated beam entering through `face` along its inward normal (new) */
+#define RTE_SRC_POINT 4  /* isotropic point source in the first voxel layer behind `face` (new) */
 
 #define RTE_STOP_REFERENCE 0 /* reference lambda > 0.9999 rule (dist.cu:1132-1172) */
 #define RTE_STOP_FIXED 1     /* exactly max_terms terms */
@@ -83,6 +86,8 @@ typedef struct {
   double mag;
   double modulation; /* must be 0: the steady-state path only */
   int kind;          /* RTE_SRC_* */
+  int face;          /* RTE_SRC_BEAM / RTE_SRC_POINT: 0 z=0, 1 z=nZ-1, 2 y=0, 3 y=nY-1, 4 x=0, 5 x=nX-1;
+                        the position on the face comes from the two in-face coordinates of pos_* */
 } rte_source;
 
 typedef struct {
@@ -170,6 +175,60 @@ int rte_gradient(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop*
  * be NULL).  Stop rule RTE_STOP_FIXED or RTE_STOP_REL_L2 (norms over all sources). */
 int rte_forward_batch(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop,
                       rte_cplx* W_out, rte_cplx* trans, rte_cplx* ref, rte_report* report);
+
+/* One forward solve of nsrc <= 4 sources on the current medium with a fixed number of terms,
+ * recorded once per context as a CUDA graph (pair-kernel precompute, series, final attenuation)
+ * and replayed afterwards; the first call on a context records the graph.  Images as
+ * rte_forward_batch.  The serving path uses it. */
+int rte_forward_graph(rte_ctx* ctx, int nsrc, const rte_source* srcs, int nterms, rte_cplx* trans,
+                      rte_cplx* ref, rte_report* report);
+
+/* ---- serving: continuous batching of forward solves (new) ---------------------------
+ * Requests of any grid, order, medium and sources are admitted as execution slots and HBM
+ * (budget) free up and run concurrently on the device, one context (and CUDA stream) per
+ * admitted request; contexts are kept per shape and reused (idle ones of other shapes are
+ * evicted when HBM is short).  Latency = submit to completion. */
+typedef struct {
+  int n;             /* voxels per edge of the cubic grid */
+  double dx;         /* voxel edge (cm); x and y centred on 0, z from 0 */
+  int nL;            /* SH order */
+  double g, n_index; /* anisotropy, refractive index */
+  int precision;     /* RTE_PREC_MIXED (stored pair kernel) or RTE_PREC_FP64 */
+  int terms;         /* Neumann terms */
+  int nsrc;          /* 1..4 sources solved together */
+  rte_source src[4];
+  const double* mua; /* n^3 values each, copied by rte_server_submit */
+  const double* mus;
+} rte_request;
+
+typedef struct {
+  int status;        /* RTE_OK or the failure code */
+  double latency_ms; /* submit -> done */
+  double queue_ms;   /* submit -> admitted */
+  double service_ms; /* admitted -> done */
+  double device_ms;  /* CUDA-event time of the solve on the device */
+} rte_result_info;
+
+typedef struct {
+  long long submitted, completed, failed, cancelled, inflight, pending;
+  int contexts;        /* contexts alive (busy or idle) */
+  size_t hbm_reserved; /* HBM reserved by admitted shapes */
+  double p50_ms, p99_ms, mean_ms; /* latency of completed requests */
+  double wall_s;       /* first submit -> last completion */
+} rte_server_info;
+
+typedef struct rte_server rte_server;
+
+/* hbm_budget_gb <= 0: 85% of the free memory; nworkers = requests in flight at most. */
+int rte_server_create(int device, double hbm_budget_gb, int nworkers, rte_server** out);
+int rte_server_submit(rte_server* srv, const rte_request* req, long long* ticket);
+/* Waits up to timeout_s; trans/ref get nsrc*n*n complex values.  Returns the request status
+ * (RTE_ERR_TIMEOUT if it is still running).  A ticket can be waited for once. */
+int rte_server_wait(rte_server* srv, long long ticket, double timeout_s, rte_cplx* trans, rte_cplx* ref,
+                    rte_result_info* info);
+int rte_server_cancel(rte_server* srv, long long ticket); /* only before it starts */
+int rte_server_stats(rte_server* srv, rte_server_info* out);
+void rte_server_destroy(rte_server* srv);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ------------------
  * For callers that must not allocate device memory when they run the solver: work recorded
