@@ -411,7 +411,8 @@ def main():
                     help="sources per phantom solved together (1 = one source per solve)")
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
-    ap.add_argument("--serve-rate", type=float, default=3.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-rate", type=float, default=1.5,
+                    help="Poisson arrival rate (requests/s); about 0.9x the measured capacity of the mix")
     ap.add_argument("--serve-workers", type=int, default=4, help="requests in flight at most")
     args = ap.parse_args()
     global N_SIDE

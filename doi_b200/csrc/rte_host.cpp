@@ -17,6 +17,9 @@
 
 #include <algorithm>
 #include <array>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <unordered_map>
 #include <cstdlib>
 #include <string>
@@ -351,6 +354,10 @@ struct rte_ctx {
   double* graph_s0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* d_bq = nullptr;       // batched point emissions [N][nb][C]
   cudaEvent_t ev_graph[2] = {nullptr, nullptr};  // device time of one graph request
+  // every device pointer and scalar a recorded graph baked into its kernel parameters; a graph whose
+  // signature differs from the context's current one (a buffer was reallocated, the self-term path
+  // or its series length changed with the medium) is recorded again before it is replayed
+  std::vector<uintptr_t> graph_sig[5];
   size_t bytes = 0;
   double last_setup_ms = 0.0;
   // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
@@ -527,7 +534,15 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   if (rc == RTE_OK) cu(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "stream");
   if (rc == RTE_OK) cu(cudaEventCreate(&c->ev0), "event");
   if (rc == RTE_OK) cu(cudaEventCreate(&c->ev1), "event");
-  if (rc == RTE_OK) cu(rte_upload_sh_tables(c->sh), "SH tables");
+  if (rc == RTE_OK) {  // the tables do not depend on the order: one upload per device and process
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), cfg->device) == done.end()) {
+      cu(rte_upload_sh_tables(c->sh), "SH tables");
+      if (rc == RTE_OK) done.push_back(cfg->device);
+    }
+  }
   const size_t NC = (size_t)c->N * c->C;
   if (const char* e = getenv("RTE_MAX_SPLIT")) c->max_split = std::max(1, std::min(32, atoi(e)));
   if (rc == RTE_OK) cu(dalloc(c, &c->d_perm, c->N), "alloc");
@@ -621,12 +636,8 @@ static int ensure_moments(rte_ctx* c, double mumax) {
   if (K <= c->K && c->d_mom) return RTE_OK;
   std::vector<double>& mom = c->h_mom;
   build_moments(c->quad, K, c->dV, mom);
-  if (c->d_mom) {
-    cudaFree(c->d_mom);
-    c->bytes -= (size_t)c->K * c->C * c->C * sizeof(double);
-    c->d_mom = nullptr;
-  }
-  CUDA_TRY(c, dalloc(c, &c->d_mom, mom.size()));
+  if (!c->d_mom)  // room for the longest series, so the table never moves (recorded graphs keep it)
+    CUDA_TRY(c, dalloc(c, &c->d_mom, (size_t)RTE_MAX_MOM * c->C * c->C));
   CUDA_TRY(c, cudaMemcpy(c->d_mom, mom.data(), sizeof(double) * mom.size(), cudaMemcpyHostToDevice));
   c->K = K;
   return RTE_OK;
@@ -672,8 +683,9 @@ static int build_self_lut(rte_ctx* c) {
         c->bytes -= c->dlut_cap * sizeof(double);
         c->d_dlut = nullptr;
       }
-      CUDA_TRY(c, dalloc(c, &c->d_dlut, dlut.size()));
-      c->dlut_cap = dlut.size();
+      const size_t cap = std::max(dlut.size(), (size_t)16 * C * C);  // headroom: fewer reallocations
+      CUDA_TRY(c, dalloc(c, &c->d_dlut, cap));
+      c->dlut_cap = cap;
     }
     (void)rc;
     CUDA_TRY(c, cudaMemcpyAsync(c->d_dlut, dlut.data(), sizeof(double) * dlut.size(), cudaMemcpyHostToDevice, c->st));
@@ -684,8 +696,9 @@ static int build_self_lut(rte_ctx* c) {
       c->bytes -= c->lut_cap * sizeof(double);
       c->d_self_lut = nullptr;
     }
-    CUDA_TRY(c, dalloc(c, &c->d_self_lut, lut.size()));
-    c->lut_cap = lut.size();
+    const size_t cap = std::max(lut.size(), (size_t)16 * C * C);
+    CUDA_TRY(c, dalloc(c, &c->d_self_lut, cap));
+    c->lut_cap = cap;
   }
   CUDA_TRY(c, cudaMemcpyAsync(c->d_self_lut, lut.data(), sizeof(double) * lut.size(), cudaMemcpyHostToDevice, c->st));
   CUDA_TRY(c, cudaMemcpyAsync(c->d_self_idx, idx.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice, c->st));
@@ -807,57 +820,10 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
 
 // Split-K plan: the number of source chunks S so that tiles x S CTAs fill whole waves of the
 // kernel's resident CTAs (a partial last wave idles SMs).
-static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
-  const int key = ((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0);
-  for (auto& e : c->splits)
-    if (e[0] == key) {
-      *S_out = e[1];
-      *chunk_out = e[2];
-      return RTE_OK;
-    }
-  int occ = 0;
-  const int cpad = (nb * ((c->C + 1) / 2 * 2) + 3) / 4 * 4;
-  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored, nb, cpad, &occ));
-  int sms = 0;
-  CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
-  const long long slots = (long long)std::max(occ, 1) * sms;
-  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
-  int bestS = 1;
-  double best = -1.0;
-  for (int S = 1; S <= c->max_split; S++) {
-    const int chunk = ((c->N + S - 1) / S + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
-    const int Sreal = (c->N + chunk - 1) / chunk;
-    if (Sreal != S) continue;
-    const double waves = (double)tiles * S / (double)slots;
-    const double eff = waves / ceil(waves);
-    // prefer the smallest S within 3% of the best fill, and at least one full wave when possible
-    if (eff > best + 0.03 || (best < 0.97 && eff > best)) {
-      best = eff;
-      bestS = S;
-    }
-    if (waves >= 1.0 && eff >= 0.97) break;
-  }
-  if (const char* e = getenv("RTE_NSPLIT")) bestS = std::max(1, std::min(c->max_split, atoi(e)));
-  const int chunk = ((c->N + bestS - 1) / bestS + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
-  const int S = (c->N + chunk - 1) / chunk;
-  c->splits.push_back({key, S, chunk});
-  *S_out = S;
-  *chunk_out = chunk;
-  return RTE_OK;
-}
+static int check_kernel_err(rte_ctx* c);
 
-// One term on the real basis for nb right-hand sides (layout [N][nb][C]): out = [D] A in.
-// in64 is FP64 (and in32 its FP32 copy for the mixed kernels).  sum != null accumulates the result;
-// d_red receives the norms.
-static int apply_term(rte_ctx* c, const double* in64, const float* in32, double* out, float* out32, double* sum,
-                      int flag, int flag_scat, int nb = 1) {
-  const int LA = flag ? c->L : 0;
-  bool stored = false;
-  int rc = ensure_pair_kernel(c, &stored);
-  if (rc) return rc;
-  int S = 1, chunk = c->N;
-  rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
-  if (rc) return rc;
+// Pair-kernel arguments for nb right-hand sides split S ways (chunk sources per split).
+static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in32, int nb, int S, int chunk) {
   PairArgs a;
   memset(&a, 0, sizeof a);
   a.N = c->N;
@@ -885,6 +851,146 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   a.cstride = (c->C + 1) / 2 * 2;
   a.cpad = (nb * a.cstride + 3) / 4 * 4;
   a.err = c->d_err;
+  return a;
+}
+
+static inline int split_chunk(int N, int S) {
+  return ((N + S - 1) / S + RTE_PAIR_TS - 1) / RTE_PAIR_TS * RTE_PAIR_TS;
+}
+
+// Split-K autotuner.  The pair kernel's grid is (destination tiles) x S source chunks; the best S
+// balances wave quantisation on the 148 SMs against the partial-sum traffic of the epilogue and
+// depends on N, the order, the right-hand-side count and the kernel variant.  Candidates are the
+// splits whose occupancy-model wave fill is within 25% of the best; each is launched on the
+// context's own buffers and timed with CUDA events (best of two), and the winner is kept for the
+// process (every context of that shape on that device reuses it).  RTE_AUTOTUNE=0 keeps the
+// occupancy model's choice; RTE_NSPLIT forces a split.
+namespace {
+using TuneKey = std::tuple<int, int, int, int, int, int, int>;  // device, N, LA, stored, nb, precision, table
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tuned;
+}  // namespace
+
+static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<std::pair<double, int>>& cands,
+                      int* S_best) {
+  const int table = c->model == RTE_MODEL_FIM ? 1 : 0;
+  const double* in64 = nb == 1 ? c->d_W : c->d_bW;
+  const float* in32 = nb == 1 ? c->d_Wf : c->d_bWf;
+  if (!in64 || (c->precision == RTE_PREC_MIXED && !in32)) return RTE_OK;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(c, cudaEventCreate(&e0));
+  CUDA_TRY(c, cudaEventCreate(&e1));
+  double best = 1e30;
+  cudaError_t err = cudaSuccess;
+  for (const auto& cand : cands) {
+    const int S = cand.second;
+    const PairArgs a = pair_args(c, in64, in32, nb, S, split_chunk(c->N, S));
+    float t = 1e30f;
+    for (int rep = 0; rep < 2 && err == cudaSuccess; rep++) {
+      cudaEventRecord(e0, c->st);
+      err = rte_launch_pair(a, LA, c->precision, table, stored, c->st);
+      cudaEventRecord(e1, c->st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0;
+      if (err == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+      if (rep == 1 || cands.size() == 1) t = std::min(t, ms);
+    }
+    c->launches += 2;
+    if (err != cudaSuccess) break;
+    if (t < best) {
+      best = t;
+      *S_best = S;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "split autotuner: %s", cudaGetErrorString(err));
+  return check_kernel_err(c);
+}
+
+static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
+  const int key = ((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0);
+  for (auto& e : c->splits)
+    if (e[0] == key) {
+      *S_out = e[1];
+      *chunk_out = e[2];
+      return RTE_OK;
+    }
+  const int table = c->model == RTE_MODEL_FIM ? 1 : 0;
+  int occ = 0;
+  const int cpad = (nb * ((c->C + 1) / 2 * 2) + 3) / 4 * 4;
+  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, table, stored, nb, cpad, &occ));
+  int sms = 0;
+  CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+  const long long slots = (long long)std::max(occ, 1) * sms;
+  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
+  int bestS = 1;
+  double best = -1.0;
+  std::vector<std::pair<double, int>> fills;  // (wave fill, S) of the realisable splits
+  for (int S = 1; S <= c->max_split; S++) {
+    const int Sreal = (c->N + split_chunk(c->N, S) - 1) / split_chunk(c->N, S);
+    if (Sreal != S) continue;
+    const double waves = (double)tiles * S / (double)slots;
+    const double eff = waves / ceil(waves);
+    fills.push_back({eff, S});
+    // prefer the smallest S within 3% of the best fill, and at least one full wave when possible
+    if (eff > best + 0.03 || (best < 0.97 && eff > best)) {
+      best = eff;
+      bestS = S;
+    }
+  }
+  const char* forced = getenv("RTE_NSPLIT");
+  const char* at = getenv("RTE_AUTOTUNE");
+  const bool tune = !forced && !(at && at[0] == '0') && !c->capturing && c->precision == RTE_PREC_MIXED &&
+                    c->N >= 4096;
+  if (forced) {
+    bestS = std::max(1, std::min(c->max_split, atoi(forced)));
+  } else if (tune) {
+    const TuneKey tk{c->cfg.device, c->N, LA, stored, nb, c->precision, table};
+    bool have = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tuned.find(tk);
+      if (it != g_tuned.end() && it->second <= c->max_split) {
+        bestS = it->second;
+        have = true;
+      }
+    }
+    if (!have) {
+      std::vector<std::pair<double, int>> cands;
+      for (auto& f : fills)
+        if (f.first >= 0.75 * best) cands.push_back(f);
+      std::sort(cands.begin(), cands.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+        return x.first > y.first || (x.first == y.first && x.second < y.second);
+      });
+      if (cands.size() > 5) cands.resize(5);
+      int rc = tune_split(c, LA, stored, nb, cands, &bestS);
+      if (rc) return rc;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tuned[tk] = bestS;
+    }
+  }
+  const int chunk = split_chunk(c->N, bestS);
+  const int S = (c->N + chunk - 1) / chunk;
+  c->splits.push_back({key, S, chunk});
+  *S_out = S;
+  *chunk_out = chunk;
+  return RTE_OK;
+}
+
+// One term on the real basis for nb right-hand sides (layout [N][nb][C]): out = [D] A in.
+// in64 is FP64 (and in32 its FP32 copy for the mixed kernels).  sum != null accumulates the result;
+// d_red receives the norms.
+static int apply_term(rte_ctx* c, const double* in64, const float* in32, double* out, float* out32, double* sum,
+                      int flag, int flag_scat, int nb = 1) {
+  const int LA = flag ? c->L : 0;
+  bool stored = false;
+  int rc = ensure_pair_kernel(c, &stored);
+  if (rc) return rc;
+  int S = 1, chunk = c->N;
+  rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
+  if (rc) return rc;
+  const PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
   {
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
@@ -1961,6 +2067,21 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
 // precompute (for the medium set before the replay), nterms x (pair, self, epilogue) and the final
 // attenuation, recorded once and replayed for every request of this shape.  W0 and S0 must be in
 // graph_w0 / graph_s0 before the replay; the result lands in d_bres (nb > 1) or d_aux2 (nb = 1).
+static std::vector<uintptr_t> graph_signature(const rte_ctx* c, int nb) {
+  auto u = [](const void* p) { return (uintptr_t)p; };
+  const double* W = nb == 1 ? c->d_W : c->d_bW;
+  const double* Wn = nb == 1 ? c->d_Wn : c->d_bWn;
+  return {u(std::min(W, Wn)), u(std::max(W, Wn)), u(nb == 1 ? c->d_sum : c->d_bsum),
+          u(nb == 1 ? c->d_aux2 : c->d_bres), u(nb == 1 ? (const void*)c->d_Wf : (const void*)c->d_bWf),
+          u(c->d_part), u(c->d_selfp), u(c->d_self_idx), u(c->d_self_lut), u(c->d_mom), (uintptr_t)c->K,
+          (uintptr_t)c->self_lut_ok, u(c->d_K), (uintptr_t)c->Kld, u(c->d_mut), u(c->d_mutf), u(c->d_mus),
+          u(c->d_red), u(c->d_err), (uintptr_t)c->bcap};
+}
+
+static bool graph_stale(const rte_ctx* c, int nb, int nterms) {
+  return !c->graph[nb] || c->graph_terms[nb] != nterms || c->graph_sig[nb] != graph_signature(c, nb);
+}
+
 static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
   const int gi = nb;
   const size_t NC = (size_t)c->N * c->C;
@@ -1972,7 +2093,7 @@ static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
   double* res = nb == 1 ? c->d_aux2 : c->d_bres;
   float* Wf = nb == 1 ? c->d_Wf : c->d_bWf;
   const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
-  if (!c->graph[gi] || c->graph_terms[gi] != nterms) {
+  if (graph_stale(c, nb, nterms)) {
     if (c->graph[gi]) {
       cudaGraphExecDestroy(c->graph[gi]);
       c->graph[gi] = nullptr;
@@ -2021,6 +2142,7 @@ static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
     cudaGraphDestroy(g);
     if (e3 != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "graph instantiate: %s", cudaGetErrorString(e3));
     c->graph_terms[gi] = nterms;
+    c->graph_sig[gi] = graph_signature(c, nb);
   }
   (void)NC;
   c->launches += 4 * nterms + 4;
@@ -2060,8 +2182,9 @@ static int forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, int nterm
   cudaEvent_t t0 = c->ev_graph[0], t1 = c->ev_graph[1];
   CUDA_TRY(c, cudaEventRecord(t0, c->st));
   double* dres = nullptr;
-  if (!c->graph[nb] || c->graph_terms[nb] != nterms) {
-    // first request of this shape: record the graph on zero inputs, then run the real one
+  if (graph_stale(c, nb, nterms)) {
+    // first request of this shape (or buffers moved since the recording): record the graph on zero
+    // inputs, then run the real one
     double* w = nb == 1 ? c->d_W : c->d_bW;
     double* sm = nb == 1 ? c->d_sum : c->d_bsum;
     CUDA_TRY(c, cudaMemsetAsync(w, 0, NC * nb * sizeof(double), c->st));

@@ -138,3 +138,25 @@ def test_graph_replay_matches_batched_solve(rte, nsrc):
         for b in range(nsrc):
             assert rel(tr[b], ref["trans"][b]) < 1e-9 and rel(rf[b], ref["ref"][b]) < 1e-9, (seed, b)
     ctx.close()
+
+
+def test_graph_rerecords_when_buffers_move(rte):
+    """One context, media whose self-term tables outgrow their buffers (1, 3, 40 distinct mu_t, then
+    per-voxel random values that take the power-series path) and a batch size that grows the batch
+    buffers (1, 2, 4, 2, 1 sources): every replay must match the un-graphed batched solve."""
+    n, L, T = 17, 3, 6  # 17^3 > 4096 voxels: per-voxel random values leave the table path
+    N = n ** 3
+    ctx = _ctx(rte, n, L, 1)
+    rng = np.random.default_rng(4)
+    uni = (np.full(N, 0.01), np.full(N, 1.0))
+    sph = rte.sphere_phantom(n, nspheres=2, seed=9, rmin=0.15, rmax=0.3)[:2]
+    few = (rng.choice(rng.uniform(0.005, 0.05, 40), N), np.full(N, 1.2))
+    many = (rng.uniform(0.005, 0.05, N), rng.uniform(0.5, 2.0, N))
+    srcs = [_face_source(rte, n, f, 7, 11, rte.SRC_BEAM if f % 2 == 0 else rte.SRC_POINT) for f in range(4)]
+    for (mua, mus), nsrc in zip((uni, sph, few, many, sph), (1, 2, 4, 2, 1)):
+        ctx.set_medium_voxel(mua, mus)
+        tr, rf, _ = ctx.forward_graph(srcs[:nsrc], T)
+        ref = ctx.forward_batch(srcs[:nsrc], rte.Stop(rte.STOP_FIXED, T), want_W=False)
+        for b in range(nsrc):
+            assert rel(tr[b], ref["trans"][b]) < 1e-9 and rel(rf[b], ref["ref"][b]) < 1e-9, (nsrc, b)
+    ctx.close()
