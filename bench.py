@@ -238,6 +238,20 @@ def run_serve(args, dev):
                    "face; warm-up: one uncounted request of every (grid, order) shape"}
 
 
+def hbm_line(traffic, avg_ms):
+    """The pair kernel's DRAM bytes per launch (ncu) over its live launch time, against the measured
+    HBM copy bandwidth: how far the kernel is from being memory-bound."""
+    if not traffic:
+        return None
+    peak = None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        peak = json.load(open(mp)).get("hbm_gbs")
+    gbs = traffic / (avg_ms * 1e-3) / 1e9
+    return {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak if peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peak else None}
+
+
 def run_ours(args):
     import torch
     import doi_b200 as R
@@ -370,7 +384,8 @@ def run_ours(args):
                          "traffic": traffic, "kernel": "k_pair_mixed<5,stored>" if prec == R.PREC_MIXED
                          else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
                          "flop_per_launch": apply_flop, "rhs_per_launch": nbk,
-                         "peak_source": "measured by rte_measure_fma_peak (8-chain FMA probe) in this run"},
+                         "peak_source": "measured by rte_measure_fma_peak (8-chain FMA probe) in this run",
+                         "hbm": hbm_line(traffic, avg_pair_ms)},
             "cpu_baseline": None,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": st["launches"],
