@@ -238,6 +238,127 @@ def run_serve(args, dev):
                    "face; warm-up: one uncounted request of every (grid, order) shape"}
 
 
+CFG1_PAR = """[Runtime]
+TransFile = trans.out
+ReflectFile = ref.out
+PhaseFile = phase.out
+[Algorithm]
+nL = 3
+nTerms = 30
+[Geometry]
+nX = 11
+nY = 11
+nZ = 11
+xMin = -0.55
+xMax = 0.55
+yMin = -0.55
+yMax = 0.55
+zMin = 0
+zMax = 1.1
+propThresh = 10
+[Phantom]
+mua = 0.01
+mus = 1.0
+g = 0.8
+n = 1.0
+c = 1.0
+[Source]
+posX = 0
+posY = 0
+diam = 0.1
+magnitude = 1.0
+"""
+
+
+def run_cfg1(dev):
+    """The plain FP64 method on the uniform 11^3, L=3 case: GPU solve with the relative-L2 rule (1e-7 or
+    30 terms) plus the 6-face flux, and the CPU package itself (oracle/_ref/rte_cpu, built from the
+    reference sources) on the same input with its own stop rule, timed on the host cores; the GPU run
+    with the package's stop rule is compared with the package's images."""
+    import doi_b200 as R
+    n, L = 11, 3
+    N = n ** 3
+    ctx = R.Context(n, n, n, dx=0.1, nL=L, g=0.8, n=1.0, c=1.0, prop_thresh=10.0, model=R.MODEL_CPU,
+                    precision=R.PREC_FP64, device=dev)
+    ctx.set_medium_voxel(np.full(N, 0.01), np.full(N, 1.0))
+    src = R.Source(diam=0.1, kind=R.SRC_CPU)
+    out = {"workload": "11^3 uniform (mu_a 0.01, mu_s 1, g 0.8), L=3, centre pencil, CPU-package model, FP64"}
+    ctx.forward(src, R.Stop(R.STOP_REL_L2, 30, 1e-7))  # warm-up
+    t = time.perf_counter()
+    r = ctx.forward(src, R.Stop(R.STOP_REL_L2, 30, 1e-7))
+    flux = ctx.detector_flux([src], R.Stop(R.STOP_REL_L2, 30, 1e-7), R.Detector(nbins=n, faces=63))
+    out["gpu_wall_ms"] = (time.perf_counter() - t) * 1e3
+    out["gpu_solve_ms_device"] = r["ms_device"]
+    out["gpu_terms_rel_l2_1e-7"] = r["terms"]
+    out["six_face_flux_total"] = float(flux.sum())
+    ref_rule = ctx.forward(src, R.Stop(R.STOP_REFERENCE))
+    ctx.close()
+    exe = os.path.join(ROOT, "oracle", "_ref", "rte_cpu")
+    if not os.path.exists(exe):
+        out["cpu_package"] = None
+        return out
+    d = tempfile.mkdtemp(prefix="cfg1_")
+    open(os.path.join(d, "c.par"), "w").write(CFG1_PAR)
+    t = time.perf_counter()
+    pr = subprocess.run([exe, "c.par"], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    wall = time.perf_counter() - t
+    if pr.returncode != 0:
+        out["cpu_package"] = {"error": pr.stdout[-300:]}
+        return out
+
+    def img(path):
+        b = open(path, "rb").read()
+        nx, ny = np.frombuffer(b[:8], np.int32)
+        v = np.frombuffer(b[8:], np.float64)
+        return (v[: nx * ny] + 1j * v[nx * ny: 2 * nx * ny]).reshape(ny, nx)
+
+    terms = [ln for ln in pr.stdout.splitlines() if ln.startswith("Neumann series:")]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["cpu_package"] = {"wall_s": wall, "cores": os.cpu_count(), "threads": "OpenMP, all host cores",
+                          "terms_own_rule": int(terms[-1].split()[-1]) - 1 if terms else None,
+                          "gpu_terms_same_rule": ref_rule["terms"],
+                          "rel_l2_trans": rel(ref_rule["trans"], img(os.path.join(d, "trans.out"))),
+                          "rel_l2_ref": rel(ref_rule["ref"], img(os.path.join(d, "ref.out")))}
+    return out
+
+
+def run_grad(dev):
+    """Adjoint gradient at the 33^3, L=5 phantom: 4 collimated z=0 sources at (+-0.825, +-0.825) cm,
+    8x8 bins on each of the 6 faces, target flux from the phantom with every sphere's coefficients
+    scaled by (1 + 0.05 N(0,1)); cost of rte_gradient against the forward solves it differentiates."""
+    import doi_b200 as R
+    from doi_b200.phantoms import sphere_phantom
+    mua, mus, sph = sphere_phantom(N_SIDE, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=3, seed=4)
+    rng = np.random.default_rng(44)
+    pa, ps = mua.copy(), mus.copy()
+    for sp in sph:  # perturb each inclusion's values
+        ka, ks = 1 + 0.05 * rng.standard_normal(2)
+        pa[mua == sp["mua"]] *= ka
+        ps[mus == sp["mus"]] *= ks
+    ctx = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_MIXED,
+                    kernel_mode=R.KERNEL_STORE, device=dev)
+    srcs = [R.Source(pos_x=x, pos_y=y, kind=R.SRC_COLUMN) for x, y in
+            ((-0.825, -0.825), (0.825, -0.825), (-0.825, 0.825), (0.825, 0.825))]
+    stop = R.Stop(R.STOP_FIXED, TERMS)
+    det = R.Detector(nbins=8, faces=63)
+    ctx.set_medium_voxel(pa, ps)
+    target = ctx.detector_flux(srcs, stop, det)
+    ctx.set_medium_voxel(mua, mus)
+    ctx.detector_flux(srcs[:1], stop, det)
+    ctx.gradient(srcs[:1], stop, det, target[:1])  # warm-up (autotuner, buffers)
+    t = time.perf_counter()
+    ctx.detector_flux(srcs, stop, det)
+    t_fwd = time.perf_counter() - t
+    t = time.perf_counter()
+    loss, ga, gs = ctx.gradient(srcs, stop, det, target)
+    t_grad = time.perf_counter() - t
+    ctx.close()
+    return {"workload": "33^3 L=5 phantom, 4 z=0 sources, 8x8 bins x 6 faces, 20 terms, mixed precision",
+            "forward_s_4src": t_fwd, "gradient_s_4src": t_grad, "ratio_gradient_over_forward": t_grad / t_fwd,
+            "loss": loss, "grad_norm_mua": float(np.linalg.norm(ga)), "grad_norm_mus": float(np.linalg.norm(gs)),
+            "check": "central finite differences on 50 voxels (step 1e-4 rel) in tests/test_gpu_gradient.py"}
+
+
 def hbm_line(traffic, avg_ms):
     """The pair kernel's DRAM bytes per launch (ncu) over its live launch time, against the measured
     HBM copy bandwidth: how far the kernel is from being memory-bound."""
@@ -399,6 +520,9 @@ def run_ours(args):
         }
         if ws == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(args.ref_seconds)
+        if not args.skip_extras:
+            line["config1_plain_fp64"] = run_cfg1(dev)
+            line["config4_gradient"] = run_grad(dev)
         if args.serve_requests > 0:
             line["serve"] = run_serve(args, dev)
         out = line
@@ -424,6 +548,7 @@ def main():
     ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
     ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
                     help="sources per phantom solved together (1 = one source per solve)")
+    ap.add_argument("--skip-extras", action="store_true", help="skip the config-1 and gradient measurements")
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
     ap.add_argument("--serve-rate", type=float, default=1.5,

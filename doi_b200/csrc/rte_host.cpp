@@ -358,6 +358,8 @@ struct rte_ctx {
   // signature differs from the context's current one (a buffer was reallocated, the self-term path
   // or its series length changed with the medium) is recorded again before it is replayed
   std::vector<uintptr_t> graph_sig[5];
+  void* d_Qbp = nullptr;        // gradient: weight of every unordered voxel pair (N x round32(N))
+  size_t qbp_bytes = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
   // measurement: launch count and per-class event pairs (0 pair, 1 store, 2 epilogue)
@@ -448,7 +450,8 @@ static void free_all(rte_ctx* c) {
                 c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img,
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
-                c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq};
+                c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq,
+                c->d_Qbp};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1859,9 +1862,12 @@ static int check_detector(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   if (d->nbins < 1 || d->nbins > 1024 || d->faces <= 0 || d->faces > 63) return fail(c, RTE_ERR_ARG, "bad detector");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   if (stop->rule == RTE_STOP_REFERENCE) return fail(c, RTE_ERR_UNSUPPORTED, "detectors take a fixed or relative-L2 stop rule");
-  for (int q = 0; q < nsrc; q++)
-    if (srcs[q].kind == RTE_SRC_CPU) return fail(c, RTE_ERR_UNSUPPORTED, "detectors support single-column sources");
-  (void)0;
+  for (int q = 0; q < nsrc; q++) {
+    std::vector<int> cols;
+    double scale;
+    if (source_columns(c, &srcs[q], cols, scale)) return fail(c, RTE_ERR_ARG, "bad source %d", q);
+    if (cols.size() > 1) return fail(c, RTE_ERR_UNSUPPORTED, "detectors support single-column sources");
+  }
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   return ensure_detector_buffers(c);
 }
@@ -1888,6 +1894,54 @@ extern "C" int rte_detector_flux(rte_ctx* c, int nsrc, const rte_source* srcs, c
 //   y = e + D lambda;
 //   dL/dmu_t(v) = -sum_{pairs} len(v) k (y.R)(R.S) + (dV/cm) y_v . dDself/dmu S_v;
 //   dL/dmu_s(v) += lambda_v . scat_l (A S)_v;   plus the source column and ballistic terms.
+// Arguments of the back-projection passes; the pair-weight buffer (N x ld, FP32 for the mixed
+// precision path, FP64 otherwise) is allocated on first use and kept with the context.
+static BpArgs bp_args(rte_ctx* c, bool accumulate) {
+  BpArgs bp;
+  memset(&bp, 0, sizeof bp);
+  bp.N = c->N;
+  bp.nx = c->nx;
+  bp.ny = c->ny;
+  bp.nz = c->nz;
+  bp.Cfull = c->C;
+  bp.dx = c->dx;
+  bp.dy = c->dy;
+  bp.dz = c->dz;
+  bp.prop_thresh = c->prop_thresh;
+  bp.kscale = c->dV / c->cm;
+  bp.perm = c->d_perm;
+  bp.islot = c->d_islot;
+  bp.mut = c->d_mut;
+  bp.mutf = c->d_mutf;
+  bp.y = c->d_y;
+  bp.S = c->d_S;
+  bp.Kmat = c->K_valid && c->d_K ? c->d_K : nullptr;
+  bp.Kld = ((size_t)c->N + 31) / 32 * 32;
+  bp.g = c->d_gt;
+  bp.Q = c->d_Qbp;
+  bp.accumulate = accumulate ? 1 : 0;
+  return bp;
+}
+
+static int ensure_bp_buffer(rte_ctx* c) {
+  const size_t ld = ((size_t)c->N + 31) / 32 * 32;
+  const size_t need = (size_t)c->N * ld * (c->precision == RTE_PREC_MIXED ? sizeof(float) : sizeof(double));
+  if (c->d_Qbp && c->qbp_bytes >= need) return RTE_OK;
+  if (c->d_Qbp) {
+    cudaFree(c->d_Qbp);
+    c->bytes -= c->qbp_bytes;
+    c->d_Qbp = nullptr;
+  }
+  size_t fr = 0, tot = 0;
+  CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
+  if (need + (1ull << 30) > fr)
+    return fail(c, RTE_ERR_NOMEM, "gradient pair weights need %.1f GB, %.1f GB free", need / 1e9, fr / 1e9);
+  CUDA_TRY(c, cudaMalloc(&c->d_Qbp, need));
+  c->qbp_bytes = need;
+  c->bytes += need;
+  return RTE_OK;
+}
+
 extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
                             const rte_detector* d, const double* target, double* loss, double* g_mua,
                             double* g_mus) {
@@ -1912,6 +1966,8 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
   std::vector<double> mut(c->N), mus(c->N);
   CUDA_TRY(c, cudaMemcpy(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
   CUDA_TRY(c, cudaMemcpy(mus.data(), c->d_mus, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  rc = ensure_bp_buffer(c);
+  if (rc) return rc;
   for (int sidx = 0; sidx < nsrc; sidx++) {
     const rte_source* s = &srcs[sidx];
     int terms = 0;
@@ -1953,40 +2009,12 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
     if (rc) return rc;
     CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_lam, c->N, c->L, c->C, c->st)));
     CUDA_TRY(c, (c->launches++, rte_launch_y_field(c->d_y, c->d_e, c->d_lam, c->d_mus, scat, c->N, c->L, c->C, c->st)));
-    // back-projection through exp(-tau)
-    BpArgs bp;
-    memset(&bp, 0, sizeof bp);
-    bp.N = c->N;
-    bp.nx = c->nx;
-    bp.ny = c->ny;
-    bp.nz = c->nz;
-    bp.Cfull = c->C;
-    bp.dx = c->dx;
-    bp.dy = c->dy;
-    bp.dz = c->dz;
-    bp.prop_thresh = c->prop_thresh;
-    bp.kscale = c->dV / c->cm;
-    bp.perm = c->d_perm;
-    bp.islot = c->d_islot;
-    bp.mut = c->d_mut;
-    bp.mutf = c->d_mutf;
-    bp.y = c->d_y;
-    bp.S = c->d_S;
-    bool stored = false;
-    rc = ensure_pair_kernel(c, &stored);
-    if (rc) return rc;
-    bp.Kmat = stored ? c->d_K : nullptr;
-    bp.Kld = c->Kld;
-    bp.g = c->d_gt;
-    const size_t accb = (size_t)c->N * (mixed ? sizeof(float) : sizeof(double));
-    bp.use_smem = accb <= 200 * 1024 ? 1 : 0;
-    const int tiles = (c->N + RTE_BP_THREADS - 1) / RTE_BP_THREADS;
-    int S = std::max(1, std::min(16, (4 * 148 + tiles - 1) / tiles));
-    bp.chunk = (c->N + S - 1) / S;
-    bp.nsplit = (c->N + bp.chunk - 1) / bp.chunk;
+    // back-projection through exp(-tau), pass 1: this source's weight of every unordered pair,
+    // summed over the sources in the pair-weight buffer (pass 2, the walk, follows the loop)
+    BpArgs bp = bp_args(c, sidx > 0);
     {
       ProfScope ps(c, 0);
-      CUDA_TRY(c, rte_launch_backproject(bp, c->L, mixed ? 0 : 1, c->st));
+      CUDA_TRY(c, (c->launches++, rte_launch_bp_weights(bp, c->L, mixed ? 0 : 1, c->st)));
     }
     GradLocalArgs gl;
     memset(&gl, 0, sizeof gl);
@@ -2047,6 +2075,11 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
         tail += Lam[i] * X[i];
       }
     }
+  }
+  {  // back-projection pass 2: one walk of every unordered pair for all sources together
+    const BpArgs bp = bp_args(c, true);
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, (c->launches++, rte_launch_bp_walk(bp, mixed ? 0 : 1, c->st)));
   }
   std::vector<double> gt(c->N), gs(c->N);
   CUDA_TRY(c, cudaMemcpyAsync(gt.data(), c->d_gt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));

@@ -8,7 +8,6 @@
 #define RTE_PAIR_THREADS 128  // destination voxels per CTA (one per thread)
 #define RTE_PAIR_TS 64        // source voxels staged in shared memory per step
 #define RTE_MAX_MOM 48        // self-term power-series terms
-#define RTE_BP_THREADS 256    // destination voxels per CTA of the back-projection
 
 struct PairArgs {
   int N, nx, ny, nz, Cfull;
@@ -113,8 +112,9 @@ struct BpArgs {
   const float* Kmat;   // stored pair kernel (null: recompute the path integral)
   size_t Kld;
   double* g;           // gradient w.r.t. mu_t, accumulated [N]
-  int chunk, nsplit;
-  int use_smem;        // per-CTA private accumulator of N entries in shared memory
+  int use_smem;        // per-CTA private accumulator of N entries in shared memory (set by the launcher)
+  void* Q;             // per unordered pair weight [source slot][destination slot] (row stride Kld), T
+  int accumulate;      // k_bp_weights: add to Q (later sources) instead of overwriting
 };
 
 struct GradLocalArgs {
@@ -143,7 +143,10 @@ cudaError_t rte_launch_parity(double* x, int N, int L, int vstride, cudaStream_t
 cudaError_t rte_launch_axpy(double* y, const double* x, double alpha, size_t n, cudaStream_t st);
 cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, const double* mus, const double* scat,
                                int N, int L, int Cfull, cudaStream_t st);
-cudaError_t rte_launch_backproject(const BpArgs& a, int LA, int fp64, cudaStream_t st);
+// Symmetric back-projection in two passes: pair weights of one source added into Q, then one walk
+// over every unordered pair scattering Q * length into the gradient.
+cudaError_t rte_launch_bp_weights(const BpArgs& a, int LA, int fp64, cudaStream_t st);
+cudaError_t rte_launch_bp_walk(const BpArgs& a, int fp64, cudaStream_t st);
 cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st);
 // message returned by rte_last_error(NULL) on this thread
 __attribute__((visibility("hidden"))) void rte_set_global_error(const char* msg);

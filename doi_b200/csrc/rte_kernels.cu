@@ -23,6 +23,8 @@
 
 #include <string.h>
 
+#include <algorithm>
+
 #include <type_traits>
 
 #include "rte_internal.h"
@@ -903,85 +905,169 @@ __device__ __forceinline__ void path_walk(int i, int j, int k, int ip, int jp, i
   add(v, Q - prev);
 }
 
-// Back-projection for the gradient w.r.t. mu_t:
-//   g(v) -= sum_{r != r'} len_rr'(v) k_rr' (y_r . R(w)) (R(w) . S_r'),   w = (r - r')/|r - r'|,
-// the derivative of y^T A S through exp(-tau).  One thread per destination voxel r (slot order),
-// sources of one split-K chunk in voxel order; k from the stored pair kernel (FP32) or recomputed
-// (FP64); each CTA accumulates into a private copy of g in shared memory when it fits, then adds
-// it to the global FP64 gradient.
+// ---------------------------------------------------------------------------------------------
+// Symmetric back-projection.  The path between voxels r and r' is the same set of segments in
+// both directions, so each unordered pair is walked once with the weight of both ordered pairs:
+//   w(r, r') = k [ (y_r . R(w)) (R(w) . S_r') + (y_r' . P R(w)) (P R(w) . S_r) ],
+// w = (r - r') / |r - r'|, P R(w) = R(-w) = (-1)^l R(w).  Pass 1 (k_bp_weights, once per source,
+// summed into Q) evaluates the weights on 64 x 64 tiles of the upper triangle in slot order; pass 2
+// (k_bp_walk, once per gradient) walks every pair with w != 0 and adds -w * length to each voxel on
+// the path, into a shared-memory copy of the whole gradient per CTA when it fits.
+__host__ __device__ constexpr int l_of_c(int c) {
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  return l;
+}
+
+__device__ __forceinline__ void tri_tile(long long t, int& bd, int& bs) {
+  bd = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
+  while ((long long)(bd + 1) * (bd + 2) / 2 <= t) ++bd;
+  while ((long long)bd * (bd + 1) / 2 > t) --bd;
+  bs = (int)(t - (long long)bd * (bd + 1) / 2);
+}
+
 template <int LA, typename T>
-__global__ void __launch_bounds__(RTE_BP_THREADS) k_backproject(BpArgs a) {
+__global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* gsh = reinterpret_cast<T*>(smem_raw);
+  T* ys = reinterpret_cast<T*>(smem_raw);             // [64][C] y of the tile's sources
+  T* Ss = ys + RTE_KT * C;                             // [64][C] S of the tile's sources
+  int* sx = reinterpret_cast<int*>(Ss + RTE_KT * C);   // [64][3] source coordinates
+  const int ntile = (a.N + RTE_KT - 1) / RTE_KT;
+  int bd, bs;
+  tri_tile(blockIdx.x, bd, bs);
+  if (bd >= ntile) return;
   const int tid = threadIdx.x;
-  if (a.use_smem) {
-    for (int v = tid; v < a.N; v += RTE_BP_THREADS) gsh[v] = T(0);
-    __syncthreads();
-  }
-  const int slot = blockIdx.x * RTE_BP_THREADS + tid;
-  const bool act = slot < a.N;
-  const int r = act ? a.perm[slot] : 0;
   const int plane = a.nx * a.ny;
-  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
-  T y[C];
+  const int s0 = bs * RTE_KT, d0 = bd * RTE_KT;
+  {
+    const int sl = s0 + tid;
+    const int v = sl < a.N ? a.perm[sl] : 0;
+    sx[tid * 3 + 0] = v % a.nx;
+    sx[tid * 3 + 1] = (v / a.nx) % a.ny;
+    sx[tid * 3 + 2] = v / plane;
+  }
+  for (int e = tid; e < RTE_KT * C; e += RTE_KT) {  // row by row: neighbouring threads, neighbouring c
+    const int q = e / C, c = e % C;
+    const int sl = s0 + q;
+    const size_t off = sl < a.N ? (size_t)a.perm[sl] * a.Cfull + c : 0;
+    ys[e] = sl < a.N ? (T)a.y[off] : T(0);
+    Ss[e] = sl < a.N ? (T)a.S[off] : T(0);
+  }
+  __syncthreads();
+  const int d = d0 + tid;
+  if (d >= a.N) return;
+  const int r = a.perm[d];
+  const int k = r % a.nx, j = (r / a.nx) % a.ny, i = r / plane;
+  T yd[C], Sd[C];
 #pragma unroll
-  for (int c = 0; c < C; ++c) y[c] = act ? (T)a.y[(size_t)r * a.Cfull + c] : T(0);
-  const int sb = blockIdx.y * a.chunk;
-  const int se = min(a.N, sb + a.chunk);
-  if (act) {
-    int kp = sb % a.nx, jp = (sb / a.nx) % a.ny, ip = sb / plane;
-    for (int rp = sb; rp < se; ++rp) {
-      if (rp != r) {
-        const T ddx = (T)(k - kp) * (T)a.dx, ddy = (T)(j - jp) * (T)a.dy, ddz = (T)(i - ip) * (T)a.dz;
-        const T d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-        const T dist = sqrt(d2);
-        if (dist < (T)a.prop_thresh) {
-          T kk;
-          if (a.Kmat) {
-            kk = (T)__ldg(a.Kmat + (size_t)a.islot[rp] * a.Kld + slot);
-          } else {
-            int Q0;
-            const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q0);
-            kk = exp(-ps * dist / (T)Q0) * (T)a.kscale / d2;
-          }
-          const T inv = T(1) / dist;
-          T R[C];
-          sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
-          T yr = 0, sr = 0;
-          const double* Sp = a.S + (size_t)rp * a.Cfull;
-#pragma unroll
-          for (int c = 0; c < C; ++c) {
-            yr = fma(y[c], R[c], yr);
-            sr = fma(R[c], (T)__ldg(Sp + c), sr);
-          }
-          const T q = kk * yr * sr;
-          if (q != T(0)) {
-            int Q = 1;
-            // lengths arrive scaled by Q/dist; coef restores them
-            const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
-            const T coef = -q * dist / (T)(2 * max(Dx, 1) * max(Dy, 1) * max(Dz, 1));
-            if (a.use_smem)
-              path_walk(i, j, k, ip, jp, kp, a.nx, plane, Q, [&](int v, int len) { atomicAdd(gsh + v, coef * (T)len); });
-            else
-              path_walk(i, j, k, ip, jp, kp, a.nx, plane, Q,
-                        [&](int v, int len) { atomicAdd(a.g + v, (double)(coef * (T)len)); });
-          }
-        }
+  for (int c = 0; c < C; ++c) {
+    yd[c] = (T)a.y[(size_t)r * a.Cfull + c];
+    Sd[c] = (T)a.S[(size_t)r * a.Cfull + c];
+  }
+  const T dxf = (T)a.dx, dyf = (T)a.dy, dzf = (T)a.dz, thr = (T)a.prop_thresh, ks = (T)a.kscale;
+  T* Qp = reinterpret_cast<T*>(a.Q);
+  const int qend = bs == bd ? tid : RTE_KT;  // diagonal tile: each unordered pair once (source slot < destination slot)
+  for (int q = 0; q < qend; ++q) {
+    const int sl = s0 + q;
+    if (sl >= a.N) break;
+    const int kp = sx[q * 3 + 0], jp = sx[q * 3 + 1], ip = sx[q * 3 + 2];
+    const T ddx = (T)(k - kp) * dxf, ddy = (T)(j - jp) * dyf, ddz = (T)(i - ip) * dzf;
+    const T d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+    const T dist = sqrt(d2);
+    T w = T(0);
+    if (d2 > T(0) && dist < thr) {
+      T kk;
+      if (a.Kmat) {
+        kk = (T)__ldg(a.Kmat + (size_t)sl * a.Kld + d);
+      } else {
+        int Q0;
+        const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q0);
+        kk = exp(-ps * dist / (T)Q0) * ks / d2;
       }
-      if (++kp == a.nx) {
-        kp = 0;
-        if (++jp == a.ny) {
-          jp = 0;
-          ++ip;
-        }
+      const T inv = T(1) / dist;
+      T R[C];
+      sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
+      const T* yq = ys + q * C;
+      const T* Sq = Ss + q * C;
+      T a1 = T(0), b1 = T(0), a2 = T(0), b2 = T(0);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const T Rp = (l_of_c(c) & 1) ? -R[c] : R[c];
+        a1 = fma(yd[c], R[c], a1);
+        b1 = fma(R[c], Sq[c], b1);
+        a2 = fma(yq[c], Rp, a2);
+        b2 = fma(Rp, Sd[c], b2);
+      }
+      w = kk * (a1 * b1 + a2 * b2);
+    }
+    const size_t idx = (size_t)sl * a.Kld + d;
+    Qp[idx] = a.accumulate ? Qp[idx] + w : w;
+  }
+}
+
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+#define RTE_BPW_THREADS 512
+template <typename T>
+__global__ void __launch_bounds__(RTE_BPW_THREADS) k_bp_walk(BpArgs a) {
+  constexpr int G = RTE_BPW_THREADS / RTE_KT;  // independent 64-thread groups, one tile each
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int* sx = reinterpret_cast<int*>(smem_raw);                          // [G][64][3]
+  T* acc = reinterpret_cast<T*>(smem_raw + G * RTE_KT * 3 * sizeof(int));  // [N] when use_smem
+  const int tid = threadIdx.x, grp = tid / RTE_KT, lane = tid % RTE_KT;
+  if (a.use_smem)
+    for (int v = tid; v < a.N; v += RTE_BPW_THREADS) acc[v] = T(0);
+  __syncthreads();
+  const int plane = a.nx * a.ny;
+  const int ntile = (a.N + RTE_KT - 1) / RTE_KT;
+  const long long ntri = (long long)ntile * (ntile + 1) / 2;
+  const T* Qp = reinterpret_cast<const T*>(a.Q);
+  int* gx = sx + grp * RTE_KT * 3;
+  for (long long t = (long long)blockIdx.x * G + grp; t < ntri; t += (long long)gridDim.x * G) {
+    int bd, bs;
+    tri_tile(t, bd, bs);
+    const int s0 = bs * RTE_KT, d0 = bd * RTE_KT;
+    {
+      const int sl = s0 + lane;
+      const int v = sl < a.N ? a.perm[sl] : 0;
+      gx[lane * 3 + 0] = v % a.nx;
+      gx[lane * 3 + 1] = (v / a.nx) % a.ny;
+      gx[lane * 3 + 2] = v / plane;
+    }
+    group_sync(grp + 1, RTE_KT);
+    const int d = d0 + lane;
+    if (d < a.N) {
+      const int r = a.perm[d];
+      const int k = r % a.nx, j = (r / a.nx) % a.ny, i = r / plane;
+      const int qend = bs == bd ? lane : RTE_KT;
+      for (int q = 0; q < qend; ++q) {
+        const int sl = s0 + q;
+        if (sl >= a.N) break;
+        const T w = Qp[(size_t)sl * a.Kld + d];
+        if (w == T(0)) continue;
+        const int kp = gx[q * 3 + 0], jp = gx[q * 3 + 1], ip = gx[q * 3 + 2];
+        const T ddx = (T)(k - kp) * (T)a.dx, ddy = (T)(j - jp) * (T)a.dy, ddz = (T)(i - ip) * (T)a.dz;
+        const T dist = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+        const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
+        // lengths arrive scaled by Q / dist, Q = 2 max(Dx,1) max(Dy,1) max(Dz,1)
+        const T coef = -w * dist / (T)(2 * max(Dx, 1) * max(Dy, 1) * max(Dz, 1));
+        int Qw = 1;
+        if (a.use_smem)
+          path_walk(i, j, k, ip, jp, kp, a.nx, plane, Qw, [&](int v, int len) { atomicAdd(acc + v, coef * (T)len); });
+        else
+          path_walk(i, j, k, ip, jp, kp, a.nx, plane, Qw,
+                    [&](int v, int len) { atomicAdd(a.g + v, (double)(coef * (T)len)); });
       }
     }
+    group_sync(grp + 1, RTE_KT);  // the group's coordinates are overwritten by its next tile
   }
   if (a.use_smem) {
     __syncthreads();
-    for (int v = tid; v < a.N; v += RTE_BP_THREADS) {
-      const T x = gsh[v];
+    for (int v = tid; v < a.N; v += RTE_BPW_THREADS) {
+      const T x = acc[v];
       if (x != T(0)) atomicAdd(a.g + v, (double)x);
     }
   }
@@ -1324,32 +1410,55 @@ cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, co
 }
 
 template <int LA, typename T>
-static cudaError_t launch_bp(const BpArgs& a, cudaStream_t st) {
-  const size_t smem = a.use_smem ? (size_t)a.N * sizeof(T) : 0;
-  cudaError_t e = cudaFuncSetAttribute(k_backproject<LA, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static cudaError_t launch_bpw(const BpArgs& a, cudaStream_t st) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  const size_t smem = (size_t)RTE_KT * C * 2 * sizeof(T) + RTE_KT * 3 * sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(k_bp_weights<LA, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((a.N + RTE_BP_THREADS - 1) / RTE_BP_THREADS, a.nsplit);
-  k_backproject<LA, T><<<grid, RTE_BP_THREADS, smem, st>>>(a);
+  const long long nt = (a.N + RTE_KT - 1) / RTE_KT;
+  k_bp_weights<LA, T><<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int LA>
-static cudaError_t launch_bp_LA(const BpArgs& a, int fp64, cudaStream_t st) {
-  return fp64 ? launch_bp<LA, double>(a, st) : launch_bp<LA, float>(a, st);
+static cudaError_t launch_bpw_LA(const BpArgs& a, int fp64, cudaStream_t st) {
+  return fp64 ? launch_bpw<LA, double>(a, st) : launch_bpw<LA, float>(a, st);
 }
 
-cudaError_t rte_launch_backproject(const BpArgs& a, int LA, int fp64, cudaStream_t st) {
+cudaError_t rte_launch_bp_weights(const BpArgs& a, int LA, int fp64, cudaStream_t st) {
   switch (LA) {
-    case 0: return launch_bp_LA<0>(a, fp64, st);
-    case 1: return launch_bp_LA<1>(a, fp64, st);
-    case 2: return launch_bp_LA<2>(a, fp64, st);
-    case 3: return launch_bp_LA<3>(a, fp64, st);
-    case 4: return launch_bp_LA<4>(a, fp64, st);
-    case 5: return launch_bp_LA<5>(a, fp64, st);
-    case 6: return launch_bp_LA<6>(a, fp64, st);
-    case 7: return launch_bp_LA<7>(a, fp64, st);
+    case 0: return launch_bpw_LA<0>(a, fp64, st);
+    case 1: return launch_bpw_LA<1>(a, fp64, st);
+    case 2: return launch_bpw_LA<2>(a, fp64, st);
+    case 3: return launch_bpw_LA<3>(a, fp64, st);
+    case 4: return launch_bpw_LA<4>(a, fp64, st);
+    case 5: return launch_bpw_LA<5>(a, fp64, st);
+    case 6: return launch_bpw_LA<6>(a, fp64, st);
+    case 7: return launch_bpw_LA<7>(a, fp64, st);
   }
   return cudaErrorInvalidValue;
+}
+
+template <typename T>
+static cudaError_t launch_walk(BpArgs a, cudaStream_t st) {
+  const size_t base = (size_t)(RTE_BPW_THREADS / RTE_KT) * RTE_KT * 3 * sizeof(int);
+  int dev = 0, maxsm = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  a.use_smem = base + (size_t)a.N * sizeof(T) <= (size_t)maxsm ? 1 : 0;
+  const size_t smem = base + (a.use_smem ? (size_t)a.N * sizeof(T) : 0);
+  cudaError_t e = cudaFuncSetAttribute(k_bp_walk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bp_walk<T>, RTE_BPW_THREADS, smem);
+  if (e != cudaSuccess) return e;
+  k_bp_walk<T><<<(unsigned)(std::max(per_sm, 1) * sms), RTE_BPW_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_bp_walk(const BpArgs& a, int fp64, cudaStream_t st) {
+  return fp64 ? launch_walk<double>(a, st) : launch_walk<float>(a, st);
 }
 
 cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st) {
