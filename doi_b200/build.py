@@ -11,7 +11,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librte_b200.so")
-SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp"]
+BINDIR = os.path.join(HERE, "bin")
+SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp", "rte_par.cpp"]
+CLI = "rte_cli.cpp"  # built into bin/ by build_cli, not into the library
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -26,6 +28,8 @@ def _stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
+    if not os.path.exists(os.path.join(BINDIR, "rte_gpu")):
+        return True
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
     deps.append(os.path.join(HERE, "..", "include", "rte_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
@@ -54,7 +58,25 @@ def build(verbose=False, force=False, ptxas_verbose=False):
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
+    build_cli(verbose)
     return LIB
+
+
+def build_cli(verbose=False):
+    """The reference's program names (rte_gpu, rte_inv, rte_test, rte_fim) as one executable over the
+    library, in doi_b200/bin (run-time path to ../lib)."""
+    os.makedirs(BINDIR, exist_ok=True)
+    exe = os.path.join(BINDIR, "rte_gpu")
+    cmd = [nvcc()] + ARCH + ["-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), os.path.join(CSRC, CLI),
+           "-o", exe, "-L", LIBDIR, "-lrte_b200", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../lib"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    for name in ("rte_inv", "rte_test", "rte_fim"):
+        link = os.path.join(BINDIR, name)
+        if os.path.lexists(link):
+            os.remove(link)
+        os.symlink("rte_gpu", link)
 
 
 if __name__ == "__main__":

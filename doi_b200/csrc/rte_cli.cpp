@@ -1,0 +1,227 @@
+// rte_cli.cpp -- the reference's command-line programs over the B200 library.
+//
+//   rte_gpu file.par   forward solve (FisherInfo_IO/src/rte.cu:92-236; the CPU package's
+//                      RTE_uniform.c for uniform-medium files): source, Neumann series with the
+//                      reference stop rule, transmission / reflection / phase images written to
+//                      [Runtime] TransFile / ReflectFile / PhaseFile in the reference's layout
+//   rte_inv file.par   region gradients of the transmission misfit against [Runtime] gFile
+//                      (FisherInfo_IO/src/compute_grad_rte.cu:205-385), one line per tissue type
+//   rte_fim file.par   Fisher information of the mu_a of a spherical region on the reflection
+//                      image (FisherInfo_IO/src/rte_fim.cu:236-331)
+//
+// One executable; the program is chosen by the name it is called under (build.py links the three
+// names).  Argument and error conventions follow the reference mains: a usage line and exit status 1
+// for a wrong argument count; a message and a non-zero status for unreadable inputs.
+#include <libgen.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "../../include/rte_b200.h"
+
+namespace {
+
+int die(rte_ctx* ctx, const char* what, int rc) {
+  fprintf(stderr, "%s failed (%d): %s\n", what, rc, rte_last_error(ctx));
+  return 1;
+}
+
+struct Loaded {
+  rte_par* par = nullptr;
+  rte_problem pr;
+  rte_ctx* ctx = nullptr;
+  ~Loaded() {
+    if (ctx) rte_destroy(ctx);
+    rte_problem_free(&pr);
+    rte_par_free(par);
+  }
+};
+
+// .par -> context with the medium set.  `forward_rule` applies the forward main's diffuse-medium
+// propThresh (rte.cu:116-119), which the gradient and Fisher mains do not have.
+int load(const char* path, bool forward_rule, Loaded& L, int read_map = 1) {
+  memset(&L.pr, 0, sizeof L.pr);
+  int rc = rte_par_load(path, &L.par);
+  if (rc) {
+    fprintf(stderr, "cannot read parameter file %s\n", path);
+    return 1;
+  }
+  rc = rte_par_problem(L.par, read_map, &L.pr);
+  if (rc) {
+    fprintf(stderr, "bad parameter file %s (%d): geometry, nL, tissue map or medium files\n", path, rc);
+    return 1;
+  }
+  rte_config cfg = L.pr.cfg;
+  if (forward_rule && L.pr.style == 0) cfg.prop_thresh = L.pr.diffuse_prop_thresh;
+  rc = rte_create(&cfg, &L.ctx);
+  if (rc) return die(nullptr, "rte_create", rc);
+  if (L.pr.mua_vox)
+    rc = rte_set_medium_voxel(L.ctx, L.pr.mua_vox, L.pr.mus_vox);
+  else
+    rc = rte_set_medium_tissue(L.ctx, L.pr.tiss, L.pr.ntypes, L.pr.mua, L.pr.mus);
+  if (rc) return die(L.ctx, "set medium", rc);
+  return 0;
+}
+
+double mut_at(const rte_problem& pr, size_t r) {
+  return pr.mua_vox ? pr.mua_vox[r] + pr.mus_vox[r] : pr.mua[pr.tiss[r]] + pr.mus[pr.tiss[r]];
+}
+
+// Phase image of the forward main (dist.cu:163-226): the diffuse transmission plus the ballistic
+// transmission of every column whose centre lies strictly inside the beam's diameter, then arg().
+std::vector<double> phase_image(const Loaded& L, const std::vector<rte_cplx>& W) {
+  const rte_config& c = L.pr.cfg;
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  std::vector<rte_cplx> tr((size_t)nx * ny);
+  std::vector<double> ph((size_t)nx * ny, 0.0);
+  if (rte_images(L.ctx, W.data(), nullptr, tr.data(), nullptr)) return ph;
+  const double dx = (c.x_max - c.x_min) / nx, dy = (c.y_max - c.y_min) / ny, dz = (c.z_max - c.z_min) / nz;
+  const rte_source& s = L.pr.src;
+  for (int j = 0; j < ny; j++)
+    for (int k = 0; k < nx; k++) {
+      std::complex<double> v(tr[(size_t)j * nx + k].re, tr[(size_t)j * nx + k].im);
+      const double xs = k * dx + c.x_min + dx / 2.0, ys = j * dy + c.y_min + dy / 2.0;
+      if (sqrt(pow(s.pos_x - xs, 2) + pow(s.pos_y - ys, 2)) < s.diam / 2.0) {
+        double t = s.mag;
+        for (int i = 0; i < nz; i++) t *= exp(-mut_at(L.pr, ((size_t)i * ny + j) * nx + k) * dz);
+        v += t;
+      }
+      ph[(size_t)j * nx + k] = std::arg(v);
+    }
+  return ph;
+}
+
+int main_forward(const char* path) {
+  Loaded L;
+  if (load(path, true, L)) return 1;
+  const rte_config& c = L.pr.cfg;
+  const size_t N = (size_t)c.nx * c.ny * c.nz, C = (size_t)(c.nL + 1) * (c.nL + 1), np = (size_t)c.nx * c.ny;
+  std::vector<rte_cplx> W(N * C), tr(np), rf(np);
+  rte_report rep;
+  int rc = rte_forward(L.ctx, &L.pr.src, &L.pr.stop, W.data(), tr.data(), rf.data(), &rep);
+  if (rc) return die(L.ctx, "rte_forward", rc);
+  printf("Neumann series: %d terms, %.3f ms on the device\n", rep.terms, rep.ms_device);
+  const int cpu_layout = L.pr.style == 1;
+  if (L.pr.trans_file[0] && (rc = rte_write_image(L.pr.trans_file, c.nx, c.ny, tr.data(), cpu_layout)))
+    return die(L.ctx, L.pr.trans_file, rc);
+  if (L.pr.ref_file[0] && (rc = rte_write_image(L.pr.ref_file, c.nx, c.ny, rf.data(), cpu_layout)))
+    return die(L.ctx, L.pr.ref_file, rc);
+  if (L.pr.phase_file[0] && L.pr.style == 0) {
+    const std::vector<double> ph = phase_image(L, W);
+    if ((rc = rte_write_phase_image(L.pr.phase_file, c.nx, c.ny, ph.data()))) return die(L.ctx, L.pr.phase_file, rc);
+  }
+  if (L.pr.flux_file[0] && L.pr.detector_bins > 0) {  // binned exitant flux on all six faces
+    rte_stop st = L.pr.stop;
+    if (st.rule == RTE_STOP_REFERENCE) st = rte_stop{RTE_STOP_FIXED, rep.terms, 0.0};
+    rte_detector det{L.pr.detector_bins, 63};
+    std::vector<double> flux((size_t)6 * det.nbins * det.nbins);
+    if ((rc = rte_detector_flux(L.ctx, 1, &L.pr.src, &st, &det, flux.data()))) return die(L.ctx, "rte_detector_flux", rc);
+    FILE* f = fopen(L.pr.flux_file, "wb");
+    if (!f || fwrite(flux.data(), sizeof(double), flux.size(), f) != flux.size()) {
+      fprintf(stderr, "cannot write %s\n", L.pr.flux_file);
+      if (f) fclose(f);
+      return 1;
+    }
+    fclose(f);
+  }
+  return 0;
+}
+
+int main_inverse(const char* path) {
+  Loaded L;
+  if (load(path, false, L)) return 1;
+  const rte_config& c = L.pr.cfg;
+  const size_t np = (size_t)c.nx * c.ny;
+  std::vector<double> g(np);
+  int rc = L.pr.g_file[0] ? rte_read_image(L.pr.g_file, c.nx, c.ny, g.data()) : RTE_ERR_IO;
+  if (rc) {
+    fprintf(stderr, "Error in opening gfile. Exiting \n");
+    return 1;
+  }
+  const int nt = L.pr.ntypes;
+  std::vector<double> ga(nt), ga2(nt), gs(nt), gs2(nt), mua(L.pr.mua, L.pr.mua + nt), mus(L.pr.mus, L.pr.mus + nt);
+  FILE* resf = fopen("Residual.out", "wb");
+  // the main sweeps tissue 1 over a fixed grid of values, one gradient evaluation per iteration
+  // (compute_grad_rte.cu:207-209); its parameter update is disabled in the reference
+  for (int itt = 0; itt < L.pr.num_iterations; itt++) {
+    mus[1] = 0.8 + round(itt / 2.0) * 0.05;
+    mua[1] = 0.008 + floor(itt / 2.0) * 0.0005;
+    rc = rte_set_medium_tissue(L.ctx, L.pr.tiss, nt, mua.data(), mus.data());
+    if (rc) return die(L.ctx, "set medium", rc);
+    double res = 0, res2 = 0;
+    rc = rte_region_gradient(L.ctx, &L.pr.src, &L.pr.stop, g.data(), L.pr.tiss, nt, 1, ga.data(), ga2.data(),
+                             gs.data(), gs2.data(), &res, &res2);
+    if (rc) return die(L.ctx, "rte_region_gradient", rc);
+    printf("Iteration No %d \n", itt);
+    for (int t = 1; t < nt; t++) {
+      printf("Value of mua = %e mus = %e \n", mua[t], mus[t]);
+      printf("Value of mua grad1 = %e musgrad1 = %e \n", ga[t], gs[t]);
+      printf("Value of mua grad2 = %e musgrad2 = %e \n", ga2[t], gs2[t]);
+    }
+    printf("Residual = %e\n", res);
+    printf("Residual2 = %e\n", res2);
+    if (resf) fwrite(&res, sizeof(double), 1, resf);
+  }
+  if (resf) fclose(resf);
+  return 0;
+}
+
+int main_fisher(const char* path) {
+  Loaded L;
+  if (load(path, false, L, 0)) return 1;  // LoadPhantom(ini, 0): no tissue map (rte_fim.cu:104)
+  const rte_config& c = L.pr.cfg;
+  const size_t N = (size_t)c.nx * c.ny * c.nz;
+  // the main sets mu_a = 0.01, mu_s = 1 for every tissue type before its solves (rte_fim.cu:226-230)
+  std::vector<double> ta(L.pr.ntypes, 0.01), ts(L.pr.ntypes, 1.0);
+  ta[0] = ts[0] = 0.0;
+  int rc = rte_set_medium_tissue(L.ctx, L.pr.tiss, L.pr.ntypes, ta.data(), ts.data());
+  if (rc) return die(L.ctx, "set medium", rc);
+  // region: the voxels within rad_sig[0] = fov/(2 nX) of voxel (nX/2, nY/2, 1), on the main's own
+  // coordinate arrays, which use the x extent for every axis (rte_fim.cu:135-206).  The reference
+  // fills its z array only for indices below nX; here every index follows the same formula.
+  const double fov = c.x_max - c.x_min;
+  auto X = [&](int i) { return i * fov / c.nx - fov / 2 + fov / (2 * c.nx); };
+  auto Y = [&](int i) { return i * fov / c.ny - fov / 2 + fov / (2 * c.ny); };
+  auto Z = [&](int i) { return i * fov / c.nz + fov / (2 * c.nz); };
+  const float rad = (float)(1 * fov / (2 * c.nx));
+  const float rad2 = rad * rad;  // a float product, compared against the double distance
+  const int lx = c.nx / 2, ly = c.ny / 2, lz = 1;
+  std::vector<uint8_t> mask(N);
+  for (int i = 0; i < c.nz; i++)
+    for (int j = 0; j < c.ny; j++)
+      for (int k = 0; k < c.nx; k++) {
+        const double d2 = (X(k) - X(lx)) * (X(k) - X(lx)) + (Y(j) - Y(ly)) * (Y(j) - Y(ly)) + (Z(i) - Z(lz)) * (Z(i) - Z(lz));
+        mask[((size_t)i * c.ny + j) * c.nx + k] = !(d2 > (double)rad2);
+      }
+  double F = 0;
+  for (int t = 1; t < L.pr.ntypes; t++) {  // the main repeats the same solve per tissue type
+    rc = rte_fisher_regions(L.ctx, &L.pr.src, &L.pr.stop, 1, mask.data(), 1, &F);
+    if (rc) return die(L.ctx, "rte_fisher_regions", rc);
+  }
+  printf("%e is fisher abs for %d as z index and %f as radius \n", F, lz, rad);
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::string name = basename(argv[0]);
+  if (argc != 2) {
+    if (name == "rte_gpu") {
+      printf("\n RTE_uniform file.ini\n");
+      printf("     file.ini is the initialization.\n\n");
+    } else {
+      printf("\n InverseRTE file.par\n");
+      printf("     file.par is the parameter file.\n\n");
+    }
+    return 1;
+  }
+  if (name == "rte_inv" || name == "rte_test") return main_inverse(argv[1]);
+  if (name == "rte_fim") return main_fisher(argv[1]);
+  return main_forward(argv[1]);
+}

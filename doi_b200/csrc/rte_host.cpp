@@ -359,6 +359,7 @@ struct rte_ctx {
   // or its series length changed with the medium) is recorded again before it is replayed
   std::vector<uintptr_t> graph_sig[5];
   void* d_Qbp = nullptr;        // gradient: weight of every unordered voxel pair (N x round32(N))
+  uint8_t* d_mask = nullptr;    // region mask of the reference-compatible tangent solves [N]
   size_t qbp_bytes = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
@@ -451,7 +452,7 @@ static void free_all(rte_ctx* c) {
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
                 c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq,
-                c->d_Qbp};
+                c->d_Qbp, c->d_mask};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -2264,4 +2265,130 @@ extern "C" int rte_forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, i
     rep->ms_setup = 0;
   }
   return RTE_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Reference-compatible region derivatives (the tangent solves of the reference's inverse and
+// Fisher mains).  The forward solution `out` stays on the device (d_out); each region tangent is
+// the series of the masked, per-l scaled copy of it, projected to the exitance images without the
+// ballistic term (FisherInfo_IO/src/compute_grad_rte.cu:273-385, rte_fim.cu:236-331).
+
+static int forward_to_out(rte_ctx* c, const rte_source* s, const rte_stop* stop, rte_cplx* trans, rte_cplx* ref) {
+  int rc = ensure_detector_buffers(c);
+  if (rc) return rc;
+  c->has_point = false;
+  if (s->kind == RTE_SRC_POINT) CUDA_TRY(c, cudaMemsetAsync(c->d_q, 0, (size_t)c->N * c->C * sizeof(double), c->st));
+  rc = launch_source(c, s, c->d_aux1, 0, nullptr, true, c->d_q);
+  if (!rc) rc = series_start(c, c->d_aux1, c->d_q, c->d_aux3, 1, c->d_Wf, c->cpad);
+  if (!rc) rc = neumann_real(c, c->d_aux3, c->d_aux1, c->d_out, 1, stop, -1, nullptr, nullptr);
+  if (!rc) rc = run_images(c, c->d_out, s, true, trans, ref);
+  return rc;
+}
+
+static int tangent_images(rte_ctx* c, const rte_source* s, const uint8_t* mask, const double* fac,
+                          const rte_stop* stop, rte_cplx* dtrans, rte_cplx* dref) {
+  if (!c->d_mask) CUDA_TRY(c, dalloc(c, &c->d_mask, (size_t)c->N));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mask, mask, (size_t)c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_masked_scale(c->d_out, c->d_aux1, c->d_mask, fac, c->N, c->L, c->st)));
+  // Neumann(src, src, 1): W_0 = src, running sum_0 = src
+  int rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, nullptr, nullptr);
+  if (!rc) rc = run_images(c, c->d_aux2, s, false, dtrans, dref);
+  return rc;
+}
+
+extern "C" int rte_region_gradient(rte_ctx* c, const rte_source* s, const rte_stop* stop, const double* g,
+                                   const uint8_t* tiss, int ntypes, int compat, double* grada, double* grada2,
+                                   double* grads, double* grads2, double* residual, double* residual2) {
+  if (!c || !s || !stop || !g || !tiss || ntypes < 2 || !grada || !grada2 || !grads || !grads2)
+    return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  const size_t np = (size_t)c->nx * c->ny;
+  std::vector<rte_cplx> gbar(np), dg(np);
+  int rc = forward_to_out(c, s, stop, gbar.data(), nullptr);
+  if (rc) return rc;
+  const double Cl = 1.0;          // the FisherInfo_IO speed of light (rte.h:15)
+  const float av_mua = 0.01f, av_mus = 1.0f;  // compute_grad_rte.cu:115-116
+  std::vector<uint8_t> mask(c->N);
+  std::vector<double> fa(c->L + 1, -Cl), fs(c->L + 1);
+  for (int l = 0; l <= c->L; l++) fs[l] = -Cl + pow(c->cfg.g, (double)l);  // -C out + PropScatmu1(out)
+  grada[0] = grada2[0] = grads[0] = grads2[0] = 0.0;
+  for (int t = 1; t < ntypes; t++) {
+    bool other = false;
+    for (int r = 0; r < c->N; r++) {
+      mask[r] = tiss[r] == t;
+      other = other || !mask[r];
+    }
+    rc = tangent_images(c, s, mask.data(), fa.data(), stop, dg.data(), nullptr);
+    if (rc) return rc;
+    double a1 = 0, a2 = 0;
+    for (size_t j = 0; j < np; j++)
+      if (g[j] || gbar[j].re) {
+        a1 -= 2.0 * av_mua * dg[j].re / (g[j] - gbar[j].re);
+        a2 -= 2.0 * av_mua * (g[j] - gbar[j].re) * dg[j].re;
+      }
+    grada[t] = a1;
+    grada2[t] = a2;
+    // the mu_s mask of the reference tests each voxel but zeroes the voxel index left over from the
+    // mu_a loop (compute_grad_rte.cu:356-363): the last voxel, whenever another tissue exists
+    if (compat) {
+      std::fill(mask.begin(), mask.end(), (uint8_t)1);
+      if (other) mask[c->N - 1] = 0;
+    }
+    rc = tangent_images(c, s, mask.data(), fs.data(), stop, dg.data(), nullptr);
+    if (rc) return rc;
+    double s1 = 0, s2 = 0;
+    for (size_t j = 0; j < np; j++)
+      if (g[j] || gbar[j].re) {
+        s1 -= 2.0 * av_mus * dg[j].re / (g[j] - gbar[j].re);
+        s2 -= 2.0 * av_mus * (g[j] - gbar[j].re) * dg[j].re;
+      }
+    grads[t] = s1;
+    grads2[t] = s2;
+  }
+  double d1 = 0, d2 = 0;  // compute_grad_rte.cu:437-444
+  for (size_t j = 0; j < np; j++) {
+    const double e = gbar[j].re - g[j];
+    if (e != 0.0) d1 += log(e * e);
+    d2 += e * e;
+  }
+  if (residual) *residual = d1;
+  if (residual2) *residual2 = d2;
+  return check_kernel_err(c);
+}
+
+extern "C" int rte_fisher_regions(rte_ctx* c, const rte_source* s, const rte_stop* stop, int P, const uint8_t* masks,
+                                  int image, double* F) {
+  if (!c || !s || !stop || P < 1 || !masks || !F || image < 0 || image > 2) return fail(c, RTE_ERR_ARG, "bad argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  const size_t np = (size_t)c->nx * c->ny;
+  std::vector<rte_cplx> gt(np), gr(np), t(np), rr(np);
+  int rc = forward_to_out(c, s, stop, gt.data(), gr.data());
+  if (rc) return rc;
+  std::vector<double> fa(c->L + 1, -1.0);  // -C mask(out), C = 1 (rte_fim.cu:270)
+  std::vector<std::vector<double>> d((size_t)P);
+  for (int p = 0; p < P; p++) {
+    rc = tangent_images(c, s, masks + (size_t)p * c->N, fa.data(), stop, t.data(), rr.data());
+    if (rc) return rc;
+    d[p].resize(2 * np);
+    for (size_t j = 0; j < np; j++) {
+      d[p][j] = t[j].re;
+      d[p][np + j] = rr[j].re;
+    }
+  }
+  // Poisson noise: F_ab = sum_j dg_a,j dg_b,j / gbar_j over pixels with gbar_j != 0 (rte_fim.cu:316-331);
+  // image 0 transmission, 1 reflection (the reference main), 2 both
+  for (int a = 0; a < P; a++)
+    for (int b = 0; b < P; b++) {
+      double f = 0.0;
+      for (int im = 0; im < 2; im++) {
+        if ((image == 0 && im == 1) || (image == 1 && im == 0)) continue;
+        const std::vector<rte_cplx>& gb = im ? gr : gt;
+        for (size_t j = 0; j < np; j++)
+          if (gb[j].re) f += (1.0 / gb[j].re) * d[a][im * np + j] * d[b][im * np + j];
+      }
+      F[(size_t)a * P + b] = f;
+    }
+  return check_kernel_err(c);
 }

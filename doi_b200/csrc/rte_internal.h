@@ -147,6 +147,8 @@ cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, co
 // over every unordered pair scattering Q * length into the gradient.
 cudaError_t rte_launch_bp_weights(const BpArgs& a, int LA, int fp64, cudaStream_t st);
 cudaError_t rte_launch_bp_walk(const BpArgs& a, int fp64, cudaStream_t st);
+cudaError_t rte_launch_masked_scale(const double* in, double* out, const uint8_t* mask, const double* fac, int N,
+                                    int L, cudaStream_t st);
 cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st);
 // message returned by rte_last_error(NULL) on this thread
 __attribute__((visibility("hidden"))) void rte_set_global_error(const char* msg);

@@ -860,6 +860,18 @@ __global__ void k_parity(double* x, int N, int L, int vstride) {
   if (l & 1) x[(size_t)r * vstride + c] = -x[(size_t)r * vstride + c];
 }
 
+// out[r][c] = mask[r] ? fac[l(c)] * in[r][c] : 0 -- the region-restricted tangent sources of the
+// reference's inverse and Fisher mains (compute_grad_rte.cu:288-363, rte_fim.cu:253-273).
+__global__ void k_masked_scale(const double* in, double* out, const uint8_t* mask, ScatTab fac, int N, int L) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = (L + 1) * (L + 1);
+  if (t >= (long long)N * C) return;
+  const int r = (int)(t / C), c = (int)(t % C);
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  out[t] = mask[r] ? fac.v[l] * in[t] : 0.0;
+}
+
 __global__ void k_axpy(double* y, const double* x, double alpha, size_t n) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) y[t] = fma(alpha, x[t], y[t]);
@@ -1386,6 +1398,15 @@ cudaError_t rte_launch_face_flux(const FaceArgs& a, cudaStream_t st) {
 cudaError_t rte_launch_adjoint_seed(const FaceArgs& a, cudaStream_t st) {
   const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
   k_adjoint_seed<<<(total + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_masked_scale(const double* in, double* out, const uint8_t* mask, const double* fac, int N,
+                                    int L, cudaStream_t st) {
+  ScatTab f;
+  for (int l = 0; l <= RTE_MAX_L; ++l) f.v[l] = l <= L ? fac[l] : 0.0;
+  const long long n = (long long)N * (L + 1) * (L + 1);
+  k_masked_scale<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, out, mask, f, N, L);
   return cudaGetLastError();
 }
 

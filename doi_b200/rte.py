@@ -31,7 +31,9 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_images", "rte_forward", "rte_forward_batch", "rte_detector_flux", "rte_gradient",
            "rte_measure_fma_peak", "rte_get_stream", "rte_set_profiling", "rte_get_stats", "rte_forward_graph",
            "rte_server_create", "rte_server_submit", "rte_server_wait", "rte_server_cancel", "rte_server_stats",
-           "rte_server_destroy")
+           "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
+           "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
+           "rte_read_image", "rte_region_gradient", "rte_fisher_regions")
 
 
 class RteError(RuntimeError):
@@ -120,6 +122,17 @@ class _Request(ctypes.Structure):
                 ("nsrc", ctypes.c_int), ("src", _Source * 4), ("mua", ctypes.c_void_p), ("mus", ctypes.c_void_p)]
 
 
+class _Problem(ctypes.Structure):
+    _fields_ = [("cfg", _Config), ("src", _Source), ("stop", _Stop), ("style", ctypes.c_int), ("ntypes", ctypes.c_int),
+                ("mua", ctypes.c_double * 256), ("mus", ctypes.c_double * 256), ("tiss", ctypes.c_void_p),
+                ("mua_vox", ctypes.c_void_p), ("mus_vox", ctypes.c_void_p), ("mut_mean", ctypes.c_double),
+                ("diffuse_prop_thresh", ctypes.c_double), ("nterms", ctypes.c_int), ("detector_bins", ctypes.c_int),
+                ("num_iterations", ctypes.c_int), ("step_a", ctypes.c_double), ("step_s", ctypes.c_double),
+                ("trans_file", ctypes.c_char * 1024), ("ref_file", ctypes.c_char * 1024),
+                ("phase_file", ctypes.c_char * 1024), ("g_file", ctypes.c_char * 1024),
+                ("flux_file", ctypes.c_char * 1024)]
+
+
 class _ResultInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
                 ("service_ms", ctypes.c_double), ("device_ms", ctypes.c_double)]
@@ -181,6 +194,25 @@ def load_library():
     L.rte_server_stats.argtypes = [P, ctypes.POINTER(_ServerInfo)]
     L.rte_server_destroy.argtypes = [P]
     L.rte_server_destroy.restype = None
+    L.rte_par_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.rte_par_free.argtypes = [P]
+    L.rte_par_free.restype = None
+    L.rte_par_get_string.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p]
+    L.rte_par_get_string.restype = ctypes.c_char_p
+    L.rte_par_get_int.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+    L.rte_par_get_double.argtypes = [P, ctypes.c_char_p, ctypes.c_double]
+    L.rte_par_get_double.restype = ctypes.c_double
+    L.rte_par_problem.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Problem)]
+    L.rte_problem_free.argtypes = [ctypes.POINTER(_Problem)]
+    L.rte_problem_free.restype = None
+    L.rte_write_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+    L.rte_write_phase_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp]
+    L.rte_read_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp]
+    L.rte_region_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, ctypes.c_int,
+                                      ctypes.c_int, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double)]
+    L.rte_fisher_regions.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.c_int, dp, ctypes.c_int,
+                                     dp]
     _LIB = L
     return L
 
@@ -361,6 +393,29 @@ class Context:
             res["trans"], res["ref"] = tr, rf
         return res
 
+    def region_gradient(self, src, stop, g, tiss, ntypes, compat=True):
+        """Region derivatives of the reference's inverse main: (grada, grada2, grads, grads2, residual,
+        residual2) with one entry per tissue type."""
+        g = np.ascontiguousarray(g, np.float64).ravel()
+        tiss = np.ascontiguousarray(tiss, np.uint8).ravel()
+        out = [np.zeros(ntypes) for _ in range(4)]
+        r1, r2 = ctypes.c_double(0), ctypes.c_double(0)
+        s, st = src.c(), stop.c()
+        self._check(self.lib.rte_region_gradient(self.h, ctypes.byref(s), ctypes.byref(st), _ptr(g), _ptr(tiss), ntypes,
+                                                 int(bool(compat)), *[_ptr(o) for o in out], ctypes.byref(r1),
+                                                 ctypes.byref(r2)), "rte_region_gradient")
+        return (*out, r1.value, r2.value)
+
+    def fisher_regions(self, src, stop, masks, image=1):
+        """Poisson Fisher information of the mu_a of each region in masks (P x N booleans)."""
+        masks = np.ascontiguousarray(np.asarray(masks).reshape(-1, self.N), np.uint8)
+        P = masks.shape[0]
+        F = np.zeros((P, P))
+        s, st = src.c(), stop.c()
+        self._check(self.lib.rte_fisher_regions(self.h, ctypes.byref(s), ctypes.byref(st), P, _ptr(masks), image,
+                                                _ptr(F)), "rte_fisher_regions")
+        return F
+
     def forward_graph(self, srcs, nterms):
         """Fixed-term forward solve of up to 4 sources, replayed from a CUDA graph recorded on the
         first call; returns (trans, ref) stacked per source and the device time in ms."""
@@ -464,3 +519,77 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class ParFile:
+    """A reference .par file read by the library's parser (section:key lookups, iniparser rules)."""
+
+    def __init__(self, path):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.rte_par_load(os.fsencode(path), ctypes.byref(h))
+        if rc != 0:
+            raise RteError(f"rte_par_load({path}) failed ({rc})")
+        self.h = h
+
+    def get(self, key, default=None):
+        v = self.lib.rte_par_get_string(self.h, key.encode(), None)
+        return default if v is None else v.decode()
+
+    def get_int(self, key, default=0):
+        return self.lib.rte_par_get_int(self.h, key.encode(), default)
+
+    def get_double(self, key, default=0.0):
+        return self.lib.rte_par_get_double(self.h, key.encode(), default)
+
+    def problem(self, read_map=True):
+        """The solver inputs the reference mains derive from this file (a dict)."""
+        pr = _Problem()
+        rc = self.lib.rte_par_problem(self.h, int(bool(read_map)), ctypes.byref(pr))
+        if rc != 0:
+            raise RteError(f"rte_par_problem failed ({rc})")
+        try:
+            c = pr.cfg
+            N = c.nx * c.ny * c.nz
+            out = {k: getattr(c, k) for k, _ in _Config._fields_}
+            out["source"] = {k: getattr(pr.src, k) for k, _ in _Source._fields_}
+            out["stop"] = {k: getattr(pr.stop, k) for k, _ in _Stop._fields_}
+            for k in ("style", "ntypes", "mut_mean", "diffuse_prop_thresh", "nterms", "detector_bins",
+                      "num_iterations", "step_a", "step_s"):
+                out[k] = getattr(pr, k)
+            for k in ("trans_file", "ref_file", "phase_file", "g_file", "flux_file"):
+                out[k] = getattr(pr, k).decode()
+            out["mua_tab"] = np.array(pr.mua[:pr.ntypes])
+            out["mus_tab"] = np.array(pr.mus[:pr.ntypes])
+            out["tiss"] = np.ctypeslib.as_array(ctypes.cast(pr.tiss, ctypes.POINTER(ctypes.c_uint8)), (N,)).copy() \
+                if pr.tiss else None
+            return out
+        finally:
+            self.lib.rte_problem_free(ctypes.byref(pr))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rte_par_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_image(path, img, cpu_layout=False):
+    img = np.ascontiguousarray(img, np.complex128)
+    ny, nx = img.shape
+    rc = load_library().rte_write_image(os.fsencode(path), nx, ny, _ptr(img), int(bool(cpu_layout)))
+    if rc != 0:
+        raise RteError(f"rte_write_image failed ({rc})")
+
+
+def read_image(path, nx, ny):
+    out = np.zeros(nx * ny)
+    rc = load_library().rte_read_image(os.fsencode(path), nx, ny, _ptr(out))
+    if rc != 0:
+        raise RteError(f"rte_read_image failed ({rc})")
+    return out.reshape(ny, nx)

@@ -169,6 +169,27 @@ int rte_gradient(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop*
                  const rte_detector* det, const double* target, double* loss, double* g_mua,
                  double* g_mus);
 
+/* Region derivatives of the reference's inverse main (FisherInfo_IO/src/compute_grad_rte.cu:205-385),
+ * one evaluation at the current medium: forward solve, gbar = transmission image; for every tissue
+ * type t >= 1 a tangent solve of -C mask_t(out) (mu_a) and of mask(-C out + g^l out) (mu_s), C = 1,
+ * projected to the transmission image dgbar without the ballistic term, and
+ *   grad[t]  = -2 av sum_j dgbar_j / (g_j - gbar_j),   grad2[t] = -2 av sum_j (g_j - gbar_j) dgbar_j
+ * over pixels with g_j or gbar_j non-zero (av = 0.01 for mu_a, 1 for mu_s); residual = sum log((gbar-g)^2)
+ * over non-zero differences, residual2 = sum (gbar-g)^2.  compat = 1 reproduces the reference's mu_s
+ * mask, which zeroes only the last voxel (a stale index, compute_grad_rte.cu:363) whenever another
+ * tissue exists; compat = 0 uses the tissue mask.  g: nX*nY measured image; tiss: N tissue types;
+ * output arrays have ntypes entries (entry 0 is 0). */
+int rte_region_gradient(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, const double* g,
+                        const uint8_t* tiss, int ntypes, int compat, double* grada, double* grada2,
+                        double* grads, double* grads2, double* residual, double* residual2);
+
+/* Fisher information of P region parameters (mu_a of the voxels in masks[p*N .. p*N+N-1]) under
+ * Poisson noise, F[a*P+b] = sum_j dg_a,j dg_b,j / gbar_j over pixels with gbar_j != 0, from one forward
+ * and P tangent solves of -C mask_p(out) (FisherInfo_IO/src/rte_fim.cu:236-331).  image: 0
+ * transmission, 1 reflection (the reference main's choice), 2 both. */
+int rte_fisher_regions(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, int P, const uint8_t* masks,
+                       int image, double* F);
+
 /* Batched forward solves (new): nsrc <= 4 sources on the current medium, propagated together so
  * each voxel pair's direction, spherical harmonics and kernel value serve every source.  Outputs
  * are the nsrc single-source results back to back (W_out nsrc*N*C, trans/ref nsrc*nX*nY, each may
@@ -229,6 +250,59 @@ int rte_server_wait(rte_server* srv, long long ticket, double timeout_s, rte_cpl
 int rte_server_cancel(rte_server* srv, long long ticket); /* only before it starts */
 int rte_server_stats(rte_server* srv, rte_server_info* out);
 void rte_server_destroy(rte_server* srv);
+
+/* ---- reference parameter and image files (drop-in for the reference programs) -------
+ * .par files in the reference's iniparser dialect (FisherInfo_IO/src/iniparser.cu:455-620): '#'
+ * comment lines, [section], key = value (quoted, or cut at ';' / '#'), trailing '\' joins lines,
+ * case-insensitive "section:key" lookup, last repeat wins; ints as strtol(s, 0, 0), doubles as
+ * atof. */
+typedef struct rte_par rte_par;
+int rte_par_load(const char* path, rte_par** out); /* RTE_ERR_IO if the file cannot be opened */
+void rte_par_free(rte_par* p);
+const char* rte_par_get_string(const rte_par* p, const char* key, const char* def);
+int rte_par_get_int(const rte_par* p, const char* key, int def);
+double rte_par_get_double(const rte_par* p, const char* key, double def);
+
+#define RTE_PAR_MAX_TISS 256
+/* Solver inputs as the reference mains derive them from a .par file: LoadGeometry / LoadPhantom /
+ * LoadSource (FisherInfo_IO/src/inits.cu:22-269; float extents and thresholds as the reference
+ * stores them) when [Phantom] TissMapFile is given, else the CPU package's uniform-medium keys
+ * (CPU package/src/Inits.c:24-131: [Phantom] mua, mus, c).  Optional keys of this library:
+ * [Algorithm] Model = fim|cpu|exact, Precision = fp64|mixed, KernelMode = auto|store|recompute,
+ * StopRule = reference|fixed|rel_l2, MaxTerms, Tol, Device, DetectorBins; [Phantom] MuaFile /
+ * MusFile (N doubles each, per-voxel media); [Source] Kind = fim|column|cpu|beam|point, Face;
+ * [Runtime] FluxFile.  Defaults reproduce the reference. */
+typedef struct {
+  rte_config cfg;
+  rte_source src;
+  rte_stop stop;                 /* StopRule / MaxTerms / Tol (default: the reference rule) */
+  int style;                     /* 0: FisherInfo_IO tissue-map file, 1: CPU-package uniform file */
+  int ntypes;                    /* tissue types including type 0 (outside, mu = 0) */
+  double mua[RTE_PAR_MAX_TISS], mus[RTE_PAR_MAX_TISS];
+  uint8_t* tiss;                 /* nX*nY*nZ tissue map (owned; rte_problem_free) */
+  double* mua_vox;               /* per-voxel media from MuaFile / MusFile, or NULL */
+  double* mus_vox;
+  double mut_mean;               /* mean mu_t over the voxels (inits.cu:136-147) */
+  double diffuse_prop_thresh;    /* propThresh after the forward main's diffuse-medium rule (rte.cu:116-119) */
+  int nterms;                    /* [Algorithm] nTerms (read; the reference's auto-stop ignores it) */
+  int detector_bins;             /* [Algorithm] DetectorBins (0: no flux file) */
+  int num_iterations;            /* [Runtime] numIterations */
+  double step_a, step_s;         /* [Runtime] stepsizea, stepsizes */
+  char trans_file[1024], ref_file[1024], phase_file[1024], g_file[1024], flux_file[1024];
+} rte_problem;
+/* read_map = 1 reads [Phantom] TissMapFile (RTE_ERR_IO when missing); 0 makes every voxel tissue 1,
+ * as LoadPhantom(ini, 0) does for the Fisher main.  No device work. */
+int rte_par_problem(const rte_par* p, int read_map, rte_problem* out);
+void rte_problem_free(rte_problem* pr);
+
+/* Image files: 2 ints then the real and the imaginary nX*nY planes (doubles, x fastest); the
+ * header is (nY, nX) as FisherInfo_IO/src/dist.cu:316-345 writes it, or (nX, nY) with cpu_layout
+ * as CPU package/src/Dist.c:16-40 does.  Phase images: 2 ints + nX*nY doubles (dist.cu:291-314).
+ * rte_read_image reads a measured image (gFile): 2 ints + nX*nY doubles
+ * (compute_grad_rte.cu:151-161). */
+int rte_write_image(const char* path, int nx, int ny, const rte_cplx* img, int cpu_layout);
+int rte_write_phase_image(const char* path, int nx, int ny, const double* phase);
+int rte_read_image(const char* path, int nx, int ny, double* out);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ------------------
  * For callers that must not allocate device memory when they run the solver: work recorded
