@@ -409,6 +409,11 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
         k0 = __ldg(Kcol);
         if (ns > 1) k1 = __ldg(Kcol + a.Kld);
       }
+      // stored kernel with exact SH: no per-pair branch (the diagonal and pairs beyond the coupling
+      // distance carry k = 0), so two sources' SH recurrences can interleave
+      constexpr bool FLAT = STORED && !TABLE;
+      constexpr int UNR = FLAT ? 2 : 1;
+#pragma unroll UNR
       for (int sv = 0; sv < ns; ++sv) {
         float kk = 0.f;
         if (STORED) {
@@ -422,7 +427,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
         bool live;
         float dist = 0.f;
         if (STORED) {
-          live = kk != 0.f;
+          live = FLAT || kk != 0.f;
         } else {
           dist = sqrtf(d2);
           live = d2 > 0.f && dist < thr;
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
             table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
             sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
           } else {
-            const float inv = rsqrtf(d2);
+            const float inv = FLAT ? (d2 > 0.f ? rsqrtf(d2) : 0.f) : rsqrtf(d2);
             sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
           }
           if (!STORED) {
