@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <complex>
 #include <array>
 #include <map>
 #include <mutex>
@@ -360,6 +361,11 @@ struct rte_ctx {
   std::vector<uintptr_t> graph_sig[5];
   void* d_Qbp = nullptr;        // gradient: weight of every unordered voxel pair (N x round32(N))
   uint8_t* d_mask = nullptr;    // region mask of the reference-compatible tangent solves [N]
+  double* d_dmut = nullptr;     // Fisher: parameter direction of mu_t and mu_s [N], tangent dA S [N][C]
+  double* d_dmus = nullptr;
+  double* d_T = nullptr;
+  int* d_cidx = nullptr;        // source-column voxels and their source derivative
+  double* d_cval = nullptr;
   size_t qbp_bytes = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
@@ -452,7 +458,7 @@ static void free_all(rte_ctx* c) {
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
                 c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq,
-                c->d_Qbp, c->d_mask};
+                c->d_Qbp, c->d_mask, c->d_dmut, c->d_dmus, c->d_T, c->d_cidx, c->d_cval};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1276,6 +1282,20 @@ static int face_voxel(const rte_ctx* c, int f, int p, int t) {
 // apart): beams put xi = D A xi_beam on their column (dist.cu:66-101; Dist.c:1077-1128 for
 // RTE_SRC_CPU) and their ballistic exitant flux in d_fball; a point source puts its isotropic
 // emission q into d_q (its uncollided and scattered orders follow from the series).
+// HG scatter of a collimated beam entering through `face`: coefficient scale g^l R_lm(d), d the
+// face's inward normal (the z = 0 face's m = 0 values written in closed form, dist.cu:86-92)
+static void beam_coefs(const rte_ctx* c, int face, double scale, double* coef) {
+  const double dirs[6][3] = {{0, 0, 1}, {0, 0, -1}, {0, 1, 0}, {0, -1, 0}, {1, 0, 0}, {-1, 0, 0}};
+  std::vector<double> R(c->C);
+  sh_real_host(c->sh, c->L, dirs[face][0], dirs[face][1], dirs[face][2], R.data());
+  for (int l = 0, q = 0; l <= c->L; l++)
+    for (int m = -l; m <= l; m++, q++) {
+      double v = scale * pow(c->cfg.g, (double)l) * R[q];
+      if (m == 0 && face == 0) v = scale * pow(c->cfg.g, (double)l) * sqrt((2.0 * l + 1.0) / (4.0 * M_PI));
+      coef[q] = fabs(v) < 1e-300 ? 0.0 : v;
+    }
+}
+
 static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vstride = 0, double* d_fball = nullptr,
                          bool zero = true, double* d_q = nullptr) {
   if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
@@ -1310,16 +1330,7 @@ static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vst
   a.face = source_face(s);
   a.ncols = (int)cols.size();
   for (size_t q = 0; q < cols.size(); q++) a.cols[q] = cols[q];
-  // HG scatter of the beam direction: coefficient g^l R_lm(d) (d = inward normal of the face)
-  const double dirs[6][3] = {{0, 0, 1}, {0, 0, -1}, {0, 1, 0}, {0, -1, 0}, {1, 0, 0}, {-1, 0, 0}};
-  std::vector<double> R(c->C);
-  sh_real_host(c->sh, c->L, dirs[a.face][0], dirs[a.face][1], dirs[a.face][2], R.data());
-  for (int l = 0, q = 0; l <= c->L; l++)
-    for (int m = -l; m <= l; m++, q++) {
-      double v = scale * pow(c->cfg.g, (double)l) * R[q];
-      if (m == 0 && a.face == 0) v = scale * pow(c->cfg.g, (double)l) * sqrt((2.0 * l + 1.0) / (4.0 * M_PI));
-      a.coef[q] = fabs(v) < 1e-300 ? 0.0 : v;
-    }
+  beam_coefs(c, a.face, scale, a.coef);
   a.scale = scale;
   a.mag = s->mag;
   a.dlen = a.face < 2 ? c->dz : (a.face < 4 ? c->dy : c->dx);
@@ -2391,4 +2402,192 @@ extern "C" int rte_fisher_regions(rte_ctx* c, const rte_source* s, const rte_sto
       F[(size_t)a * P + b] = f;
     }
   return check_kernel_err(c);
+}
+
+// ---------------------------------------------------------------------------------------
+// Fisher information of parameters of the medium, from tangent (sensitivity) solves.
+// For a parameter direction (dmu_a, dmu_s) per voxel and a converged forward solution
+// S = sum_k (DA)^k xi, out = A S, the discrete model's derivative is
+//   dS = (I - DA)^-1 [ dxi + dD (A S) + D (dA S) ],   d out = A dS + dA S,
+// dA S from k_pair_tangent (path integrals of dmu_t along every pair, the kernel recomputed or read
+// from the stored FP32 copy) plus the self-term derivative; dxi and the ballistic derivative of the
+// collimated beam by a complex step on the host (exact to rounding).  J = d(binned flux)/dtheta and,
+// with Poisson counts, F = J^T diag(1 / flux) J.
+
+static int tangent_dA(rte_ctx* c, const double* d_in, double* d_outT, const std::vector<double>& dmut) {
+  const size_t NC = (size_t)c->N * c->C;
+  int lo[3] = {c->nx, c->ny, c->nz}, hi[3] = {-1, -1, -1};
+  for (int r = 0; r < c->N; r++)
+    if (dmut[r] != 0.0) {
+      const int v[3] = {r % c->nx, (r / c->nx) % c->ny, r / (c->nx * c->ny)};
+      for (int a = 0; a < 3; a++) {
+        lo[a] = std::min(lo[a], v[a]);
+        hi[a] = std::max(hi[a], v[a]);
+      }
+    }
+  if (hi[0] < 0) return cudaMemsetAsync(d_outT, 0, NC * sizeof(double), c->st) == cudaSuccess
+                            ? RTE_OK : fail(c, RTE_ERR_DEVICE, "memset");
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_dmut, dmut.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
+  const int S = std::max(1, std::min(c->max_split, (4 * 148 + tiles - 1) / tiles));
+  PairArgs a = pair_args(c, d_in, nullptr, 1, S, split_chunk(c->N, S));
+  a.nsplit = (c->N + a.chunk - 1) / a.chunk;
+  a.Kmat = c->K_valid && c->d_K ? c->d_K : nullptr;
+  a.islot = c->d_islot;
+  a.dmut = c->d_dmut;
+  for (int q = 0; q < 3; q++) {
+    a.box_lo[q] = lo[q];
+    a.box_hi[q] = hi[q];
+  }
+  {
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, (c->launches++, rte_launch_pair_tangent(a, c->L, c->precision == RTE_PREC_MIXED ? 0 : 1,
+                                                         c->model == RTE_MODEL_FIM ? 1 : 0, c->st)));
+  }
+  SelfArgs sa;
+  memset(&sa, 0, sizeof sa);
+  sa.N = c->N;
+  sa.nb = 1;
+  sa.Cfull = c->C;
+  sa.Cact = c->C;
+  sa.K = c->K;
+  sa.W = d_in;
+  sa.mut = c->d_mut;
+  sa.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
+  sa.lut = c->d_self_lut;
+  sa.mom = c->d_mom;
+  sa.scale = c->dV / c->cm;
+  sa.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
+  sa.out = c->d_selfp;
+  sa.dmut = c->d_dmut;
+  sa.dlut = c->d_dlut;
+  CUDA_TRY(c, (c->launches++, rte_launch_self(sa, c->st)));
+  EpiArgs e;
+  memset(&e, 0, sizeof e);
+  e.N = c->N;
+  e.nx = c->nx;
+  e.ny = c->ny;
+  e.nz = c->nz;
+  e.Cfull = c->C;
+  e.S = a.nsplit;
+  e.nb = 1;
+  e.part = c->d_part;
+  e.selfp = c->d_selfp;
+  e.mus = c->d_mus;
+  e.flag_scat = 0;
+  e.Wout = d_outT;
+  e.islot = c->d_islot;
+  e.red = c->d_red;
+  CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_epilogue(e, c->L, c->st)));
+  return RTE_OK;
+}
+
+extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* d,
+                          int P, const double* dmua, const double* dmus, double* J, double* F) {
+  if (!c || P < 1 || !dmua || !dmus || !F) return fail(c, RTE_ERR_ARG, "null argument");
+  int rc = check_detector(c, nsrc, srcs, stop, d);
+  if (rc) return rc;
+  for (int q = 0; q < nsrc; q++)
+    if (srcs[q].kind != RTE_SRC_COLUMN && srcs[q].kind != RTE_SRC_FIM && srcs[q].kind != RTE_SRC_BEAM)
+      return fail(c, RTE_ERR_UNSUPPORTED, "the Fisher information takes collimated beams");
+  const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  const int nb = d->nbins;
+  const size_t NB2 = (size_t)6 * nb * nb;
+  if (!c->d_dmut) {
+    CUDA_TRY(c, dalloc(c, &c->d_dmut, (size_t)c->N));
+    CUDA_TRY(c, dalloc(c, &c->d_dmus, (size_t)c->N));
+    CUDA_TRY(c, dalloc(c, &c->d_T, NC));
+    CUDA_TRY(c, dalloc(c, &c->d_cidx, (size_t)std::max(c->nx, std::max(c->ny, c->nz))));
+    CUDA_TRY(c, dalloc(c, &c->d_cval, (size_t)std::max(c->nx, std::max(c->ny, c->nz)) * c->C));
+  }
+  std::vector<double> mut(c->N), mus(c->N);
+  CUDA_TRY(c, cudaMemcpy(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(mus.data(), c->d_mus, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  double scat[RTE_MAX_L + 1];
+  scatter_factors(c, c->cfg.g != 0.0 ? 1 : 0, scat);
+  const size_t a0 = np, a1 = (size_t)c->nz * c->nx, a2 = (size_t)c->nz * c->ny;
+  const size_t off[6] = {0, a0, 2 * a0, 2 * a0 + a1, 2 * a0 + 2 * a1, 2 * a0 + 2 * a1 + a2};
+  std::vector<double> Jpix(npix), dJ(npix), ybar(NB2), dbin(NB2), Js(NB2 * P), dmt(c->N);
+  std::vector<double> coef(c->C);
+  for (int q = 0; q < P * P; q++) F[q] = 0.0;
+  const double h = 1e-20;  // complex-step increment
+  for (int si = 0; si < nsrc; si++) {
+    const rte_source* s = &srcs[si];
+    int terms = 0;
+    rc = forward_with_flux(c, s, stop, Jpix, &terms);  // S -> d_S, out -> d_out
+    if (rc) return rc;
+    bin_faces(c, d, Jpix, ybar.data());
+    std::vector<int> cols;
+    double scale = 1.0;
+    source_columns(c, s, cols, scale);
+    const int face = source_face(s);
+    const int ncol = face < 2 ? c->nz : (face < 4 ? c->ny : c->nx);
+    const double dlen = face < 2 ? c->dz : (face < 4 ? c->dy : c->dx);
+    beam_coefs(c, face, scale, coef.data());
+    for (int p = 0; p < P; p++) {
+      const double* da = dmua + (size_t)p * c->N;
+      const double* ds = dmus + (size_t)p * c->N;
+      for (int r = 0; r < c->N; r++) dmt[r] = da[r] + ds[r];
+      rc = tangent_dA(c, c->d_S, c->d_T, dmt);  // T = dA S
+      if (rc) return rc;
+      CUDA_TRY(c, cudaMemcpyAsync(c->d_dmus, ds, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+      CUDA_TRY(c, (c->launches++, rte_launch_tangent_rhs(c->d_aux1, c->d_T, c->d_out, c->d_mus, c->d_dmus, scat,
+                                                           c->N, c->L, c->st)));
+      // the beam's source column and ballistic transmission, differentiated by a complex step
+      double dball = 0.0;
+      int ball_pix = -1;
+      if (!cols.empty()) {
+        std::vector<int> idx(ncol);
+        std::vector<double> vals((size_t)ncol * c->C);
+        std::complex<double> att(1.0, 0.0);
+        for (int t = 0; t < ncol; t++) {
+          const int r = face_voxel(c, face, cols[0], t);
+          idx[t] = r;
+          const std::complex<double> mt(mut[r], h * dmt[r]), ms(mus[r], h * ds[r]);
+          const std::complex<double> e = std::exp(-mt * dlen);
+          const std::complex<double> amp = ms / mt * (att * (1.0 - e)) / c->dV;
+          att *= e;
+          for (int q = 0; q < c->C; q++) vals[(size_t)t * c->C + q] = amp.imag() / h * coef[q];
+        }
+        dball = s->mag * att.imag() / h;
+        ball_pix = (int)(off[face ^ 1] + cols[0]);
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_cidx, idx.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, c->st));
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_cval, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, c->st));
+        CUDA_TRY(c, (c->launches++, rte_launch_scatter_add(c->d_aux1, c->d_cidx, c->d_cval, ncol, c->C, c->st)));
+      }
+      // dS = (I - DA)^-1 q; the series returns A dS
+      rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, nullptr, nullptr);
+      if (rc) return rc;
+      CUDA_TRY(c, (c->launches++, rte_launch_axpy(c->d_aux2, c->d_T, 1.0, NC, c->st)));  // d out = A dS + dA S
+      FaceArgs fa;
+      memset(&fa, 0, sizeof fa);
+      fa.nx = c->nx;
+      fa.ny = c->ny;
+      fa.nz = c->nz;
+      fa.Cfull = c->C;
+      fa.vstride = c->C;
+      fa.out = c->d_aux2;
+      fa.h = c->d_h;
+      fa.J = c->d_J;
+      CUDA_TRY(c, (c->launches++, rte_launch_face_flux(fa, c->st)));
+      CUDA_TRY(c, cudaMemcpyAsync(dJ.data(), c->d_J, npix * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+      if (ball_pix >= 0) dJ[ball_pix] += dball;
+      bin_faces(c, d, dJ, dbin.data());
+      for (size_t b = 0; b < NB2; b++) Js[b * P + p] = ((d->faces >> (b / ((size_t)nb * nb))) & 1) ? dbin[b] : 0.0;
+    }
+    rc = check_kernel_err(c);
+    if (rc) return rc;
+    if (J) memcpy(J + (size_t)si * NB2 * P, Js.data(), sizeof(double) * NB2 * P);
+    for (size_t b = 0; b < NB2; b++) {
+      if (!((d->faces >> (b / ((size_t)nb * nb))) & 1) || !(ybar[b] > 0.0)) continue;
+      const double w = 1.0 / ybar[b];
+      const double* jb = &Js[b * P];
+      for (int p = 0; p < P; p++)
+        for (int q = 0; q < P; q++) F[(size_t)p * P + q] += w * jb[p] * jb[q];
+    }
+  }
+  return RTE_OK;
 }

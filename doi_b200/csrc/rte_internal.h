@@ -29,6 +29,11 @@ struct PairArgs {
   int cpad;             // FP32 source row length in floats: nb*cstride rounded up to a multiple of 4
   int cstride;          // FP32 row stride of one right-hand side: Cfull rounded up to even
   int* err;             // set to 1 when a bounded wait runs out (kernel result invalid)
+  // tangent pass (k_pair_tangent): derivative of mu_t along a parameter direction, and the voxel
+  // bounding box of its support (pairs whose segment misses the box have no path derivative)
+  const double* dmut;
+  int box_lo[3], box_hi[3];  // (x, y, z) voxel indices
+  const int* islot;          // voxel -> slot (row of the stored kernel)
 };
 
 struct EpiArgs {
@@ -56,6 +61,9 @@ struct SelfArgs {
   double scale;         // dV / cm
   int air_no_self;
   double* out;          // [N][nb][Cfull]
+  // derivative mode: out = scale * dmut(r) * dD/dmu(mu_t(r)) W (dlut rows, or the series' derivative)
+  const double* dmut;   // null: the self term itself
+  const double* dlut;   // [ndistinct][Cfull][Cfull]
 };
 
 struct ImgArgs {
@@ -147,6 +155,11 @@ cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, co
 // over every unordered pair scattering Q * length into the gradient.
 cudaError_t rte_launch_bp_weights(const BpArgs& a, int LA, int fp64, cudaStream_t st);
 cudaError_t rte_launch_bp_walk(const BpArgs& a, int fp64, cudaStream_t st);
+cudaError_t rte_launch_pair_tangent(const PairArgs& a, int LA, int fp64, int table, cudaStream_t st);
+// q = mus * scat_l * T + dmus * scat_l * out (per voxel and coefficient)
+cudaError_t rte_launch_tangent_rhs(double* q, const double* T, const double* out, const double* mus,
+                                   const double* dmus, const double* scat, int N, int L, cudaStream_t st);
+cudaError_t rte_launch_scatter_add(double* dst, const int* idx, const double* vals, int n, int C, cudaStream_t st);
 cudaError_t rte_launch_masked_scale(const double* in, double* out, const uint8_t* mask, const double* fac, int N,
                                     int L, cudaStream_t st);
 cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st);

@@ -291,6 +291,133 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Tangent pair operator: the derivative of the off-diagonal attenuation operator along one
+// parameter direction dmu_t,
+//   out[r] = sum_{r' != r} -dtau(r, r') k(r, r') R(w) (R(w) . W[r']),  dtau = path integral of dmu_t,
+// the same pair walk as the forward operator over the perturbation field.  Pairs whose segment misses
+// the support box of dmu_t are skipped before the walk, pairs with dtau = 0 after it, so a localised
+// perturbation costs far less than a forward pass.  k from the stored FP32 kernel or recomputed.
+__device__ __forceinline__ bool segment_hits_box(float ax, float ay, float az, float bx, float by, float bz,
+                                                 const int* lo, const int* hi) {
+  const float a3[3] = {ax, ay, az}, b3[3] = {bx, by, bz};
+  float t0 = 0.f, t1 = 1.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float l = (float)lo[d] - 0.5001f, h = (float)hi[d] + 0.5001f, dd = b3[d] - a3[d];
+    if (dd == 0.f) {
+      if (a3[d] < l || a3[d] > h) return false;
+    } else {
+      float ta = (l - a3[d]) / dd, tb = (h - a3[d]) / dd;
+      if (ta > tb) {
+        const float x = ta;
+        ta = tb;
+        tb = x;
+      }
+      t0 = fmaxf(t0, ta);
+      t1 = fminf(t1, tb);
+      if (t0 > t1) return false;
+    }
+  }
+  return true;
+}
+
+template <int LA, bool TABLE, typename T>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  __shared__ T sW[RTE_PAIR_TS * C];
+  const int tid = threadIdx.x;
+  const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
+  const bool act = slot < a.N;
+  const int r = act ? a.perm[slot] : 0;
+  const int plane = a.nx * a.ny;
+  const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
+  T acc[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) acc[c] = T(0);
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  const T thr = (T)a.prop_thresh;
+  for (int s0 = sb; s0 < se; s0 += RTE_PAIR_TS) {
+    const int ns = min(RTE_PAIR_TS, se - s0);
+    __syncthreads();
+    for (int q = tid; q < ns * C; q += RTE_PAIR_THREADS) {
+      const int sv = q / C, c = q - sv * C;
+      sW[q] = (T)a.Win[(size_t)(s0 + sv) * a.Cfull + c];
+    }
+    __syncthreads();
+    if (!act) continue;
+    int kp = s0 % a.nx, jp = (s0 / a.nx) % a.ny, ip = s0 / plane;
+    for (int sv = 0; sv < ns; ++sv) {
+      const int rp = s0 + sv;
+      if (rp != r && segment_hits_box((float)k, (float)j, (float)i, (float)kp, (float)jp, (float)ip, a.box_lo, a.box_hi)) {
+        const T ddx = (T)(k - kp) * (T)a.dx, ddy = (T)(j - jp) * (T)a.dy, ddz = (T)(i - ip) * (T)a.dz;
+        const T d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        const T dist = sqrt(d2);
+        if (dist < thr) {
+          int Q;
+          const T dps = path_sum<T, double>(i, j, k, ip, jp, kp, a.dmut, a.nx, plane, Q);
+          if (dps != T(0)) {
+            const T dtau = dps * dist / (T)Q;
+            T kk;
+            if (a.Kmat) {
+              kk = (T)__ldg(a.Kmat + (size_t)a.islot[rp] * a.Kld + slot);
+            } else {
+              int Q2;
+              const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q2);
+              kk = exp(-ps * dist / (T)Q2) * (T)a.kscale / d2;
+            }
+            T R[C];
+            if (TABLE) {
+              double ux, uy, uz;
+              table_direction((double)ddx, (double)ddy, (double)ddz, (double)dist, ux, uy, uz);
+              sh_eval<LA, T>((T)ux, (T)uy, (T)uz, R);
+            } else {
+              const T inv = T(1) / dist;
+              sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
+            }
+            T S = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c) S = fma(R[c], sW[sv * C + c], S);
+            const T t = -dtau * kk * S;
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] = fma(R[c], t, acc[c]);
+          }
+        }
+      }
+      if (++kp == a.nx) {
+        kp = 0;
+        if (++jp == a.ny) {
+          jp = 0;
+          ++ip;
+        }
+      }
+    }
+  }
+  if (act) {
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * a.Cfull;
+#pragma unroll
+    for (int c = 0; c < C; ++c) o[c] = (double)acc[c];
+  }
+}
+
+__global__ void k_tangent_rhs(double* q, const double* T, const double* out, const double* mus, const double* dmus,
+                              ScatTab sc, int N, int L) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = (L + 1) * (L + 1);
+  if (t >= (long long)N * C) return;
+  const int r = (int)(t / C), c = (int)(t % C);
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  q[t] = sc.v[l] * (mus[r] * T[t] + dmus[r] * out[t]);
+}
+
+__global__ void k_scatter_add(double* dst, const int* idx, const double* vals, int n, int C) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * C) return;
+  dst[(size_t)idx[t / C] * C + t % C] += vals[t];
+}
+
+// ---------------------------------------------------------------------------------------------
 // Mixed precision: path integrals, SH and projections in FP32 (SH in FP64 for l >= 7).  NB right-
 // hand sides that share the medium are propagated together: the direction, its SH and the pair
 // kernel are computed once per pair and used NB times.  Sources are visited in slot order (the
@@ -645,17 +772,19 @@ __global__ void k_self(SelfArgs a) {
   double u = 0.0;
   if (!(a.air_no_self && mu == 0.0)) {
     const double* w = a.W + base;
+    const bool der = a.dmut != nullptr;
     if (a.idx) {
-      const double* D = a.lut + ((size_t)a.idx[r] * a.Cfull + c) * a.Cfull;
+      const double* D = (der ? a.dlut : a.lut) + ((size_t)a.idx[r] * a.Cfull + c) * a.Cfull;
       for (int cp = 0; cp < a.Cact; ++cp) u = fma(__ldg(D + cp), __ldg(w + cp), u);
-    } else {
-      for (int kk = a.K - 1; kk >= 0; --kk) {
+    } else {  // D(mu) = sum_k mu^k M_k; its derivative sum_k k mu^(k-1) M_k, both by Horner
+      for (int kk = a.K - 1; kk >= (der ? 1 : 0); --kk) {
         const double* M = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
         double tk = 0.0;
         for (int cp = 0; cp < a.Cact; ++cp) tk = fma(__ldg(M + cp), __ldg(w + cp), tk);
-        u = fma(mu, u, tk);
+        u = fma(mu, u, der ? (double)kk * tk : tk);
       }
     }
+    if (der) u *= a.dmut[r];
   }
   a.out[base + c] = a.scale * u;
 }
@@ -1403,6 +1532,52 @@ cudaError_t rte_launch_face_flux(const FaceArgs& a, cudaStream_t st) {
 cudaError_t rte_launch_adjoint_seed(const FaceArgs& a, cudaStream_t st) {
   const int total = 2 * (a.nx * a.ny + a.nz * a.nx + a.nz * a.ny);
   k_adjoint_seed<<<(total + 127) / 128, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int LA>
+static cudaError_t launch_tangent_LA(const PairArgs& a, int fp64, int table, cudaStream_t st) {
+  dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+  if (fp64) {
+    if (table)
+      k_pair_tangent<LA, true, double><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+    else
+      k_pair_tangent<LA, false, double><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+  } else {
+    if (table)
+      k_pair_tangent<LA, true, float><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+    else
+      k_pair_tangent<LA, false, float><<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_pair_tangent(const PairArgs& a, int LA, int fp64, int table, cudaStream_t st) {
+  switch (LA) {
+    case 0: return launch_tangent_LA<0>(a, fp64, table, st);
+    case 1: return launch_tangent_LA<1>(a, fp64, table, st);
+    case 2: return launch_tangent_LA<2>(a, fp64, table, st);
+    case 3: return launch_tangent_LA<3>(a, fp64, table, st);
+    case 4: return launch_tangent_LA<4>(a, fp64, table, st);
+    case 5: return launch_tangent_LA<5>(a, fp64, table, st);
+    case 6: return launch_tangent_LA<6>(a, fp64, table, st);
+    case 7: return launch_tangent_LA<7>(a, fp64, table, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t rte_launch_tangent_rhs(double* q, const double* T, const double* out, const double* mus,
+                                   const double* dmus, const double* scat, int N, int L, cudaStream_t st) {
+  ScatTab sc;
+  for (int l = 0; l <= RTE_MAX_L; ++l) sc.v[l] = l <= L ? scat[l] : 0.0;
+  const long long n = (long long)N * (L + 1) * (L + 1);
+  k_tangent_rhs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q, T, out, mus, dmus, sc, N, L);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_scatter_add(double* dst, const int* idx, const double* vals, int n, int C, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_scatter_add<<<(n * C + 255) / 256, 256, 0, st>>>(dst, idx, vals, n, C);
   return cudaGetLastError();
 }
 

@@ -33,7 +33,7 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_server_create", "rte_server_submit", "rte_server_wait", "rte_server_cancel", "rte_server_stats",
            "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
            "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
-           "rte_read_image", "rte_region_gradient", "rte_fisher_regions")
+           "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher")
 
 
 class RteError(RuntimeError):
@@ -211,6 +211,8 @@ def load_library():
     L.rte_region_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, ctypes.c_int,
                                       ctypes.c_int, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
+    L.rte_fisher.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.POINTER(_Detector),
+                             ctypes.c_int, dp, dp, dp, dp]
     L.rte_fisher_regions.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.c_int, dp, ctypes.c_int,
                                      dp]
     _LIB = L
@@ -405,6 +407,22 @@ class Context:
                                                  int(bool(compat)), *[_ptr(o) for o in out], ctypes.byref(r1),
                                                  ctypes.byref(r2)), "rte_region_gradient")
         return (*out, r1.value, r2.value)
+
+    def fisher(self, srcs, stop, det, dmua, dmus, want_J=False):
+        """Poisson Fisher information (P x P) of the parameters whose per-voxel derivatives are
+        dmua, dmus (P x N), from tangent solves; with want_J also J, shape
+        (len(srcs), 6, nbins, nbins, P)."""
+        dmua = np.ascontiguousarray(np.asarray(dmua, np.float64).reshape(-1, self.N))
+        dmus = np.ascontiguousarray(np.asarray(dmus, np.float64).reshape(-1, self.N))
+        P = dmua.shape[0]
+        B = len(srcs)
+        F = np.zeros((P, P))
+        J = np.zeros((B, 6, det.nbins, det.nbins, P)) if want_J else None
+        arr = (_Source * B)(*[x.c() for x in srcs])
+        st, d = stop.c(), det.c()
+        self._check(self.lib.rte_fisher(self.h, B, arr, ctypes.byref(st), ctypes.byref(d), P, _ptr(dmua), _ptr(dmus),
+                                        _ptr(J), _ptr(F)), "rte_fisher")
+        return (F, J) if want_J else F
 
     def fisher_regions(self, src, stop, masks, image=1):
         """Poisson Fisher information of the mu_a of each region in masks (P x N booleans)."""

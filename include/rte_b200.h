@@ -190,6 +190,18 @@ int rte_region_gradient(rte_ctx* ctx, const rte_source* src, const rte_stop* sto
 int rte_fisher_regions(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, int P, const uint8_t* masks,
                        int image, double* F);
 
+/* Fisher information of P parameters of the medium (new).  dmua, dmus: P x N arrays, the
+ * derivative of each voxel's mu_a / mu_s with respect to each parameter (e.g. the position and
+ * contrast of an inclusion through a smooth partial-volume rasterisation).  For every collimated
+ * source: one forward solve and P tangent solves of the discrete model (the derivative of the
+ * attenuation operator recomputes the path integral of the parameter direction along every voxel
+ * pair), giving J = d(binned exitant flux)/d(parameter) on the detector of rte_detector_flux; with
+ * Poisson counts F = sum over sources and bins with flux > 0 of J_b,p J_b,q / flux_b.  Exact for the
+ * discrete model when the series converge (RTE_STOP_REL_L2 with a small tolerance).  J (may be NULL):
+ * nsrc * 6 * nbins^2 rows of P.  F: P x P.  Sources: RTE_SRC_COLUMN, RTE_SRC_FIM, RTE_SRC_BEAM. */
+int rte_fisher(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* det,
+               int P, const double* dmua, const double* dmus, double* J, double* F);
+
 /* Batched forward solves (new): nsrc <= 4 sources on the current medium, propagated together so
  * each voxel pair's direction, spherical harmonics and kernel value serve every source.  Outputs
  * are the nsrc single-source results back to back (W_out nsrc*N*C, trans/ref nsrc*nX*nY, each may

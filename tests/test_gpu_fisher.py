@@ -1,0 +1,71 @@
+"""Fisher information from tangent solves (rte_fisher) on the GPU: the sensitivity J of the binned
+exitant flux to the position and contrast of inclusions (smooth partial-volume rasterisation)
+against central finite differences of rte_detector_flux, F against J^T diag(1/flux) J, and the
+mixed-precision F against FP64.  Series run to convergence (relative L2 1e-13) so the tangent of the
+converged model is the exact derivative."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+N_SIDE, L = 9, 2
+
+
+def _problem(rte, prec):
+    sph = rte.random_spheres(N_SIDE, 2, seed=3, rmin=0.15, rmax=0.25)
+    ctx = rte.Context(N_SIDE, N_SIDE, N_SIDE, dx=0.1, nL=L, g=0.9, precision=prec,
+                      kernel_mode=rte.KERNEL_STORE if prec == rte.PREC_MIXED else rte.KERNEL_RECOMPUTE)
+    mua, mus, dmua, dmus = rte.smooth_sphere_phantom(N_SIDE, sph, mua_bg=0.02, mus_bg=2.0)
+    ctx.set_medium_voxel(mua, mus)
+    c = 0.45 - 0.45  # face centres of the 0.9 cm box (x, y centred on 0, z from 0.05 to 0.85)
+    srcs = [rte.Source(pos_x=c, pos_y=c, kind=rte.SRC_BEAM, face=0),
+            rte.Source(pos_y=0.05, pos_z=0.45, kind=rte.SRC_BEAM, face=4)]
+    return ctx, sph, srcs, mua, mus, dmua, dmus
+
+
+def _flux(rte, ctx, sph, srcs, stop, det):
+    mua, mus, _, _ = rte.smooth_sphere_phantom(N_SIDE, sph, mua_bg=0.02, mus_bg=2.0)
+    ctx.set_medium_voxel(mua, mus)
+    return ctx.detector_flux(srcs, stop, det)
+
+
+def test_sensitivity_matches_finite_differences(rte):
+    ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, rte.PREC_FP64)
+    stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-13)
+    det = rte.Detector(nbins=3, faces=63)
+    F, J = ctx.fisher(srcs, stop, det, dmua, dmus, want_J=True)
+    y = ctx.detector_flux(srcs, stop, det)
+    P = dmua.shape[0]
+    for p in range(P):
+        i, k = divmod(p, 4)
+        h = 1e-5 if k < 3 else 1e-5 * sph[i]["ka"]
+        fd = []
+        for sgn in (1, -1):
+            sp = [dict(x) for x in sph]
+            if k < 3:
+                cc = list(sp[i]["c"])
+                cc[k] += sgn * h
+                sp[i]["c"] = cc
+            else:
+                sp[i]["ka"] += sgn * h
+            fd.append(_flux(rte, ctx, sp, srcs, stop, det))
+        fdj = (fd[0] - fd[1]) / (2 * h)
+        assert rel(J[..., p], fdj) < 1e-5, (p, rel(J[..., p], fdj))
+    Jm = J.reshape(-1, P)
+    w = np.where(y.ravel() > 0, 1.0 / np.where(y.ravel() > 0, y.ravel(), 1.0), 0.0)
+    assert rel(F, Jm.T @ (w[:, None] * Jm)) < 1e-12
+    assert np.allclose(F, F.T) and np.linalg.eigvalsh(F).min() > -1e-12 * np.abs(F).max()
+    ctx.close()
+
+
+def test_fisher_mixed_vs_fp64(rte):
+    stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-12)
+    det = rte.Detector(nbins=3, faces=63)
+    out = []
+    for prec in (rte.PREC_FP64, rte.PREC_MIXED):
+        ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, prec)
+        out.append(ctx.fisher(srcs, stop, det, dmua, dmus))
+        ctx.close()
+    assert rel(out[1], out[0]) < 1e-4, rel(out[1], out[0])
