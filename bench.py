@@ -359,6 +359,44 @@ def run_grad(dev):
             "check": "central finite differences on 50 voxels (step 1e-4 rel) in tests/test_gpu_gradient.py"}
 
 
+def run_fisher(dev, n=25, Lq=5, nbins=16, terms=TERMS):
+    """Fisher information of 8 seeded inclusions x (x, y, z, mu_a contrast) = 32 parameters: background
+    mu_a 0.02, mu_s 2, g 0.9, six collimated beams at the face centres, nbins x nbins bins per face,
+    Poisson noise; J from one forward and 32 tangent solves per source (path integrals of each
+    parameter direction recomputed along every pair).  The full configuration is 49^3, L=7, 16x16."""
+    import doi_b200 as R
+    sph = R.random_spheres(n, 8, seed=55, dx=DX)
+    mua, mus, dmua, dmus = R.smooth_sphere_phantom(n, sph, dx=DX, mua_bg=0.02, mus_bg=2.0)
+    ctx = R.Context(n, n, n, dx=DX, nL=Lq, g=0.9, precision=R.PREC_MIXED, kernel_mode=R.KERNEL_STORE, device=dev)
+    ctx.set_medium_voxel(mua, mus)
+    h = n * DX / 2
+    srcs = [R.Source(kind=R.SRC_BEAM, face=0), R.Source(kind=R.SRC_BEAM, face=1, pos_z=n * DX),
+            R.Source(kind=R.SRC_BEAM, face=2, pos_z=h), R.Source(kind=R.SRC_BEAM, face=3, pos_z=h),
+            R.Source(kind=R.SRC_BEAM, face=4, pos_z=h), R.Source(kind=R.SRC_BEAM, face=5, pos_z=h)]
+    stop = R.Stop(R.STOP_FIXED, terms)
+    det = R.Detector(nbins=nbins, faces=63)
+    ctx.fisher(srcs[:1], stop, det, dmua[:1], dmus[:1])  # warm-up (pair kernel, buffers)
+    ctx.stats()
+    ctx.set_profiling(True)
+    t = time.perf_counter()
+    F = ctx.fisher(srcs, stop, det, dmua, dmus)
+    wall = time.perf_counter() - t
+    st = ctx.stats()
+    t = time.perf_counter()
+    ctx.forward_batch(srcs[:2], stop, want_W=False)
+    ctx.forward_batch(srcs[2:4], stop, want_W=False)
+    ctx.forward_batch(srcs[4:], stop, want_W=False)
+    t_fwd = time.perf_counter() - t
+    ctx.close()
+    ev = np.linalg.eigvalsh(F)
+    return {"workload": f"{n}^3 L={Lq}, 8 inclusions x 4 = 32 parameters, 6 face-centre beams, {nbins}x{nbins} bins "
+                        f"x 6 faces, {terms} terms, mixed precision",
+            "seconds": wall, "tangent_solves": 6 * 32, "forward_solves_6src_s": t_fwd,
+            "pair_kernel_ms": st["ms_pair"], "launches": st["launches"],
+            "F_trace": float(np.trace(F)), "F_cond": float(ev.max() / max(ev.min(), 1e-300)),
+            "F_min_eig": float(ev.min())}
+
+
 def hbm_line(traffic, avg_ms):
     """The pair kernel's DRAM bytes per launch (ncu) over its live launch time, against the measured
     HBM copy bandwidth: how far the kernel is from being memory-bound."""
@@ -523,6 +561,7 @@ def run_ours(args):
         if not args.skip_extras:
             line["config1_plain_fp64"] = run_cfg1(dev)
             line["config4_gradient"] = run_grad(dev)
+            line["config5_fisher"] = run_fisher(dev, **({"n": 49, "Lq": 7} if args.fisher_full else {}))
         if args.serve_requests > 0:
             line["serve"] = run_serve(args, dev)
         out = line
@@ -548,7 +587,8 @@ def main():
     ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
     ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
                     help="sources per phantom solved together (1 = one source per solve)")
-    ap.add_argument("--skip-extras", action="store_true", help="skip the config-1 and gradient measurements")
+    ap.add_argument("--skip-extras", action="store_true", help="skip the config-1, gradient and Fisher measurements")
+    ap.add_argument("--fisher-full", action="store_true", help="Fisher at the full 49^3, L=7 size (long)")
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
     ap.add_argument("--serve-rate", type=float, default=1.5,

@@ -1624,6 +1624,37 @@ static int ensure_batch(rte_ctx* c, int nb) {
   return RTE_OK;
 }
 
+// Neumann series of nb right-hand sides together (mixed precision): W_0 in d_bW, the initial running
+// sum in d_bsum ([N][nb][C]); result A sum in d_bres.  Stop rule FIXED or REL_L2 (norms over all
+// right-hand sides).
+static int series_batch(rte_ctx* c, int nb, const rte_stop* stop, int* terms_out, double* rel_out) {
+  const int vs = nb * c->C;
+  const int cp = (nb * c->cstride + 3) / 4 * 4;
+  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
+  const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
+  int terms = 0;
+  double rel = 0.0;
+  while (terms < stop->max_terms) {
+    int rc = apply_term(c, c->d_bW, c->d_bWf, c->d_bWn, c->d_bWf, c->d_bsum, flag_l, 1, nb);
+    if (rc) return rc;
+    std::swap(c->d_bW, c->d_bWn);
+    terms++;
+    if (stop->rule == RTE_STOP_REL_L2) {
+      double hred[4];
+      CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+      rel = hred[1] > 0 ? sqrt(hred[0] / hred[1]) : 0.0;
+      if (rel < stop->tol) break;
+    }
+  }
+  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bsum, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
+  int rc = apply_term(c, c->d_bsum, c->d_bWf, c->d_bres, nullptr, nullptr, 1, 0, nb);
+  if (!rc) rc = check_kernel_err(c);
+  if (terms_out) *terms_out = terms;
+  if (rel_out) *rel_out = rel;
+  return rc;
+}
+
 extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
                                  rte_cplx* W_out, rte_cplx* trans, rte_cplx* ref, rte_report* rep) {
   if (!c || !srcs || !stop || nsrc < 1) return fail(c, RTE_ERR_ARG, "bad argument");
@@ -1668,26 +1699,9 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   // W0 -> d_bW, S0 -> d_bsum
   rc = series_start(c, c->d_bsum, c->d_bq, c->d_bW, nb, c->d_bWf, cp);
   if (rc) return rc;
-  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
-  const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
   int terms = 0;
   double rel = 0.0;
-  while (terms < stop->max_terms) {
-    rc = apply_term(c, c->d_bW, c->d_bWf, c->d_bWn, c->d_bWf, c->d_bsum, flag_l, 1, nb);
-    if (rc) return rc;
-    std::swap(c->d_bW, c->d_bWn);
-    terms++;
-    if (stop->rule == RTE_STOP_REL_L2) {
-      double hred[4];
-      CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-      CUDA_TRY(c, cudaStreamSynchronize(c->st));
-      rel = hred[1] > 0 ? sqrt(hred[0] / hred[1]) : 0.0;
-      if (rel < stop->tol) break;
-    }
-  }
-  CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bsum, c->d_bWf, c->d_islot, c->N, vs, cp, c->C, c->cstride, c->st)));
-  rc = apply_term(c, c->d_bsum, c->d_bWf, c->d_bres, nullptr, nullptr, 1, 0, nb);
-  if (!rc) rc = check_kernel_err(c);
+  rc = series_batch(c, nb, stop, &terms, &rel);
   for (int b = 0; b < nsrc && !rc && (trans || ref); b++)
     rc = run_images(c, c->d_bres + b * c->C, &srcs[b], true, trans ? trans + b * np : nullptr,
                     ref ? ref + b * np : nullptr, vs, c->d_bball + b * npix);
@@ -2495,10 +2509,15 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
   const int nb = d->nbins;
   const size_t NB2 = (size_t)6 * nb * nb;
+  const int nbt = c->precision == RTE_PREC_MIXED ? 2 : 1;  // tangent series run together
+  if (nbt > 1) {
+    rc = ensure_batch(c, nbt);
+    if (rc) return rc;
+  }
   if (!c->d_dmut) {
     CUDA_TRY(c, dalloc(c, &c->d_dmut, (size_t)c->N));
     CUDA_TRY(c, dalloc(c, &c->d_dmus, (size_t)c->N));
-    CUDA_TRY(c, dalloc(c, &c->d_T, NC));
+    CUDA_TRY(c, dalloc(c, &c->d_T, 2 * NC));
     CUDA_TRY(c, dalloc(c, &c->d_cidx, (size_t)std::max(c->nx, std::max(c->ny, c->nz))));
     CUDA_TRY(c, dalloc(c, &c->d_cval, (size_t)std::max(c->nx, std::max(c->ny, c->nz)) * c->C));
   }
@@ -2526,57 +2545,79 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
     const int ncol = face < 2 ? c->nz : (face < 4 ? c->ny : c->nx);
     const double dlen = face < 2 ? c->dz : (face < 4 ? c->dy : c->dx);
     beam_coefs(c, face, scale, coef.data());
-    for (int p = 0; p < P; p++) {
-      const double* da = dmua + (size_t)p * c->N;
-      const double* ds = dmus + (size_t)p * c->N;
-      for (int r = 0; r < c->N; r++) dmt[r] = da[r] + ds[r];
-      rc = tangent_dA(c, c->d_S, c->d_T, dmt);  // T = dA S
-      if (rc) return rc;
-      CUDA_TRY(c, cudaMemcpyAsync(c->d_dmus, ds, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
-      CUDA_TRY(c, (c->launches++, rte_launch_tangent_rhs(c->d_aux1, c->d_T, c->d_out, c->d_mus, c->d_dmus, scat,
-                                                           c->N, c->L, c->st)));
-      // the beam's source column and ballistic transmission, differentiated by a complex step
-      double dball = 0.0;
+    // parameters in groups of nbt: the tangent series of a group run together (mixed precision)
+    for (int p0 = 0; p0 < P; p0 += nbt) {
+      const int vs = nbt * c->C;
+      double* q = nbt == 1 ? c->d_aux1 : c->d_bW;
+      if (nbt > 1) CUDA_TRY(c, cudaMemsetAsync(q, 0, NC * nbt * sizeof(double), c->st));
+      double dball[4] = {0, 0, 0, 0};
       int ball_pix = -1;
-      if (!cols.empty()) {
-        std::vector<int> idx(ncol);
-        std::vector<double> vals((size_t)ncol * c->C);
-        std::complex<double> att(1.0, 0.0);
-        for (int t = 0; t < ncol; t++) {
-          const int r = face_voxel(c, face, cols[0], t);
-          idx[t] = r;
-          const std::complex<double> mt(mut[r], h * dmt[r]), ms(mus[r], h * ds[r]);
-          const std::complex<double> e = std::exp(-mt * dlen);
-          const std::complex<double> amp = ms / mt * (att * (1.0 - e)) / c->dV;
-          att *= e;
-          for (int q = 0; q < c->C; q++) vals[(size_t)t * c->C + q] = amp.imag() / h * coef[q];
+      for (int b = 0; b < nbt && p0 + b < P; b++) {
+        const int p = p0 + b;
+        const double* da = dmua + (size_t)p * c->N;
+        const double* ds = dmus + (size_t)p * c->N;
+        for (int r = 0; r < c->N; r++) dmt[r] = da[r] + ds[r];
+        rc = tangent_dA(c, c->d_S, c->d_T + (size_t)b * NC, dmt);  // T = dA S
+        if (rc) return rc;
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_dmus, ds, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+        CUDA_TRY(c, (c->launches++, rte_launch_tangent_rhs(q + (size_t)b * c->C, vs, c->d_T + (size_t)b * NC, c->d_out,
+                                                             c->d_mus, c->d_dmus, scat, c->N, c->L, c->st)));
+        // the beam's source column and ballistic transmission, differentiated by a complex step
+        if (!cols.empty()) {
+          std::vector<int> idx(ncol);
+          std::vector<double> vals((size_t)ncol * c->C);
+          std::complex<double> att(1.0, 0.0);
+          for (int t = 0; t < ncol; t++) {
+            const int r = face_voxel(c, face, cols[0], t);
+            idx[t] = r;
+            const std::complex<double> mt(mut[r], h * dmt[r]), ms(mus[r], h * ds[r]);
+            const std::complex<double> e = std::exp(-mt * dlen);
+            const std::complex<double> amp = ms / mt * (att * (1.0 - e)) / c->dV;
+            att *= e;
+            for (int k = 0; k < c->C; k++) vals[(size_t)t * c->C + k] = amp.imag() / h * coef[k];
+          }
+          dball[b] = s->mag * att.imag() / h;
+          ball_pix = (int)(off[face ^ 1] + cols[0]);
+          CUDA_TRY(c, cudaMemcpyAsync(c->d_cidx, idx.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, c->st));
+          CUDA_TRY(c, cudaMemcpyAsync(c->d_cval, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice,
+                                      c->st));
+          CUDA_TRY(c, (c->launches++, rte_launch_scatter_add(q + (size_t)b * c->C, vs, c->d_cidx, c->d_cval, ncol, c->C,
+                                                               c->st)));
         }
-        dball = s->mag * att.imag() / h;
-        ball_pix = (int)(off[face ^ 1] + cols[0]);
-        CUDA_TRY(c, cudaMemcpyAsync(c->d_cidx, idx.data(), sizeof(int) * ncol, cudaMemcpyHostToDevice, c->st));
-        CUDA_TRY(c, cudaMemcpyAsync(c->d_cval, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, c->st));
-        CUDA_TRY(c, (c->launches++, rte_launch_scatter_add(c->d_aux1, c->d_cidx, c->d_cval, ncol, c->C, c->st)));
       }
       // dS = (I - DA)^-1 q; the series returns A dS
-      rc = neumann_real(c, c->d_aux1, c->d_aux1, c->d_aux2, 1, stop, -1, nullptr, nullptr);
+      const double* res;
+      if (nbt == 1) {
+        rc = neumann_real(c, q, q, c->d_aux2, 1, stop, -1, nullptr, nullptr);
+        res = c->d_aux2;
+      } else {
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_bsum, q, NC * nbt * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        rc = series_batch(c, nbt, stop, nullptr, nullptr);
+        res = c->d_bres;
+      }
       if (rc) return rc;
-      CUDA_TRY(c, (c->launches++, rte_launch_axpy(c->d_aux2, c->d_T, 1.0, NC, c->st)));  // d out = A dS + dA S
-      FaceArgs fa;
-      memset(&fa, 0, sizeof fa);
-      fa.nx = c->nx;
-      fa.ny = c->ny;
-      fa.nz = c->nz;
-      fa.Cfull = c->C;
-      fa.vstride = c->C;
-      fa.out = c->d_aux2;
-      fa.h = c->d_h;
-      fa.J = c->d_J;
-      CUDA_TRY(c, (c->launches++, rte_launch_face_flux(fa, c->st)));
-      CUDA_TRY(c, cudaMemcpyAsync(dJ.data(), c->d_J, npix * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-      CUDA_TRY(c, cudaStreamSynchronize(c->st));
-      if (ball_pix >= 0) dJ[ball_pix] += dball;
-      bin_faces(c, d, dJ, dbin.data());
-      for (size_t b = 0; b < NB2; b++) Js[b * P + p] = ((d->faces >> (b / ((size_t)nb * nb))) & 1) ? dbin[b] : 0.0;
+      for (int b = 0; b < nbt && p0 + b < P; b++) {
+        const int p = p0 + b;
+        // d out = A dS + dA S
+        CUDA_TRY(c, (c->launches++, rte_launch_strided_add(c->d_aux4, res + (size_t)b * c->C, vs,
+                                                             c->d_T + (size_t)b * NC, c->N, c->C, c->st)));
+        FaceArgs fa;
+        memset(&fa, 0, sizeof fa);
+        fa.nx = c->nx;
+        fa.ny = c->ny;
+        fa.nz = c->nz;
+        fa.Cfull = c->C;
+        fa.vstride = c->C;
+        fa.out = c->d_aux4;
+        fa.h = c->d_h;
+        fa.J = c->d_J;
+        CUDA_TRY(c, (c->launches++, rte_launch_face_flux(fa, c->st)));
+        CUDA_TRY(c, cudaMemcpyAsync(dJ.data(), c->d_J, npix * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CUDA_TRY(c, cudaStreamSynchronize(c->st));
+        if (ball_pix >= 0) dJ[ball_pix] += dball[b];
+        bin_faces(c, d, dJ, dbin.data());
+        for (size_t k = 0; k < NB2; k++) Js[k * P + p] = ((d->faces >> (k / ((size_t)nb * nb))) & 1) ? dbin[k] : 0.0;
+      }
     }
     rc = check_kernel_err(c);
     if (rc) return rc;

@@ -156,10 +156,13 @@ cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, co
 cudaError_t rte_launch_bp_weights(const BpArgs& a, int LA, int fp64, cudaStream_t st);
 cudaError_t rte_launch_bp_walk(const BpArgs& a, int fp64, cudaStream_t st);
 cudaError_t rte_launch_pair_tangent(const PairArgs& a, int LA, int fp64, int table, cudaStream_t st);
-// q = mus * scat_l * T + dmus * scat_l * out (per voxel and coefficient)
-cudaError_t rte_launch_tangent_rhs(double* q, const double* T, const double* out, const double* mus,
+// q = mus * scat_l * T + dmus * scat_l * out (per voxel and coefficient; q rows qstride apart)
+cudaError_t rte_launch_tangent_rhs(double* q, int qstride, const double* T, const double* out, const double* mus,
                                    const double* dmus, const double* scat, int N, int L, cudaStream_t st);
-cudaError_t rte_launch_scatter_add(double* dst, const int* idx, const double* vals, int n, int C, cudaStream_t st);
+cudaError_t rte_launch_scatter_add(double* dst, int dstride, const int* idx, const double* vals, int n, int C,
+                                   cudaStream_t st);
+cudaError_t rte_launch_strided_add(double* dst, const double* a, int astride, const double* b, int N, int C,
+                                   cudaStream_t st);
 cudaError_t rte_launch_masked_scale(const double* in, double* out, const uint8_t* mask, const double* fac, int N,
                                     int L, cudaStream_t st);
 cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st);

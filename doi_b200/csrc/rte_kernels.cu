@@ -400,21 +400,30 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
   }
 }
 
-__global__ void k_tangent_rhs(double* q, const double* T, const double* out, const double* mus, const double* dmus,
-                              ScatTab sc, int N, int L) {
+// q (rows qstride apart) = scat_l (mu_s T + dmu_s out): the tangent right-hand side D dA S + dD A S
+__global__ void k_tangent_rhs(double* q, int qstride, const double* T, const double* out, const double* mus,
+                              const double* dmus, ScatTab sc, int N, int L) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int C = (L + 1) * (L + 1);
   if (t >= (long long)N * C) return;
   const int r = (int)(t / C), c = (int)(t % C);
   int l = 0;
   while ((l + 1) * (l + 1) <= c) ++l;
-  q[t] = sc.v[l] * (mus[r] * T[t] + dmus[r] * out[t]);
+  q[(size_t)r * qstride + c] = sc.v[l] * (mus[r] * T[t] + dmus[r] * out[t]);
 }
 
-__global__ void k_scatter_add(double* dst, const int* idx, const double* vals, int n, int C) {
+__global__ void k_scatter_add(double* dst, int dstride, const int* idx, const double* vals, int n, int C) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * C) return;
-  dst[(size_t)idx[t / C] * C + t % C] += vals[t];
+  dst[(size_t)idx[t / C] * dstride + t % C] += vals[t];
+}
+
+// dst [N][C] = a (rows astride apart) + b [N][C]
+__global__ void k_strided_add(double* dst, const double* a, int astride, const double* b, int N, int C) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * C) return;
+  const int r = (int)(t / C), c = (int)(t % C);
+  dst[t] = a[(size_t)r * astride + c] + b[t];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1566,18 +1575,26 @@ cudaError_t rte_launch_pair_tangent(const PairArgs& a, int LA, int fp64, int tab
   return cudaErrorInvalidValue;
 }
 
-cudaError_t rte_launch_tangent_rhs(double* q, const double* T, const double* out, const double* mus,
+cudaError_t rte_launch_tangent_rhs(double* q, int qstride, const double* T, const double* out, const double* mus,
                                    const double* dmus, const double* scat, int N, int L, cudaStream_t st) {
   ScatTab sc;
   for (int l = 0; l <= RTE_MAX_L; ++l) sc.v[l] = l <= L ? scat[l] : 0.0;
   const long long n = (long long)N * (L + 1) * (L + 1);
-  k_tangent_rhs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q, T, out, mus, dmus, sc, N, L);
+  k_tangent_rhs<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(q, qstride, T, out, mus, dmus, sc, N, L);
   return cudaGetLastError();
 }
 
-cudaError_t rte_launch_scatter_add(double* dst, const int* idx, const double* vals, int n, int C, cudaStream_t st) {
+cudaError_t rte_launch_scatter_add(double* dst, int dstride, const int* idx, const double* vals, int n, int C,
+                                   cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_scatter_add<<<(n * C + 255) / 256, 256, 0, st>>>(dst, idx, vals, n, C);
+  k_scatter_add<<<(n * C + 255) / 256, 256, 0, st>>>(dst, dstride, idx, vals, n, C);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_strided_add(double* dst, const double* a, int astride, const double* b, int N, int C,
+                                   cudaStream_t st) {
+  const long long n = (long long)N * C;
+  k_strided_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dst, a, astride, b, N, C);
   return cudaGetLastError();
 }
 
