@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librte_b200.so")
 BINDIR = os.path.join(HERE, "bin")
-SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp", "rte_par.cpp"]
+SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp", "rte_par.cpp", "rte_faces.cpp"]
 CLI = "rte_cli.cpp"  # built into bin/ by build_cli, not into the library
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

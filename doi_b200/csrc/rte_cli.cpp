@@ -111,6 +111,22 @@ int main_forward(const char* path) {
     return die(L.ctx, L.pr.trans_file, rc);
   if (L.pr.ref_file[0] && (rc = rte_write_image(L.pr.ref_file, c.nx, c.ny, rf.data(), cpu_layout)))
     return die(L.ctx, L.pr.ref_file, rc);
+  if (L.pr.style == 1) {  // the CPU package's side-face images and photon number (RTE_uniform.c:184-185)
+    std::vector<rte_cplx> sx0((size_t)c.nz * c.ny), sx1(sx0.size()), sy0((size_t)c.nz * c.nx), sy1(sy0.size());
+    rte_cplx ph{0, 0};
+    rc = rte_cpu_face_outputs(&c, W.data(), &L.pr.src, L.pr.mua[1] + L.pr.mus[1], sx0.data(), sx1.data(), sy0.data(),
+                              sy1.data(), &ph);
+    if (rc) return die(L.ctx, "rte_cpu_face_outputs", rc);
+    const char* names[4] = {"SideFace1(-X).out", "SideFace2(+X).out", "SideFace3(-Y).out", "SideFace4(+Y).out"};
+    std::vector<rte_cplx>* imgs[4] = {&sx0, &sx1, &sy0, &sy1};
+    for (int q = 0; q < 4; q++) {
+      // the package writes these buffers through its z-face writer (nX x nY values read in order)
+      std::vector<rte_cplx> buf(np, rte_cplx{0, 0});
+      for (size_t e = 0; e < np && e < imgs[q]->size(); e++) buf[e] = (*imgs[q])[e];
+      if ((rc = rte_write_image(names[q], c.nx, c.ny, buf.data(), 1))) return die(L.ctx, names[q], rc);
+    }
+    printf("Number of photons total: %f\n", ph.re);
+  }
   if (L.pr.phase_file[0] && L.pr.style == 0) {
     const std::vector<double> ph = phase_image(L, W);
     if ((rc = rte_write_phase_image(L.pr.phase_file, c.nx, c.ny, ph.data()))) return die(L.ctx, L.pr.phase_file, rc);

@@ -34,6 +34,8 @@ namespace {
 
 inline int ncoef(int L) { return (L + 1) * (L + 1); }
 
+}  // namespace
+
 // ---------------------------------------------------------------------------------------
 // Real spherical harmonics (host copy of the device recurrence in rte_kernels.cu).
 // Normalisation K_lm = sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!) (times sqrt2 for m > 0) of the
@@ -90,6 +92,8 @@ void sh_real_host(const ShTables& t, int L, double x, double y, double z, double
     }
   }
 }
+
+namespace {
 
 // Legendre polynomial P_l(u) (m = 0 associated Legendre of sph_harm.cu:172-237).
 double legendre(int l, double u) {

@@ -173,6 +173,9 @@ cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut,
                               int N, double* red_max, cudaStream_t st);
 cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks);
 cudaError_t rte_upload_sh_tables(const ShTables& t);
+// host copies: the recurrence tables and the real SH R_c at a unit direction (index l*l + l + m)
+ShTables make_sh_tables();
+void sh_real_host(const ShTables& t, int L, double x, double y, double z, double* R);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
 cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm);

@@ -33,7 +33,8 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_server_create", "rte_server_submit", "rte_server_wait", "rte_server_cancel", "rte_server_stats",
            "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
            "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
-           "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher")
+           "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
+           "rte_cpu_face_outputs")
 
 
 class RteError(RuntimeError):
@@ -211,6 +212,8 @@ def load_library():
     L.rte_region_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, ctypes.c_int,
                                       ctypes.c_int, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
+    L.rte_cpu_face_outputs.argtypes = [ctypes.POINTER(_Config), dp, ctypes.POINTER(_Source), ctypes.c_double, dp, dp,
+                                       dp, dp, dp]
     L.rte_fisher.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.POINTER(_Detector),
                              ctypes.c_int, dp, dp, dp, dp]
     L.rte_fisher_regions.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.c_int, dp, ctypes.c_int,
@@ -611,3 +614,22 @@ def read_image(path, nx, ny):
     if rc != 0:
         raise RteError(f"rte_read_image failed ({rc})")
     return out.reshape(ny, nx)
+
+
+def cpu_face_outputs(W, nx, ny, nz, nL, x_min, x_max, y_min, y_max, z_min, z_max, src, mu_t, c=1.0, n=1.0):
+    """The CPU package's side-face images (-x, +x, -y, +y; x faces (nY, nZ), y faces (nX, nZ)) and
+    photon number of a final distribution W (N x C complex, reference layout); host computation."""
+    lib = load_library()
+    cfg = _Config(nx, ny, nz, x_min, x_max, y_min, y_max, z_min, z_max, nL, 0.0, 1, 0.0, n, c, MODEL_CPU, 0, 0, 0)
+    W = np.ascontiguousarray(W, np.complex128)
+    sx0 = np.zeros(nz * ny, np.complex128)
+    sx1 = np.zeros(nz * ny, np.complex128)
+    sy0 = np.zeros(nz * nx, np.complex128)
+    sy1 = np.zeros(nz * nx, np.complex128)
+    ph = np.zeros(1, np.complex128)
+    s = src.c()
+    rc = lib.rte_cpu_face_outputs(ctypes.byref(cfg), _ptr(W), ctypes.byref(s), float(mu_t), _ptr(sx0), _ptr(sx1),
+                                  _ptr(sy0), _ptr(sy1), _ptr(ph))
+    if rc != 0:
+        raise RteError(f"rte_cpu_face_outputs failed ({rc})")
+    return [sx0.reshape(ny, nz), sx1.reshape(ny, nz), sy0.reshape(nx, nz), sy1.reshape(nx, nz)], ph[0]

@@ -316,6 +316,16 @@ int rte_write_image(const char* path, int nx, int ny, const rte_cplx* img, int c
 int rte_write_phase_image(const char* path, int nx, int ny, const double* phase);
 int rte_read_image(const char* path, int nx, int ny, double* out);
 
+/* The CPU package's boundary outputs of a final distribution W (N*C complex, reference layout;
+ * host code, no context): the side-face images of ComputeSideFaceImages (CPU package/src/Dist.c:
+ * 353-532; x faces nZ*nY values at k + j*nZ, y faces nZ*nX at k + i*nZ; each pointer may be NULL) and
+ * the photon number of ComputePhotonNumber (Dist.c:538-989: outgoing and "incoming" hemisphere sums
+ * on all six faces plus the ballistic beam, with the package's 101 x 101 rectangle rule and its uniform
+ * mu_t).  cfg gives the geometry, nL and c / n. */
+int rte_cpu_face_outputs(const rte_config* cfg, const rte_cplx* W, const rte_source* src, double mu_t,
+                         rte_cplx* side_x0, rte_cplx* side_x1, rte_cplx* side_y0, rte_cplx* side_y1,
+                         rte_cplx* photons);
+
 /* ---- allocation-free entry point (no counterpart in the reference) ------------------
  * For callers that must not allocate device memory when they run the solver: work recorded
  * into a CUDA graph (cudaMalloc is illegal during stream capture), plug-ins whose host

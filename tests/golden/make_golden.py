@@ -143,14 +143,12 @@ def cpu_case(name, n, nL, mua, mus, g, diam):
     log = run([os.path.join(ROOT, "oracle", "_ref", "rte_cpu"), "c.par"], d)
     terms = int([l for l in log.splitlines() if l.startswith("Neumann series:")][-1].split()[-1]) - 1
     photons = float([l for l in log.splitlines() if l.startswith("Number of photons total")][-1].split()[-1])
-    side = {}
-    for f in os.listdir(d):
-        if f.startswith("SideFace"):
-            b = open(os.path.join(d, f), "rb").read()
-            side[f.split(".")[0]] = np.frombuffer(b, np.uint8)
+    # the four side-face images, same file layout as the z-face images (Dist.c:353-532)
+    side = {f"side{q}": read_img(os.path.join(d, f"SideFace{q}({ax}).out"))
+            for q, ax in ((1, "-X"), (2, "+X"), (3, "-Y"), (4, "+Y"))}
     np.savez_compressed(os.path.join(HERE, name + ".npz"), n=n, nL=nL, mua=mua, mus=mus, g=g, diam=diam,
                         trans=read_img(os.path.join(d, "trans.out")), ref=read_img(os.path.join(d, "ref.out")),
-                        terms=terms, photons=photons, par=par)
+                        terms=terms, photons=photons, par=par, **side)
     print("wrote", name, "terms", terms)
 
 
@@ -158,6 +156,15 @@ def main():
     if not os.path.isdir(REF):
         sys.exit(f"reference tree {REF} not found")
     subprocess.run(["bash", os.path.join(ROOT, "oracle", "build.sh")], check=True)
+    if "--cpu-only" not in sys.argv:
+        fim_cases()
+    # 4. the CPU package on the 11^3, L=3 configuration (uniform, g = 0.8)
+    cpu_case("cpu_uniform_11_L3", 11, 3, 0.01, 1.0, 0.8, 0.1)
+    # 5. the CPU package, isotropic scattering (g = 0: only l = 0 propagated), 9^3, L=2
+    cpu_case("cpu_isotropic_9_L2", 9, 2, 0.05, 2.0, 0.0, 0.1)
+
+
+def fim_cases():
     rng = np.random.default_rng(2024)
     # 1. uniform medium, 10x10x20, L=2, the reference stop rule (FIM forward)
     fim_case("fim_uniform_10x10x20_L2", 10, 10, 20, 2, np.ones(2000, np.uint8), [0.0, 0.01], [0.0, 1.0],
@@ -173,10 +180,6 @@ def main():
     # 3. the shipped non-uniform 20^3 tissue map, L=1
     shipped = np.fromfile(os.path.join(REF, "GPU package", "utility", "tiss_map_nonuni.bin"), np.uint8)
     fim_case("fim_shipped_nonuni_20_L1", 20, 20, 20, 1, shipped, [0.0, 0.01, 0.02, 0.03], [0.0, 1.0, 1.2, 0.8])
-    # 4. the CPU package on the 11^3, L=3 configuration (uniform, g = 0.8)
-    cpu_case("cpu_uniform_11_L3", 11, 3, 0.01, 1.0, 0.8, 0.1)
-    # 5. the CPU package, isotropic scattering (g = 0: only l = 0 propagated), 9^3, L=2
-    cpu_case("cpu_isotropic_9_L2", 9, 2, 0.05, 2.0, 0.0, 0.1)
 
 
 if __name__ == "__main__":

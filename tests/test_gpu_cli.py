@@ -146,3 +146,25 @@ def test_rte_inv_matches_oracle(rte, oracle, tmp_path):
         assert abs(got[t - 1][0] - ga) <= 1e-3 * abs(ga), (t, got[t - 1][0], ga)
         assert abs(got[t - 1][1] - gs) <= 1e-3 * abs(gs), (t, got[t - 1][1], gs)
     assert os.path.getsize(os.path.join(d, "Residual.out")) == 8
+
+
+@pytest.mark.parametrize("case", ["cpu_uniform_11_L3", "cpu_isotropic_9_L2"])
+def test_rte_gpu_on_cpu_package_files(rte, tmp_path, case):
+    """A CPU-package parameter file (uniform medium keys): same images, side-face files and printed
+    photon number as the CPU package itself."""
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    d = str(tmp_path)
+    text = str(g["par"])
+    for k, f in (("TransFile", "trans.out"), ("ReflectFile", "ref.out"), ("PhaseFile", "phase.out")):
+        text = re.sub(rf"(?im)^{k}\s*=.*$", f"{k} = {d}/{f}", text)
+    par = os.path.join(d, "c.par")
+    open(par, "w").write(text)
+    r = subprocess.run([_exe(rte, "rte_gpu"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+    assert f"Neumann series: {int(g['terms'])} terms" in r.stdout
+    assert rel(_read_img(os.path.join(d, "trans.out")), g["trans"]) < 1e-10
+    assert rel(_read_img(os.path.join(d, "ref.out")), g["ref"]) < 1e-10
+    for q, ax in ((1, "-X"), (2, "+X"), (3, "-Y"), (4, "+Y")):
+        assert rel(_read_img(os.path.join(d, f"SideFace{q}({ax}).out")), g[f"side{q}"]) < 1e-10
+    ph = float(re.search(r"Number of photons total: (\S+)", r.stdout).group(1))
+    assert abs(ph - float(g["photons"])) < 2e-6

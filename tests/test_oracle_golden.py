@@ -81,3 +81,25 @@ def test_cpu_package_forward(oracle, case):
     assert r["terms"] == int(g["terms"])
     assert rel(r["trans"], g["trans"]) < 1e-12
     assert rel(r["ref"], g["ref"]) < 1e-12
+
+
+@pytest.mark.parametrize("case", CPU_CASES)
+def test_cpu_package_side_faces_and_photons(rte, oracle, case):
+    """rte_cpu_face_outputs on the oracle's final distribution reproduces the CPU package's side-face
+    images (1e-12) and its printed photon number (6 decimals) for the same input."""
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    n, L = int(g["n"]), int(g["nL"])
+    N = n ** 3
+    lo, hi = -n * 0.05, n * 0.05
+    p = oracle.params(n, n, n, 0.1, 0.1, 0.1, L, float(g["g"]), 1.0, 10.0, mode=oracle.MODE_CPU, x_min=lo, y_min=lo)
+    mua, mus = np.full(N, float(g["mua"])), np.full(N, float(g["mus"]))
+    r = oracle.forward(p, mua, mus, src_kind=oracle.SRC_CPU, img_mode=2, stop_rule=oracle.STOP_REFERENCE, n0=1,
+                       diam=float(g["diam"]))
+    src = rte.Source(diam=float(g["diam"]), kind=rte.SRC_CPU)
+    sides, ph = rte.rte.cpu_face_outputs(r["out"], n, n, n, L, lo, hi, lo, hi, 0.0, n * 0.1, src,
+                                         float(g["mua"]) + float(g["mus"]))
+    for q in range(4):
+        # the package writes each side image through its z-face writer: header (nX, nY), then the
+        # buffer (index k + u*nZ) in order -- for these cubic grids the same array read as (nY, nX)
+        assert rel(sides[q].ravel(), g[f"side{q + 1}"].ravel()) < 1e-12, q
+    assert abs(ph.real - float(g["photons"])) < 5e-7
