@@ -12,7 +12,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librte_b200.so")
 BINDIR = os.path.join(HERE, "bin")
-SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp", "rte_par.cpp", "rte_faces.cpp"]
+SOURCES = ["rte_kernels.cu", "rte_noalloc.cu", "rte_host.cpp", "rte_server.cpp", "rte_par.cpp", "rte_faces.cpp",
+           "rte_fft.cpp"]
 CLI = "rte_cli.cpp"  # built into bin/ by build_cli, not into the library
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -52,7 +53,7 @@ def build(verbose=False, force=False, ptxas_verbose=False):
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc(), "-shared"] + ARCH + ["-o", LIB] + objs + ["-lpthread"]
+    cmd = [nvcc(), "-shared"] + ARCH + ["-o", LIB] + objs + ["-lcufft", "-lpthread"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
@@ -63,7 +64,7 @@ def build(verbose=False, force=False, ptxas_verbose=False):
 
 
 def build_cli(verbose=False):
-    """The reference's program names (rte_gpu, rte_inv, rte_test, rte_fim) as one executable over the
+    """The reference's program names (rte_gpu, rte_inv, rte_test, rte_fim, rte_snr) as one executable over the
     library, in doi_b200/bin (run-time path to ../lib)."""
     os.makedirs(BINDIR, exist_ok=True)
     exe = os.path.join(BINDIR, "rte_gpu")
@@ -72,7 +73,7 @@ def build_cli(verbose=False):
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    for name in ("rte_inv", "rte_test", "rte_fim"):
+    for name in ("rte_inv", "rte_test", "rte_fim", "rte_snr"):
         link = os.path.join(BINDIR, name)
         if os.path.lexists(link):
             os.remove(link)

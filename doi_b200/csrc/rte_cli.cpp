@@ -8,6 +8,7 @@
 //                      (FisherInfo_IO/src/compute_grad_rte.cu:205-385), one line per tissue type
 //   rte_fim file.par   Fisher information of the mu_a of a spherical region on the reflection
 //                      image (FisherInfo_IO/src/rte_fim.cu:236-331)
+//   rte_snr file.par   detection SNR of a mu_a lesion against depth (FisherInfo_IO/src/rte_snr.cu)
 //
 // One executable; the program is chosen by the name it is called under (build.py links the three
 // names).  Argument and error conventions follow the reference mains: a usage line and exit status 1
@@ -17,6 +18,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include <stdint.h>
 
 #include <complex>
 #include <string>
@@ -187,6 +190,75 @@ int main_inverse(const char* path) {
   return 0;
 }
 
+// rte_snr (FisherInfo_IO/src/rte_snr.cu:80-385): squared detection SNR of a spherical mu_a lesion
+// (radius 3 fov / (2 nX), tissue 2, mu_a 0.35 against 0.25, mu_s 1) at depths z index 2 .. 15 on the
+// reflection image, SNR^2 = sum_j (g1_j - g0_j)^2 / g0_j, written to snr_terms.dat (nZ - 2 doubles).
+// The reference steps its depth loop with `loc_indz = loc_indz++` (undefined in C); here it steps by
+// one and stops at the last layer of small grids.
+int main_snr(const char* path) {
+  Loaded L;
+  if (load(path, false, L)) return 1;
+  const rte_config& c = L.pr.cfg;
+  const size_t N = (size_t)c.nx * c.ny * c.nz, np = (size_t)c.nx * c.ny;
+  FILE* gf = L.pr.g_file[0] ? fopen(L.pr.g_file, "rb") : nullptr;
+  if (!gf) {
+    printf("Error in opening gfile. Exiting \n");
+    return 0;
+  }
+  fclose(gf);
+  if (L.pr.ntypes < 3) {
+    fprintf(stderr, "rte_snr needs NoTiss >= 2 (the lesion is tissue 2)\n");
+    return 1;
+  }
+  const int max_ind = 10;
+  double mua_tab[max_ind], mus_tab[max_ind];
+  for (int q = 0; q < max_ind; q++) {
+    mus_tab[q] = q * 0.25 + 0.25;
+    mua_tab[q] = q * 0.0025 + 0.0025;
+  }
+  auto dump = [](const char* name, const double* v, size_t n) {
+    FILE* f = fopen(name, "wb");
+    if (f) {
+      if (n) fwrite(v, sizeof(double), n, f);
+      fclose(f);
+    }
+  };
+  dump("abs_co_fim.dat", mua_tab, max_ind);
+  dump("sc_co_fim.dat", mus_tab, max_ind);
+  for (const char* nm : {"grada_terms_fim.dat", "grads_terms_fim.dat", "res_terms_fim.dat", "fim_terms.dat"})
+    dump(nm, nullptr, 0);
+  const double fov = c.x_max - c.x_min;
+  auto X = [&](int i) { return i * fov / c.nx - fov / 2 + fov / (2 * c.nx); };
+  auto Y = [&](int i) { return i * fov / c.ny - fov / 2 + fov / (2 * c.ny); };
+  auto Z = [&](int i) { return i * fov / c.nz + fov / (2 * c.nz); };
+  const float rad = (float)(3 * fov / (2 * c.nx));
+  const float rad2 = rad * rad;
+  const int initz = 2, lx = c.nx / 2, ly = c.ny / 2;
+  std::vector<double> snr(c.nz > initz ? c.nz - initz : 0, 0.0);
+  std::vector<uint8_t> tiss(N);
+  std::vector<double> ta(L.pr.mua, L.pr.mua + L.pr.ntypes), ts(L.pr.mus, L.pr.mus + L.pr.ntypes);
+  std::vector<rte_cplx> tr(np), g1(np), g0(np);
+  for (int lz = initz; lz < 16 && lz < c.nz; lz++) {
+    for (int i = 0; i < c.nz; i++)
+      for (int j = 0; j < c.ny; j++)
+        for (int k = 0; k < c.nx; k++) {
+          const double d2 = (X(k) - X(lx)) * (X(k) - X(lx)) + (Y(j) - Y(ly)) * (Y(j) - Y(ly)) + (Z(i) - Z(lz)) * (Z(i) - Z(lz));
+          tiss[((size_t)i * c.ny + j) * c.nx + k] = d2 < (double)rad2 ? 2 : 1;
+        }
+    for (int hyp = 1; hyp >= 0; hyp--) {
+      ta[2] = 0.25 + 0.1 * hyp;
+      ts[2] = 1.0;
+      int rc = rte_set_medium_tissue(L.ctx, tiss.data(), L.pr.ntypes, ta.data(), ts.data());
+      if (!rc) rc = rte_forward(L.ctx, &L.pr.src, &L.pr.stop, nullptr, tr.data(), hyp ? g1.data() : g0.data(), nullptr);
+      if (rc) return die(L.ctx, "rte_forward", rc);
+    }
+    for (size_t q = 0; q < np; q++) snr[lz - initz] += (g1[q].re - g0[q].re) * (g1[q].re - g0[q].re) / g0[q].re;
+    printf("%e is the SNR^2 for the lesion at z index %d \n", snr[lz - initz], lz);
+  }
+  dump("snr_terms.dat", snr.data(), snr.size());
+  return 0;
+}
+
 int main_fisher(const char* path) {
   Loaded L;
   if (load(path, false, L, 0)) return 1;  // LoadPhantom(ini, 0): no tissue map (rte_fim.cu:104)
@@ -239,5 +311,6 @@ int main(int argc, char** argv) {
   }
   if (name == "rte_inv" || name == "rte_test") return main_inverse(argv[1]);
   if (name == "rte_fim") return main_fisher(argv[1]);
+  if (name == "rte_snr") return main_snr(argv[1]);
   return main_forward(argv[1]);
 }

@@ -365,6 +365,9 @@ struct rte_ctx {
   std::vector<uintptr_t> graph_sig[5];
   void* d_Qbp = nullptr;        // gradient: weight of every unordered voxel pair (N x round32(N))
   uint8_t* d_mask = nullptr;    // region mask of the reference-compatible tangent solves [N]
+  bool uniform = false;         // the medium has one mu_t: the operator is a convolution
+  double uniform_mut = 0.0;
+  FftState* fft = nullptr;      // its table spectra, buffers and plans
   double* d_dmut = nullptr;     // Fisher: parameter direction of mu_t and mu_s [N], tangent dA S [N][C]
   double* d_dmus = nullptr;
   double* d_T = nullptr;
@@ -447,6 +450,8 @@ static cudaError_t dalloc(rte_ctx* c, T** p, size_t n) {
 }
 
 static void free_all(rte_ctx* c) {
+  rte_fft_destroy(c->fft);
+  c->fft = nullptr;
   for (int k = 0; k < 5; k++)
     if (c->graph[k]) cudaGraphExecDestroy(c->graph[k]);
   for (int k = 0; k < 2; k++)
@@ -672,6 +677,7 @@ static int build_self_lut(rte_ctx* c) {
     if (it == id.end()) {
       if (vals.size() >= 4096) {
         c->self_lut_ok = false;
+        c->uniform = false;
         return RTE_OK;
       }
       it = id.emplace(mut[r], (int)vals.size()).first;
@@ -718,6 +724,8 @@ static int build_self_lut(rte_ctx* c) {
   CUDA_TRY(c, cudaMemcpyAsync(c->d_self_idx, idx.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->self_lut_ok = true;
+  c->uniform = vals.size() == 1;
+  c->uniform_mut = vals[0];
   return RTE_OK;
 }
 
@@ -995,17 +1003,50 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
 // One term on the real basis for nb right-hand sides (layout [N][nb][C]): out = [D] A in.
 // in64 is FP64 (and in32 its FP32 copy for the mixed kernels).  sum != null accumulates the result;
 // d_red receives the norms.
+static const int kMaxBatch = 4;  // right-hand sides of one batched solve
+
+// Uniform media in automatic kernel mode take the convolution path (rte_fft.cpp), outside graph
+// capture (the transforms plan and synchronise); RTE_NO_FFT=1 keeps the pair kernels.
+static bool fft_active(const rte_ctx* c) {
+  static const bool off = getenv("RTE_NO_FFT") && getenv("RTE_NO_FFT")[0] == '1';
+  return c->uniform && c->kernel_mode == RTE_KERNEL_AUTO && !c->capturing && !off;
+}
+
+static int ensure_fft(rte_ctx* c) {
+  FftTabArgs a;
+  memset(&a, 0, sizeof a);
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  a.dx = c->dx;
+  a.dy = c->dy;
+  a.dz = c->dz;
+  a.prop_thresh = c->prop_thresh;
+  a.kscale = c->dV / c->cm;
+  a.mut = c->uniform_mut;
+  const bool first = c->fft == nullptr;
+  CUDA_TRY(c, rte_fft_prepare(&c->fft, a, c->L, c->model == RTE_MODEL_FIM ? 1 : 0, kMaxBatch, c->st));
+  if (first) c->bytes += rte_fft_bytes(c->nx, c->ny, c->nz, c->L, kMaxBatch);
+  return RTE_OK;
+}
+
 static int apply_term(rte_ctx* c, const double* in64, const float* in32, double* out, float* out32, double* sum,
                       int flag, int flag_scat, int nb = 1) {
   const int LA = flag ? c->L : 0;
-  bool stored = false;
-  int rc = ensure_pair_kernel(c, &stored);
-  if (rc) return rc;
   int S = 1, chunk = c->N;
-  rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
-  if (rc) return rc;
-  const PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
-  {
+  int rc;
+  if (fft_active(c)) {
+    rc = ensure_fft(c);
+    if (rc) return rc;
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, (c->launches += 5, rte_fft_apply(c->fft, in64, nb * c->C, c->C, LA, nb, c->d_part, c->st)));
+  } else {
+    bool stored = false;
+    rc = ensure_pair_kernel(c, &stored);
+    if (rc) return rc;
+    rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
+    if (rc) return rc;
+    const PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
   }
@@ -1586,7 +1627,6 @@ extern "C" int rte_get_stats(rte_ctx* c, rte_stats* out) {
 // ---------------------------------------------------------------------------------------
 // Batched forward solves: nsrc sources on one medium propagated together (the pair kernels reuse
 // each pair's direction, SH and kernel value for every source).
-static const int kMaxBatch = 4;
 
 template <class T>
 static int grow(rte_ctx* c, T** p, size_t& cap, size_t n) {

@@ -173,6 +173,27 @@ cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut,
                               int N, double* red_max, cudaStream_t st);
 cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks);
 cudaError_t rte_upload_sh_tables(const ShTables& t);
+// Uniform-medium convolution path (rte_fft.cpp): grid, padded grid, spacing, coupling distance,
+// kernel scale, mu_t, and the pair range [p0, p1) of one sampling launch.
+struct FftTabArgs {
+  int nx, ny, nz, Mx, My, Mz;
+  double dx, dy, dz, prop_thresh, kscale, mut;
+  int p0, p1;
+};
+cudaError_t rte_launch_fft_table(const FftTabArgs& a, int L, int table, double* T, size_t M, cudaStream_t st);
+cudaError_t rte_launch_fft_pad(const double* W, int vstride, int Cfull, int Cact, int nb, const FftTabArgs& a, double* F,
+                               size_t M, cudaStream_t st);
+cudaError_t rte_launch_fft_product(const void* That, const void* Wh, void* Oh, int C, int Cact, int nb, size_t Mk,
+                                   cudaStream_t st);
+cudaError_t rte_launch_fft_crop(const double* F, int Cfull, int Cact, int nb, const FftTabArgs& a, double* part,
+                                size_t M, cudaStream_t st);
+struct FftState;
+cudaError_t rte_fft_prepare(FftState** s, const FftTabArgs& a, int L, int table, int nbmax, cudaStream_t st);
+cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, int LA, int nb, double* part,
+                          cudaStream_t st);
+size_t rte_fft_bytes(int nx, int ny, int nz, int L, int nbmax);
+void rte_fft_destroy(FftState* s);
+
 // host copies: the recurrence tables and the real SH R_c at a unit direction (index l*l + l + m)
 ShTables make_sh_tables();
 void sh_real_host(const ShTables& t, int L, double x, double y, double z, double* R);

@@ -1683,3 +1683,137 @@ cudaError_t rte_launch_grad_local(const GradLocalArgs& a, cudaStream_t st) {
   k_grad_local<<<(a.N + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------------------------
+// Uniform medium: the off-diagonal operator as a convolution over displacements (host side and the
+// transforms in rte_fft.cpp).  k_fft_table samples T_cc'(d) = k(d) R_c(d) R_c'(d) on the padded
+// grid, k_fft_pad / k_fft_crop move fields in and out of it, k_fft_product forms the spectral
+// products.
+// T_cc'(d) for c <= c' (pair p in row-major upper-triangle order) on the padded grid; the padded
+// index g maps to the displacement g (g < n), g - M (g > n) or none (g == n).
+template <int LA, bool TABLE>
+__global__ void k_fft_table(FftTabArgs a, double* T, size_t M) {
+  constexpr int C = (LA + 1) * (LA + 1);
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M) return;
+  const int gx = (int)(t % a.Mx), gy = (int)((t / a.Mx) % a.My), gz = (int)(t / ((size_t)a.Mx * a.My));
+  auto disp = [](int g, int n, int Mg, bool& ok) {
+    if (g < n) return g;
+    if (g > Mg - n) return g - Mg;
+    ok = false;
+    return 0;
+  };
+  bool ok = true;
+  const int ix = disp(gx, a.nx, a.Mx, ok), iy = disp(gy, a.ny, a.My, ok), iz = disp(gz, a.nz, a.Mz, ok);
+  const double ddx = ix * a.dx, ddy = iy * a.dy, ddz = iz * a.dz;
+  const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+  const double dist = sqrt(d2);
+  ok = ok && d2 > 0.0 && dist < a.prop_thresh;
+  double R[C];
+  double k = 0.0;
+  if (ok) {
+    k = exp(-a.mut * dist) * a.kscale / d2;
+    double ux, uy, uz;
+    if (TABLE) {
+      table_direction(ddx, ddy, ddz, dist, ux, uy, uz);
+    } else {
+      ux = ddx / dist;
+      uy = ddy / dist;
+      uz = ddz / dist;
+    }
+    sh_eval<LA, double>(ux, uy, uz, R);
+  }
+  int p = 0;
+#pragma unroll 1
+  for (int c = 0; c < C; ++c)
+#pragma unroll 1
+    for (int cp = c; cp < C; ++cp, ++p)
+      if (p >= a.p0 && p < a.p1) T[(size_t)(p - a.p0) * M + t] = ok ? k * R[c] * R[cp] : 0.0;
+}
+
+// W [N][vstride] (coefficient c of right-hand side b at b*Cfull + c) -> padded fields F[b*Cact + c][M]
+__global__ void k_fft_pad(const double* W, int vstride, int Cfull, int Cact, int nb, FftTabArgs a, double* F,
+                          size_t M) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long N = (long long)a.nx * a.ny * a.nz;
+  if (t >= N * nb * Cact) return;
+  const int c = (int)(t % Cact);
+  const int b = (int)((t / Cact) % nb);
+  const long long r = t / ((long long)Cact * nb);
+  const int x = (int)(r % a.nx), y = (int)((r / a.nx) % a.ny), z = (int)(r / ((long long)a.nx * a.ny));
+  F[(size_t)(b * Cact + c) * M + ((size_t)z * a.My + y) * a.Mx + x] = W[(size_t)r * vstride + (size_t)b * Cfull + c];
+}
+
+// O_c(k) = sum_c' That_cc'(k) W_c'(k) for every frequency k and right-hand side; the table holds
+// c <= c' (row-major upper triangle of the full order)
+__global__ void k_fft_product(const double2* That, const double2* Wh, double2* Oh, int C, int Cact, int nb,
+                              size_t Mk) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Mk) return;
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < Cact; ++c) {
+      double ox = 0.0, oy = 0.0;
+      for (int cp = 0; cp < Cact; ++cp) {
+        const int lo = min(c, cp), hi = max(c, cp);
+        const size_t p = (size_t)lo * C - (size_t)lo * (lo - 1) / 2 + (hi - lo);
+        const double2 t = That[p * Mk + k];
+        const double2 w = Wh[(size_t)(b * Cact + cp) * Mk + k];
+        ox += t.x * w.x - t.y * w.y;
+        oy += t.x * w.y + t.y * w.x;
+      }
+      Oh[(size_t)(b * Cact + c) * Mk + k] = make_double2(ox, oy);
+    }
+}
+
+// padded result fields -> split-K partial layout [N][nb][Cfull] (one split), scaled by 1/M
+__global__ void k_fft_crop(const double* F, int Cfull, int Cact, int nb, FftTabArgs a, double* part, size_t M) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long N = (long long)a.nx * a.ny * a.nz;
+  if (t >= N * nb * Cact) return;
+  const int c = (int)(t % Cact);
+  const int b = (int)((t / Cact) % nb);
+  const long long r = t / ((long long)Cact * nb);
+  const int x = (int)(r % a.nx), y = (int)((r / a.nx) % a.ny), z = (int)(r / ((long long)a.nx * a.ny));
+  part[(size_t)r * nb * Cfull + (size_t)b * Cfull + c] =
+      F[(size_t)(b * Cact + c) * M + ((size_t)z * a.My + y) * a.Mx + x] / (double)M;
+}
+
+
+cudaError_t rte_launch_fft_table(const FftTabArgs& a, int L, int table, double* T, size_t M, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((M + 127) / 128);
+  switch (L) {
+#define RTE_FFT_TAB(LL)                                          \
+  case LL:                                                       \
+    if (table)                                                   \
+      k_fft_table<LL, true><<<blocks, 128, 0, st>>>(a, T, M);    \
+    else                                                         \
+      k_fft_table<LL, false><<<blocks, 128, 0, st>>>(a, T, M);   \
+    break;
+    RTE_FFT_TAB(0) RTE_FFT_TAB(1) RTE_FFT_TAB(2) RTE_FFT_TAB(3) RTE_FFT_TAB(4) RTE_FFT_TAB(5) RTE_FFT_TAB(6)
+    RTE_FFT_TAB(7)
+#undef RTE_FFT_TAB
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_fft_pad(const double* W, int vstride, int Cfull, int Cact, int nb, const FftTabArgs& a, double* F,
+                               size_t M, cudaStream_t st) {
+  const long long n = (long long)a.nx * a.ny * a.nz * nb * Cact;
+  k_fft_pad<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(W, vstride, Cfull, Cact, nb, a, F, M);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_fft_product(const void* That, const void* Wh, void* Oh, int C, int Cact, int nb, size_t Mk,
+                                   cudaStream_t st) {
+  k_fft_product<<<(unsigned)((Mk + 127) / 128), 128, 0, st>>>(
+      (const double2*)That, (const double2*)Wh, (double2*)Oh, C, Cact, nb, Mk);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_fft_crop(const double* F, int Cfull, int Cact, int nb, const FftTabArgs& a, double* part,
+                                size_t M, cudaStream_t st) {
+  const long long n = (long long)a.nx * a.ny * a.nz * nb * Cact;
+  k_fft_crop<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(F, Cfull, Cact, nb, a, part, M);
+  return cudaGetLastError();
+}

@@ -168,3 +168,33 @@ def test_rte_gpu_on_cpu_package_files(rte, tmp_path, case):
         assert rel(_read_img(os.path.join(d, f"SideFace{q}({ax}).out")), g[f"side{q}"]) < 1e-10
     ph = float(re.search(r"Number of photons total: (\S+)", r.stdout).group(1))
     assert abs(ph - float(g["photons"])) < 2e-6
+
+
+def test_rte_snr_matches_oracle(rte, oracle, tmp_path):
+    g = np.load(os.path.join(GOLD, "fim_tissues_10x10x20_L2.npz"))
+    d = str(tmp_path)
+    nx, ny, nz = (int(g[k]) for k in ("nx", "ny", "nz"))
+    with open(os.path.join(d, "g.out"), "wb") as f:  # the program insists on a measured image
+        f.write(struct.pack("2i", ny, nx) + np.zeros(nx * ny).tobytes())
+    par = _par(g, d, extra=f"gFile = {d}/g.out\n")
+    r = subprocess.run([_exe(rte, "rte_snr"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+    snr = np.fromfile(os.path.join(d, "snr_terms.dat"), np.float64)
+    assert snr.size == nz - 2 and np.all(snr[:14] > 0)
+    fov = nx * float(g["delX"])
+    X = np.arange(nx) * fov / nx - fov / 2 + fov / (2 * nx)
+    Y = np.arange(ny) * fov / ny - fov / 2 + fov / (2 * ny)
+    Z = np.arange(nz) * fov / nz + fov / (2 * nz)
+    rad = np.float32(3 * fov / (2 * nx))
+    mua_t, mus_t = np.array(g["mua_t"], float), np.array(g["mus_t"], float)
+    for lz in (2, 5):
+        d2 = (X[None, None, :] - X[nx // 2]) ** 2 + (Y[None, :, None] - Y[ny // 2]) ** 2 + (Z[:, None, None] - Z[lz]) ** 2
+        tiss = np.where(d2 < float(rad * rad), 2, 1).ravel()
+        imgs = []
+        for hyp in (1, 0):
+            a, s = mua_t.copy(), mus_t.copy()
+            a[2], s[2] = 0.25 + 0.1 * hyp, 1.0
+            p, mua, mus, out = _oracle_setup(oracle, g, a, s, tiss)
+            imgs.append(oracle.images(p, mua, mus, out, 1, mag=float(g["mag"]))[1].real.ravel())
+        ref = float(np.sum((imgs[0] - imgs[1]) ** 2 / imgs[1]))
+        assert abs(snr[lz - 2] - ref) <= 1e-5 * abs(ref), (lz, snr[lz - 2], ref)

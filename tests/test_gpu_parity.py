@@ -159,3 +159,31 @@ def test_forward_batch_matches_single(rte, oracle):
         assert rel(rb4["W"][b], ref["out"]) < 1e-5
         assert rel(rb4["trans"][b], ref["trans"]) < 1e-5
     ctx.close()
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-11), (1, 1e-9)])
+def test_uniform_medium_convolution_path(rte, oracle, prec, tol):
+    """A uniform medium in automatic kernel mode runs the operator as an FFT convolution: the same
+    forward solve as the oracle and as the pair kernels (RTE_KERNEL_RECOMPUTE), single and batched."""
+    nx, ny, nz, L = 9, 8, 7, 3
+    N = nx * ny * nz
+    mua, mus = np.full(N, 0.02), np.full(N, 1.3)
+    stop = rte.Stop(rte.STOP_FIXED, 12)
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_EXACT, prec, kernel_mode=rte.KERNEL_AUTO)
+    ctx.set_medium_voxel(mua, mus)
+    srcs = [rte.Source(pos_x=0.05, pos_y=-0.1), rte.Source(pos_x=-0.2, pos_y=0.1)]
+    res = ctx.forward(srcs[0], stop)
+    ref = oracle.forward(p, mua, mus, src_kind=oracle.SRC_COLUMN, img_mode=0, stop_rule=oracle.STOP_FIXED, max_terms=12,
+                         pos_x=0.05, pos_y=-0.1)
+    assert rel(res["W"], ref["out"]) < tol and rel(res["trans"], ref["trans"]) < tol
+    W = real_to_complex(np.random.default_rng(4).standard_normal((N, (L + 1) ** 2)), L)
+    assert rel(ctx.prop_abs(W, 1, 1), oracle.apply(p, mua, mus, W, 1, 1)) < tol
+    assert rel(ctx.prop_abs(W, 0, 1), oracle.apply(p, mua, mus, W, 0, 1)) < tol
+    if prec == 1:
+        rb = ctx.forward_batch(srcs, stop)
+        assert rel(rb["W"][0], res["W"]) < 1e-9
+    ctx.close()
+    pair, _ = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_EXACT, 0, kernel_mode=rte.KERNEL_RECOMPUTE)
+    pair.set_medium_voxel(mua, mus)
+    assert rel(pair.forward(srcs[0], stop)["W"], res["W"]) < max(tol, 1e-12)
+    pair.close()
