@@ -397,6 +397,34 @@ def run_fisher(dev, n=25, Lq=5, nbins=16, terms=TERMS):
             "F_min_eig": float(ev.min())}
 
 
+def run_uniform(dev):
+    """A uniform 33^3, L=5 medium (the background of the phantom): forward solves through the FFT
+    convolution path (automatic kernel mode) against the stored-kernel pair path, FP64 error of each."""
+    import doi_b200 as R
+    N = N_SIDE ** 3
+    mua, mus = np.full(N, 0.01), np.full(N, 1.0)
+    src = R.Source(kind=R.SRC_COLUMN)
+    stop = R.Stop(R.STOP_FIXED, TERMS)
+    out = {"workload": f"{N_SIDE}^3 uniform (mu_a 0.01, mu_s 1, g 0.8), L={L}, centre beam, {TERMS} terms"}
+    res = {}
+    for name, prec, km in (("fft", R.PREC_MIXED, R.KERNEL_AUTO), ("pair_stored", R.PREC_MIXED, R.KERNEL_STORE),
+                           ("fp64_pairs", R.PREC_FP64, R.KERNEL_RECOMPUTE)):
+        ctx = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=prec, kernel_mode=km, device=dev)
+        ctx.set_medium_voxel(mua, mus)
+        ctx.forward(src, stop, want_W=False)  # warm-up: tables, plans, stored kernel
+        t = time.perf_counter()
+        r = ctx.forward(src, stop, want_W=True)
+        res[name] = r
+        out[name + "_ms"] = (time.perf_counter() - t) * 1e3
+        out[name + "_ms_device"] = r["ms_device"]
+        ctx.close()
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    out["fft_rel_err_vs_fp64"] = rel(res["fft"]["W"], res["fp64_pairs"]["W"])
+    out["pair_rel_err_vs_fp64"] = rel(res["pair_stored"]["W"], res["fp64_pairs"]["W"])
+    out["speedup_fft_over_pairs"] = out["pair_stored_ms_device"] / out["fft_ms_device"]
+    return out
+
+
 def hbm_line(traffic, avg_ms):
     """The pair kernel's DRAM bytes per launch (ncu) over its live launch time, against the measured
     HBM copy bandwidth: how far the kernel is from being memory-bound."""
@@ -562,6 +590,7 @@ def run_ours(args):
             line["config1_plain_fp64"] = run_cfg1(dev)
             line["config4_gradient"] = run_grad(dev)
             line["config5_fisher"] = run_fisher(dev, **({"n": 49, "Lq": 7} if args.fisher_full else {}))
+            line["uniform_fft"] = run_uniform(dev)
         if args.serve_requests > 0:
             line["serve"] = run_serve(args, dev)
         out = line
