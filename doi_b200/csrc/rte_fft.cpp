@@ -7,7 +7,8 @@
 // shift-invariant table, CPU package/src/Kernels_selfsub.c:710-1084, and sums it directly).  Here
 // it runs through FP64 FFTs on a grid zero-padded to at least 2n - 1 per axis: the spectra of the
 // C(C+1)/2 distinct T_cc' are built once per medium; each application transforms the C input
-// fields, forms the C x C spectral products (memory-bound on the table spectra) and transforms back.
+// fields, forms the C x C spectral products (memory-bound on the table spectra, which are real or
+// imaginary by the parity of T_cc' and stored as one real number each) and transforms back.
 // cuFFT does the transforms; the sampling, padding, product and cropping kernels are in
 // rte_kernels.cu.
 #include <cuda_runtime.h>
@@ -41,7 +42,7 @@ struct FftState {
   int L = -1, table = 0;
   size_t M = 0, Mk = 0;
   int npair = 0;
-  double2* That = nullptr;  // [npair][Mk]
+  double* tau = nullptr;    // table spectra [npair][Mk]: one real number each, or complex (FIM table)
   double* F = nullptr;      // padded real fields [cap][M]
   double2* Fh = nullptr;    // their spectra [cap][Mk]
   double2* Oh = nullptr;    // product spectra [cap][Mk]
@@ -57,7 +58,7 @@ void rte_fft_destroy(FftState* s) {
     cufftDestroy(kv.second.first);
     cufftDestroy(kv.second.second);
   }
-  cudaFree(s->That);
+  cudaFree(s->tau);
   cudaFree(s->F);
   cudaFree(s->Fh);
   cudaFree(s->Oh);
@@ -68,7 +69,7 @@ size_t rte_fft_bytes(int nx, int ny, int nz, int L, int nbmax) {
   const size_t Mx = fft_size(nx), My = fft_size(ny), Mz = fft_size(nz);
   const size_t M = Mx * My * Mz, Mk = Mz * My * (Mx / 2 + 1);
   const size_t C = (size_t)(L + 1) * (L + 1), npair = C * (C + 1) / 2;
-  return npair * Mk * 16 + (size_t)nbmax * C * (M * 8 + 2 * Mk * 16);
+  return npair * Mk * 16 + (size_t)nbmax * C * (M * 8 + 2 * Mk * 16);  // (a complex table at most)
 }
 
 // Table spectra for a uniform medium of attenuation mut (rebuilt when mut or the order changes).
@@ -85,10 +86,10 @@ cudaError_t rte_fft_prepare(FftState** ps, const FftTabArgs& args, int L, int ta
   const size_t M = (size_t)a.Mx * a.My * a.Mz, Mk = (size_t)a.Mz * a.My * (a.Mx / 2 + 1);
   const int C = (L + 1) * (L + 1), npair = C * (C + 1) / 2;
   cudaError_t e = cudaSuccess;
-  if (!s->That || s->M != M || s->L != L) {
-    cudaFree(s->That);
-    s->That = nullptr;
-    e = cudaMalloc(&s->That, sizeof(double2) * (size_t)npair * Mk);
+  if (!s->tau || s->M != M || s->L != L || s->table != table) {
+    cudaFree(s->tau);
+    s->tau = nullptr;
+    e = cudaMalloc(&s->tau, sizeof(double) * (table ? 2 : 1) * (size_t)npair * Mk);
     if (e != cudaSuccess) return e;
     s->valid = false;
   }
@@ -134,8 +135,9 @@ cudaError_t rte_fft_prepare(FftState** ps, const FftTabArgs& args, int L, int ta
     if (e == cudaSuccess) e = rte_launch_fft_table(b, L, table, s->F, M, st);
     if (e == cudaSuccess) e = cufft_err(cufftExecD2Z(plan, s->F, reinterpret_cast<cufftDoubleComplex*>(s->Fh)));
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s->That + (size_t)p0 * Mk, s->Fh, sizeof(double2) * (size_t)(b.p1 - b.p0) * Mk,
-                          cudaMemcpyDeviceToDevice, st);
+      e = table ? cudaMemcpyAsync(reinterpret_cast<double2*>(s->tau) + (size_t)p0 * Mk, s->Fh,
+                                  sizeof(double2) * (size_t)(b.p1 - b.p0) * Mk, cudaMemcpyDeviceToDevice, st)
+                : rte_launch_fft_extract(s->Fh, s->tau, p0, b.p1 - b.p0, C, Mk, st);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // before the plan goes
   cufftDestroy(plan);
@@ -170,7 +172,7 @@ cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, 
   cudaError_t e = rte_launch_fft_pad(W, vstride, Cfull, Cact, nb, s->a, s->F, s->M, st);
   if (e == cudaSuccess) e = cufft_err(cufftExecD2Z(it->second.first, s->F, reinterpret_cast<cufftDoubleComplex*>(s->Fh)));
   if (e != cudaSuccess) return e;
-  e = rte_launch_fft_product(s->That, s->Fh, s->Oh, (s->L + 1) * (s->L + 1), Cact, nb, s->Mk, st);
+  e = rte_launch_fft_product(s->tau, s->Fh, s->Oh, (s->L + 1) * (s->L + 1), Cact, nb, s->Mk, s->table, st);
   if (e != cudaSuccess) return e;
   // the inverse overwrites the padded buffer; the crop below reads only the grid, and the padding
   // is restored to zero for the next application

@@ -183,8 +183,9 @@ struct FftTabArgs {
 cudaError_t rte_launch_fft_table(const FftTabArgs& a, int L, int table, double* T, size_t M, cudaStream_t st);
 cudaError_t rte_launch_fft_pad(const double* W, int vstride, int Cfull, int Cact, int nb, const FftTabArgs& a, double* F,
                                size_t M, cudaStream_t st);
+cudaError_t rte_launch_fft_extract(const void* spec, double* tau, int p0, int np, int C, size_t Mk, cudaStream_t st);
 cudaError_t rte_launch_fft_product(const void* That, const void* Wh, void* Oh, int C, int Cact, int nb, size_t Mk,
-                                   cudaStream_t st);
+                                   int complex_table, cudaStream_t st);
 cudaError_t rte_launch_fft_crop(const double* F, int Cfull, int Cact, int nb, const FftTabArgs& a, double* part,
                                 size_t M, cudaStream_t st);
 struct FftState;

@@ -1744,10 +1744,90 @@ __global__ void k_fft_pad(const double* W, int vstride, int Cfull, int Cact, int
   F[(size_t)(b * Cact + c) * M + ((size_t)z * a.My + y) * a.Mx + x] = W[(size_t)r * vstride + (size_t)b * Cfull + c];
 }
 
-// O_c(k) = sum_c' That_cc'(k) W_c'(k) for every frequency k and right-hand side; the table holds
-// c <= c' (row-major upper triangle of the full order)
-__global__ void k_fft_product(const double2* That, const double2* Wh, double2* Oh, int C, int Cact, int nb,
+// Spectral products O_c(k) = sum_c' That_cc'(k) W_c'(k).  T_cc'(-d) = (-1)^(l+l') T_cc'(d), so each
+// table spectrum is real (l + l' even) or imaginary (odd): the table holds one real number tau per
+// pair and frequency (That = tau or i tau), c <= c' in row-major upper-triangle order of the full
+// order.  The complex products then split into two real systems over the coefficients,
+//   set 0: inputs (Re W_even, Im W_odd) -> outputs (Re O_even, Im O_odd),
+//   set 1: inputs (Im W_even, Re W_odd) -> outputs (Im O_even, Re O_odd),
+// with sign -1 on the even<-odd terms of set 0 and the odd<-even terms of set 1 (i * i = -1).
+__device__ __forceinline__ double fft_sign(int set, bool c_even, bool cp_even) {
+  if (c_even == cp_even) return 1.0;
+  return (set == 0) == c_even ? -1.0 : 1.0;
+}
+
+template <int LA>
+__global__ void __launch_bounds__(128) k_fft_product_reg(const double* tau, const double2* Wh, double2* Oh, int C,
+                                                         int nb, size_t Mk) {
+  constexpr int CA = (LA + 1) * (LA + 1);
+  __shared__ double sv[CA][128];  // this thread's inputs of the current set (column tid)
+  const int tid = threadIdx.x;
+  const size_t k = (size_t)blockIdx.x * blockDim.x + tid;
+  const bool act = k < Mk;
+  double* Ohd = reinterpret_cast<double*>(Oh);
+  for (int b = 0; b < nb; ++b) {
+#pragma unroll 1
+    for (int set = 0; set < 2; ++set) {
+      double q[CA];
+#pragma unroll
+      for (int c = 0; c < CA; ++c) {
+        const bool ev = !(l_of_c(c) & 1);
+        const double2 w = act ? Wh[(size_t)(b * CA + c) * Mk + k] : make_double2(0.0, 0.0);
+        sv[c][tid] = ((set == 0) == ev) ? w.x : w.y;
+        q[c] = 0.0;
+      }
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < CA; ++c) {
+          const size_t row = (size_t)c * C - (size_t)c * (c - 1) / 2;
+          const double vc = sv[c][tid];
+#pragma unroll
+          for (int cp = c; cp < CA; ++cp) {
+            const double t = __ldg(tau + (row + (cp - c)) * Mk + k);
+            const bool ec = !(l_of_c(c) & 1), ecp = !(l_of_c(cp) & 1);
+            q[c] = fma(fft_sign(set, ec, ecp) * t, sv[cp][tid], q[c]);
+            if (cp != c) q[cp] = fma(fft_sign(set, ecp, ec) * t, vc, q[cp]);
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < CA; ++c) {
+          const bool ev = !(l_of_c(c) & 1);
+          Ohd[2 * ((size_t)(b * CA + c) * Mk + k) + (((set == 0) == ev) ? 0 : 1)] = q[c];
+        }
+      }
+    }
+  }
+}
+
+// any order: coefficients indexed at run time, table entries read once per output coefficient
+__global__ void k_fft_product(const double* tau, const double2* Wh, double2* Oh, int C, int Cact, int nb,
                               size_t Mk) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Mk) return;
+  for (int b = 0; b < nb; ++b)
+    for (int c = 0; c < Cact; ++c) {
+      const bool ec = !(l_of_c(c) & 1);
+      double ox = 0.0, oy = 0.0;
+      for (int cp = 0; cp < Cact; ++cp) {
+        const int lo = min(c, cp), hi = max(c, cp);
+        const double t = tau[((size_t)lo * C - (size_t)lo * (lo - 1) / 2 + (hi - lo)) * Mk + k];
+        const double2 w = Wh[(size_t)(b * Cact + cp) * Mk + k];
+        if (ec == !(l_of_c(cp) & 1)) {  // real spectrum
+          ox = fma(t, w.x, ox);
+          oy = fma(t, w.y, oy);
+        } else {  // i tau
+          ox = fma(-t, w.y, ox);
+          oy = fma(t, w.x, oy);
+        }
+      }
+      Oh[(size_t)(b * Cact + c) * Mk + k] = make_double2(ox, oy);
+    }
+}
+
+// The FIM model snaps directions to its SH table, which breaks the parity of T_cc'; its table keeps
+// complex spectra and this product reads them directly.
+__global__ void k_fft_product_cplx(const double2* That, const double2* Wh, double2* Oh, int C, int Cact, int nb,
+                                   size_t Mk) {
   const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= Mk) return;
   for (int b = 0; b < nb; ++b)
@@ -1755,14 +1835,28 @@ __global__ void k_fft_product(const double2* That, const double2* Wh, double2* O
       double ox = 0.0, oy = 0.0;
       for (int cp = 0; cp < Cact; ++cp) {
         const int lo = min(c, cp), hi = max(c, cp);
-        const size_t p = (size_t)lo * C - (size_t)lo * (lo - 1) / 2 + (hi - lo);
-        const double2 t = That[p * Mk + k];
+        const double2 t = That[((size_t)lo * C - (size_t)lo * (lo - 1) / 2 + (hi - lo)) * Mk + k];
         const double2 w = Wh[(size_t)(b * Cact + cp) * Mk + k];
-        ox += t.x * w.x - t.y * w.y;
-        oy += t.x * w.y + t.y * w.x;
+        ox = fma(t.x, w.x, fma(-t.y, w.y, ox));
+        oy = fma(t.x, w.y, fma(t.y, w.x, oy));
       }
       Oh[(size_t)(b * Cact + c) * Mk + k] = make_double2(ox, oy);
     }
+}
+
+// tau[p][k] = Re or Im of the table spectrum of pair p (by the parity of l + l')
+__global__ void k_fft_extract(const double2* spec, double* tau, int p0, int np, int C, size_t Mk) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)np * Mk) return;
+  const int q = (int)(t / Mk);
+  int p = p0 + q, c = 0;
+  while (p >= C - c) {  // row c of the upper triangle holds C - c pairs
+    p -= C - c;
+    ++c;
+  }
+  const int cp = c + p;
+  const double2 v = spec[t];
+  tau[(size_t)p0 * Mk + t] = ((l_of_c(c) + l_of_c(cp)) & 1) ? v.y : v.x;
 }
 
 // padded result fields -> split-K partial layout [N][nb][Cfull] (one split), scaled by 1/M
@@ -1804,10 +1898,31 @@ cudaError_t rte_launch_fft_pad(const double* W, int vstride, int Cfull, int Cact
   return cudaGetLastError();
 }
 
+cudaError_t rte_launch_fft_extract(const void* spec, double* tau, int p0, int np, int C, size_t Mk, cudaStream_t st) {
+  const size_t n = (size_t)np * Mk;
+  k_fft_extract<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const double2*)spec, tau, p0, np, C, Mk);
+  return cudaGetLastError();
+}
+
 cudaError_t rte_launch_fft_product(const void* That, const void* Wh, void* Oh, int C, int Cact, int nb, size_t Mk,
-                                   cudaStream_t st) {
-  k_fft_product<<<(unsigned)((Mk + 127) / 128), 128, 0, st>>>(
-      (const double2*)That, (const double2*)Wh, (double2*)Oh, C, Cact, nb, Mk);
+                                   int complex_table, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((Mk + 127) / 128);
+  if (complex_table) {
+    k_fft_product_cplx<<<blocks, 128, 0, st>>>((const double2*)That, (const double2*)Wh, (double2*)Oh, C, Cact, nb, Mk);
+    return cudaGetLastError();
+  }
+  const double* T = (const double*)That;
+  const double2* W = (const double2*)Wh;
+  double2* O = (double2*)Oh;
+  switch (Cact) {
+    case 1: k_fft_product_reg<0><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    case 4: k_fft_product_reg<1><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    case 9: k_fft_product_reg<2><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    case 16: k_fft_product_reg<3><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    case 25: k_fft_product_reg<4><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    case 36: k_fft_product_reg<5><<<blocks, 128, 0, st>>>(T, W, O, C, nb, Mk); break;
+    default: k_fft_product<<<blocks, 128, 0, st>>>(T, W, O, C, Cact, nb, Mk);
+  }
   return cudaGetLastError();
 }
 
