@@ -197,21 +197,13 @@ def serve_requests(count, seed):
 
 
 def run_serve(args, dev):
-    """Continuous-batching stream through rte_server_* with Poisson arrivals; latency from submit to
-    completion, throughput = completed requests / (first submit -> last completion)."""
+    """Continuous-batching stream through rte_server_*.  Capacity: every request submitted at once,
+    completed requests / (first submit -> last completion).  Latency: Poisson arrivals at
+    --serve-rate (default 0.7 x the capacity just measured), submit -> completion, p50 / p99."""
     import doi_b200 as R
     reqs = serve_requests(args.serve_requests, seed=17)
-    rng = np.random.default_rng(23)
-    gaps = rng.exponential(1.0 / args.serve_rate, len(reqs))
-    with R.Server(device=dev, workers=args.serve_workers) as srv:
-        # one request of every shape first (context creation, self-term tables, graph capture) so the
-        # stream measures steady-state serving; these are not counted
-        N0 = [(n, Lq) for n in SERVE_GRIDS for Lq in SERVE_ORDERS]
-        warm = [srv.submit(np.full(n ** 3, 0.01), np.full(n ** 3, 1.0), [R.Source(kind=R.SRC_BEAM)], n, dx=DX,
-                           nL=Lq, g=0.8, terms=TERMS) for n, Lq in N0]
-        for t in warm:
-            srv.wait(t, timeout=1800)
-        srv_stats0 = srv.stats()
+
+    def stream(srv, gaps):
         t0 = time.perf_counter()
         tickets, t_next = [], t0
         for (n, Lq, mua, mus, src), gap in zip(reqs, gaps):
@@ -225,15 +217,31 @@ def run_serve(args, dev):
             _, _, info = srv.wait(t, timeout=3600)
             lat.append(info["latency_ms"])
             dev_ms += info["device_ms"]
-        wall = time.perf_counter() - t0
+        return time.perf_counter() - t0, np.array(lat), dev_ms
+
+    with R.Server(device=dev, workers=args.serve_workers) as srv:
+        # one request of every shape first (context creation, self-term tables, graph capture) so the
+        # stream measures steady-state serving; these are not counted
+        N0 = [(n, Lq) for n in SERVE_GRIDS for Lq in SERVE_ORDERS]
+        warm = [srv.submit(np.full(n ** 3, 0.01), np.full(n ** 3, 1.0), [R.Source(kind=R.SRC_BEAM)], n, dx=DX,
+                           nL=Lq, g=0.8, terms=TERMS) for n, Lq in N0]
+        for t in warm:
+            srv.wait(t, timeout=1800)
+        st0 = srv.stats()
+        wall_sat, lat_sat, _ = stream(srv, np.zeros(len(reqs)))
+        capacity = len(reqs) / wall_sat
+        rate = args.serve_rate if args.serve_rate > 0 else 0.7 * capacity
+        gaps = np.random.default_rng(23).exponential(1.0 / rate, len(reqs))
+        wall, lat, dev_ms = stream(srv, gaps)
         st = srv.stats()
-    lat = np.array(lat)
-    return {"requests": len(reqs), "arrival_rate_per_s": args.serve_rate, "workers": args.serve_workers,
-            "solves_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
+    return {"requests": len(reqs), "workers": args.serve_workers,
+            "capacity_solves_per_s": capacity, "saturated_wall_s": wall_sat,
+            "arrival_rate_per_s": rate, "solves_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "wall_s": wall,
-            "device_ms_sum": dev_ms, "terms": TERMS, "precision": "mixed (stored FP32 pair kernel)",
+            "device_ms_sum": dev_ms, "terms": TERMS,
+            "precision": "mixed (stored FP32 pair kernel; FFT convolution for uniform media)",
             "contexts": st["contexts"], "hbm_reserved_gb": st["hbm_reserved"] / 1e9,
-            "failed": st["failed"] - srv_stats0["failed"],
+            "failed": st["failed"] - st0["failed"],
             "mix": "grid {17,25,33,41}^3, L {3,5,7}, 0-3 inclusions, beam or isotropic point on a random "
                    "face; warm-up: one uncounted request of every (grid, order) shape"}
 
@@ -620,8 +628,8 @@ def main():
     ap.add_argument("--fisher-full", action="store_true", help="Fisher at the full 49^3, L=7 size (long)")
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
-    ap.add_argument("--serve-rate", type=float, default=1.5,
-                    help="Poisson arrival rate (requests/s); about 0.9x the measured capacity of the mix")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="Poisson arrival rate (requests/s); 0 = 0.7 x the capacity measured first")
     ap.add_argument("--serve-workers", type=int, default=4, help="requests in flight at most")
     args = ap.parse_args()
     global N_SIDE

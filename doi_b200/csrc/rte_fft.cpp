@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <math.h>
+#include <stdint.h>
 #include <string.h>
 
 #include <map>
@@ -147,14 +148,7 @@ cudaError_t rte_fft_prepare(FftState** ps, const FftTabArgs& args, int L, int ta
   return e;
 }
 
-// out (split-K partial layout, one split) = off-diagonal operator applied to W [N][vstride], nb
-// right-hand sides, coefficients below Cact.
-cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, int LA, int nb, double* part,
-                          cudaStream_t st) {
-  if (!s || !s->valid) return cudaErrorInvalidValue;
-  const int Cact = (LA + 1) * (LA + 1);
-  const int nf = nb * Cact;
-  if (nf > s->cap) return cudaErrorInvalidValue;
+static cudaError_t plans_for(FftState* s, int nf, std::pair<cufftHandle, cufftHandle>** out) {
   auto it = s->plans.find(nf);
   if (it == s->plans.end()) {
     int dims[3] = {s->a.Mz, s->a.My, s->a.Mx};
@@ -167,16 +161,44 @@ cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, 
     }
     it = s->plans.emplace(nf, std::make_pair(f, i)).first;
   }
-  cufftSetStream(it->second.first, st);
-  cufftSetStream(it->second.second, st);
+  *out = &it->second;
+  return cudaSuccess;
+}
+
+// Plans for nf transformed fields made ahead of a stream capture (planning allocates).
+cudaError_t rte_fft_warm(FftState* s, int nf) {
+  if (!s || !s->valid || nf > s->cap) return cudaErrorInvalidValue;
+  std::pair<cufftHandle, cufftHandle>* pl;
+  return plans_for(s, nf, &pl);
+}
+
+// Every device address the transforms and kernels of an application use (a recorded graph holds them).
+uintptr_t rte_fft_signature(const FftState* s) {
+  if (!s) return 0;
+  return (uintptr_t)s->tau ^ ((uintptr_t)s->F << 1) ^ ((uintptr_t)s->Fh << 2) ^ ((uintptr_t)s->Oh << 3) ^ s->M;
+}
+
+// out (split-K partial layout, one split) = off-diagonal operator applied to W [N][vstride], nb
+// right-hand sides, coefficients below Cact.
+cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, int LA, int nb, double* part,
+                          cudaStream_t st) {
+  if (!s || !s->valid) return cudaErrorInvalidValue;
+  const int Cact = (LA + 1) * (LA + 1);
+  const int nf = nb * Cact;
+  if (nf > s->cap) return cudaErrorInvalidValue;
+  std::pair<cufftHandle, cufftHandle>* pl = nullptr;
+  cudaError_t e0 = plans_for(s, nf, &pl);
+  if (e0 != cudaSuccess) return e0;
+  cufftSetStream(pl->first, st);
+  cufftSetStream(pl->second, st);
   cudaError_t e = rte_launch_fft_pad(W, vstride, Cfull, Cact, nb, s->a, s->F, s->M, st);
-  if (e == cudaSuccess) e = cufft_err(cufftExecD2Z(it->second.first, s->F, reinterpret_cast<cufftDoubleComplex*>(s->Fh)));
+  if (e == cudaSuccess) e = cufft_err(cufftExecD2Z(pl->first, s->F, reinterpret_cast<cufftDoubleComplex*>(s->Fh)));
   if (e != cudaSuccess) return e;
   e = rte_launch_fft_product(s->tau, s->Fh, s->Oh, (s->L + 1) * (s->L + 1), Cact, nb, s->Mk, s->table, st);
   if (e != cudaSuccess) return e;
   // the inverse overwrites the padded buffer; the crop below reads only the grid, and the padding
   // is restored to zero for the next application
-  e = cufft_err(cufftExecZ2D(it->second.second, reinterpret_cast<cufftDoubleComplex*>(s->Oh), s->F));
+  e = cufft_err(cufftExecZ2D(pl->second, reinterpret_cast<cufftDoubleComplex*>(s->Oh), s->F));
   if (e != cudaSuccess) return e;
   e = rte_launch_fft_crop(s->F, Cfull, Cact, nb, s->a, part, s->M, st);
   if (e != cudaSuccess) return e;

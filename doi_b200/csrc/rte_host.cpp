@@ -368,6 +368,9 @@ struct rte_ctx {
   bool uniform = false;         // the medium has one mu_t: the operator is a convolution
   double uniform_mut = 0.0;
   FftState* fft = nullptr;      // its table spectra, buffers and plans
+  bool fft_capture_ready = false;  // a graph recording may capture the transforms
+  bool fft_graph_failed = false;   // recording the transforms failed once: graphs use the pair kernels
+  bool fft_in_graph[5] = {false, false, false, false, false};
   double* d_dmut = nullptr;     // Fisher: parameter direction of mu_t and mu_s [N], tangent dA S [N][C]
   double* d_dmus = nullptr;
   double* d_T = nullptr;
@@ -1007,10 +1010,13 @@ static const int kMaxBatch = 4;  // right-hand sides of one batched solve
 
 // Uniform media in automatic kernel mode take the convolution path (rte_fft.cpp), outside graph
 // capture (the transforms plan and synchronise); RTE_NO_FFT=1 keeps the pair kernels.
-static bool fft_active(const rte_ctx* c) {
+static bool fft_eligible(const rte_ctx* c) {
   static const bool off = getenv("RTE_NO_FFT") && getenv("RTE_NO_FFT")[0] == '1';
-  return c->uniform && c->kernel_mode == RTE_KERNEL_AUTO && !c->capturing && !off;
+  return c->uniform && c->kernel_mode == RTE_KERNEL_AUTO && !off;
 }
+
+// inside a graph capture only when the recording prepared the transforms beforehand
+static bool fft_active(const rte_ctx* c) { return fft_eligible(c) && (!c->capturing || c->fft_capture_ready); }
 
 static int ensure_fft(rte_ctx* c) {
   FftTabArgs a;
@@ -2178,7 +2184,8 @@ static std::vector<uintptr_t> graph_signature(const rte_ctx* c, int nb) {
           u(nb == 1 ? c->d_aux2 : c->d_bres), u(nb == 1 ? (const void*)c->d_Wf : (const void*)c->d_bWf),
           u(c->d_part), u(c->d_selfp), u(c->d_self_idx), u(c->d_self_lut), u(c->d_mom), (uintptr_t)c->K,
           (uintptr_t)c->self_lut_ok, u(c->d_K), (uintptr_t)c->Kld, u(c->d_mut), u(c->d_mutf), u(c->d_mus),
-          u(c->d_red), u(c->d_err), (uintptr_t)c->bcap};
+          u(c->d_red), u(c->d_err), (uintptr_t)c->bcap, (uintptr_t)(fft_eligible(c) && !c->fft_graph_failed),
+          rte_fft_signature(c->fft)};
 }
 
 static bool graph_stale(const rte_ctx* c, int nb, int nterms) {
@@ -2202,14 +2209,24 @@ static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
       c->graph[gi] = nullptr;
     }
     // everything that may allocate or synchronise happens before the capture
+    const bool use_fft = fft_eligible(c) && !c->fft_graph_failed;
     bool stored = false;
-    int rc = ensure_pair_kernel(c, &stored);
+    int rc = RTE_OK;
+    if (use_fft) {  // uniform medium: table spectra and transform plans now, the transforms in the graph
+      rc = ensure_fft(c);
+      if (!rc) CUDA_TRY(c, rte_fft_warm(c->fft, nb * c->C));
+      if (!rc && flag_l == 0) CUDA_TRY(c, rte_fft_warm(c->fft, nb));
+    } else {
+      rc = ensure_pair_kernel(c, &stored);
+      if (rc) return rc;
+      int S, chunk;
+      rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
+      if (!rc) rc = plan_split(c, c->L, stored ? 1 : 0, nb, &S, &chunk);
+      if (!rc && flag_l == 0) rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
+    }
     if (rc) return rc;
-    int S, chunk;
-    rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
-    if (!rc) rc = plan_split(c, c->L, stored ? 1 : 0, nb, &S, &chunk);
-    if (!rc && flag_l == 0) rc = plan_split(c, 0, stored ? 1 : 0, nb, &S, &chunk);
-    if (rc) return rc;
+    c->fft_in_graph[gi] = use_fft;
+    c->fft_capture_ready = use_fft;
     c->graph_w0[gi] = W;
     c->graph_s0[gi] = sum;
     const bool prof = c->profiling;
@@ -2234,7 +2251,15 @@ static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
     }
     cudaError_t e2 = cudaStreamEndCapture(c->st, &g);
     c->capturing = false;
+    c->fft_capture_ready = false;
     c->profiling = prof;
+    if ((rc || e != cudaSuccess || e2 != cudaSuccess) && use_fft) {
+      // the transforms could not be recorded: record the pair kernels instead from now on
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      c->fft_graph_failed = true;
+      return run_series_graph(c, nb, nterms, d_res);
+    }
     if (rc) {
       if (g) cudaGraphDestroy(g);
       return rc;
@@ -2246,11 +2271,14 @@ static int run_series_graph(rte_ctx* c, int nb, int nterms, double** d_res) {
     if (e3 != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "graph instantiate: %s", cudaGetErrorString(e3));
     c->graph_terms[gi] = nterms;
     c->graph_sig[gi] = graph_signature(c, nb);
+  } else if (c->fft_in_graph[gi]) {
+    int rc = ensure_fft(c);  // the table spectra of the current medium, outside the graph
+    if (rc) return rc;
   }
   (void)NC;
   c->launches += 4 * nterms + 4;
   CUDA_TRY(c, cudaGraphLaunch(c->graph[gi], c->st));
-  c->K_valid = true;
+  if (!c->fft_in_graph[gi]) c->K_valid = true;  // the graph recomputed the stored kernel
   *d_res = res;
   return RTE_OK;
 }

@@ -193,6 +193,8 @@ cudaError_t rte_fft_prepare(FftState** s, const FftTabArgs& a, int L, int table,
 cudaError_t rte_fft_apply(FftState* s, const double* W, int vstride, int Cfull, int LA, int nb, double* part,
                           cudaStream_t st);
 size_t rte_fft_bytes(int nx, int ny, int nz, int L, int nbmax);
+cudaError_t rte_fft_warm(FftState* s, int nf);
+uintptr_t rte_fft_signature(const FftState* s);
 void rte_fft_destroy(FftState* s);
 
 // host copies: the recurrence tables and the real SH R_c at a unit direction (index l*l + l + m)

@@ -134,7 +134,7 @@ static rte_ctx* make_ctx(const rte_server* s, const ShapeKey& key, int* rc) {
   cfg.c = 1.0;
   cfg.model = RTE_MODEL_EXACT;
   cfg.precision = key.prec;
-  cfg.kernel_mode = key.prec == RTE_PREC_MIXED ? RTE_KERNEL_STORE : RTE_KERNEL_RECOMPUTE;
+  cfg.kernel_mode = RTE_KERNEL_AUTO;  // stored pair kernel when it fits; uniform media by FFT
   cfg.device = s->device;
   rte_ctx* ctx = nullptr;
   *rc = rte_create(&cfg, &ctx);

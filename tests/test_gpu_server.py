@@ -25,7 +25,7 @@ def _request(rte, rng, n, L, nsrc):
 
 def _alone(rte, n, L, prec, mua, mus, srcs, terms):
     ctx = rte.Context(n, n, n, dx=DX, nL=L, g=0.8, precision=prec, prop_thresh=4.0 * n * DX,
-                      kernel_mode=rte.KERNEL_STORE if prec else rte.KERNEL_RECOMPUTE)
+                      kernel_mode=rte.KERNEL_AUTO)
     ctx.set_medium_voxel(mua, mus)
     tr, rf, _ = ctx.forward_graph(srcs, terms)
     ctx.close()

@@ -160,3 +160,20 @@ def test_graph_rerecords_when_buffers_move(rte):
         for b in range(nsrc):
             assert rel(tr[b], ref["trans"][b]) < 1e-9 and rel(rf[b], ref["ref"][b]) < 1e-9, (nsrc, b)
     ctx.close()
+
+
+def test_graph_records_the_fft_path_for_uniform_media(rte):
+    """Graph replay on uniform media (the FFT path recorded in the graph) equals the eager solve, and
+    switching to a non-uniform medium and back re-records the graph."""
+    n, L, T = 11, 3, 6
+    N = n ** 3
+    ctx = rte.Context(n, n, n, dx=DX, nL=L, g=0.8, precision=1, kernel_mode=rte.KERNEL_AUTO)
+    srcs = [_face_source(rte, n, 0, 5, 5, rte.SRC_BEAM), _face_source(rte, n, 3, 4, 6, rte.SRC_POINT)]
+    sph = rte.sphere_phantom(n, nspheres=2, seed=9, rmin=0.15, rmax=0.3)[:2]
+    for mua, mus in ((np.full(N, 0.01), np.full(N, 1.0)), sph, (np.full(N, 0.03), np.full(N, 1.4))):
+        ctx.set_medium_voxel(mua, mus)
+        tr, rf, _ = ctx.forward_graph(srcs, T)
+        ref = ctx.forward_batch(srcs, rte.Stop(rte.STOP_FIXED, T), want_W=False)
+        for b in range(2):
+            assert rel(tr[b], ref["trans"][b]) < 1e-9 and rel(rf[b], ref["ref"][b]) < 1e-9, b
+    ctx.close()
