@@ -21,6 +21,7 @@
 
 #include <stdint.h>
 
+#include <algorithm>
 #include <complex>
 #include <string>
 #include <vector>
@@ -99,6 +100,143 @@ std::vector<double> phase_image(const Loaded& L, const std::vector<rte_cplx>& W)
   return ph;
 }
 
+typedef std::complex<double> cd;
+
+// Source columns of the CPU package's beam (GenerateSourceBeam, Dist.c:1087-1093: voxel centres in
+// the circle |xy - pos| <= diam/2; the library adds 1e-16 to diam/2 against rounding at the rim).
+int cpu_columns(const rte_config& c, const rte_source& s) {
+  const double dx = (c.x_max - c.x_min) / c.nx, dy = (c.y_max - c.y_min) / c.ny;
+  int n = 0;
+  for (int j = 0; j < c.ny; j++)
+    for (int k = 0; k < c.nx; k++) {
+      const double xs = k * dx + c.x_min + dx / 2.0, ys = j * dy + c.y_min + dy / 2.0;
+      if (sqrt((xs - s.pos_x) * (xs - s.pos_x) + (ys - s.pos_y) * (ys - s.pos_y)) <= (s.diam + 1.0e-16) / 2.0) n++;
+    }
+  return n;
+}
+
+// StopIteration of the CPU package (Kernels_selfsub.c:1184-1220): real parts of all coefficients on
+// the layer z = nZ-1.
+bool cpu_stop(const rte_config& c, double& fi, int n, const std::vector<rte_cplx>& W, const std::vector<rte_cplx>& out) {
+  const size_t C = (size_t)(c.nL + 1) * (c.nL + 1), plane = (size_t)c.nx * c.ny;
+  double sw = 0.0, so = 0.0;
+  for (size_t q = (size_t)(c.nz - 1) * plane * C; q < (size_t)c.nz * plane * C; q++) {
+    sw += W[q].re;
+    so += out[q].re;
+  }
+  double hi = 0.0;
+  if (n > 1) {
+    if (so == 0.0) return true;
+    hi = 1.0 - (sw / so) * (1.0 / (1.0 - (sw / so) / fi));
+    fi = sw / so;
+    if (hi > 1.0 || hi < 0.0) hi = 0.0;
+  }
+  return hi > 0.9999;
+}
+
+// ComputePhaseImage (CPU package/src/Dist.c:71-131): the diffuse transmission with the weight
+// 1/(100-1) per abscissa (the transmission image uses 1/100) plus the ballistic beam with the package's
+// current mu_t and magnitude, then arg() in degrees.
+std::vector<double> cpu_phase_image(rte_ctx* ctx, const rte_config& c, const std::vector<rte_cplx>& W,
+                                    const rte_source& s, double mag, cd mut) {
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  std::vector<rte_cplx> tr((size_t)nx * ny);
+  std::vector<double> ph((size_t)nx * ny, 0.0);
+  if (rte_images(ctx, W.data(), nullptr, tr.data(), nullptr)) return ph;
+  const double dx = (c.x_max - c.x_min) / nx, dy = (c.y_max - c.y_min) / ny, dz = (c.z_max - c.z_min) / nz;
+  const double zs = (nz - 1) * dz + c.z_min + dz / 2.0;
+  for (int j = 0; j < ny; j++)
+    for (int k = 0; k < nx; k++) {
+      cd v = cd(tr[(size_t)j * nx + k].re, tr[(size_t)j * nx + k].im) * (100.0 / 99.0);
+      const double xs = k * dx + c.x_min + dx / 2.0, ys = j * dy + c.y_min + dy / 2.0;
+      if (sqrt((xs - s.pos_x) * (xs - s.pos_x) + (ys - s.pos_y) * (ys - s.pos_y)) <= s.diam / 2.0)
+        v += mag * std::exp(-mut * (zs + dz / 2.0));
+      ph[(size_t)j * nx + k] = std::arg(v) * 180.0 / M_PI;
+    }
+  return ph;
+}
+
+int write_cpu_faces(const Loaded& L, const std::vector<rte_cplx>& W, const rte_source& s, cd mut) {
+  const rte_config& c = L.pr.cfg;
+  const size_t np = (size_t)c.nx * c.ny;
+  std::vector<rte_cplx> sx0((size_t)c.nz * c.ny), sx1(sx0.size()), sy0((size_t)c.nz * c.nx), sy1(sy0.size());
+  rte_cplx ph{0, 0};
+  int rc = rte_cpu_face_outputs(&c, W.data(), &s, mut.real(), mut.imag(), sx0.data(), sx1.data(), sy0.data(),
+                                sy1.data(), &ph);
+  if (rc) return die(L.ctx, "rte_cpu_face_outputs", rc);
+  const char* names[4] = {"SideFace1(-X).out", "SideFace2(+X).out", "SideFace3(-Y).out", "SideFace4(+Y).out"};
+  std::vector<rte_cplx>* imgs[4] = {&sx0, &sx1, &sy0, &sy1};
+  for (int q = 0; q < 4; q++) {
+    // the package writes these buffers through its z-face writer (nX x nY values read in order)
+    std::vector<rte_cplx> buf(np, rte_cplx{0, 0});
+    for (size_t e = 0; e < np && e < imgs[q]->size(); e++) buf[e] = (*imgs[q])[e];
+    if ((rc = rte_write_image(names[q], c.nx, c.ny, buf.data(), 1))) return die(L.ctx, names[q], rc);
+  }
+  printf("Number of photons total: %f\n", ph.re);
+  return 0;
+}
+
+// The CPU package's main (RTE_uniform.c:64-196) on a uniform-medium file.  Steady state: source,
+// Neumann series with the package's stop rule, final A.  With [Source] modulation != 0 the package
+// continues as written: the source is built again with the real mu_a (GenerateSourceBeam divides the
+// magnitude by the column count once more, Dist.c:1113-1114), mu_a gains i modulation/(c/n), the
+// modulated terms (D A)^n src are added to the steady-state result itself under its stop rule, the
+// modulated output is A src alone, its phase image is written, and the images come from
+// CombineOuts = 0.5 out + 0.25 out2 + 0.25 conj(out2) (Dist.c:1294-1303).  Reproduced step by step.
+int forward_cpu_package(Loaded& L, std::vector<rte_cplx>& W, std::vector<rte_cplx>& tr, std::vector<rte_cplx>& rf,
+                        rte_report& rep) {
+  const rte_config& c = L.pr.cfg;
+  const size_t N = (size_t)c.nx * c.ny * c.nz, C = (size_t)(c.nL + 1) * (c.nL + 1);
+  const double modulation = L.pr.src.modulation;
+  rte_source s = L.pr.src;
+  s.modulation = 0.0;
+  int rc = rte_forward(L.ctx, &s, &L.pr.stop, W.data(), tr.data(), rf.data(), &rep);
+  if (rc) return die(L.ctx, "rte_forward", rc);
+  printf("Neumann series: %d terms, %.3f ms on the device\n", rep.terms, rep.ms_device);
+  const int cols = std::max(1, cpu_columns(c, s));
+  const double mut = L.pr.mua[1] + L.pr.mus[1];
+  s.mag = L.pr.src.mag / cols;  // source->mag after GenerateSourceBeam
+  std::vector<rte_cplx> out2 = W;
+  cd mutc(mut, 0.0);
+  if (modulation != 0.0) {
+    std::vector<rte_cplx> xi(N * C), Wn(N * C);
+    if ((rc = rte_source_beam(L.ctx, &s, xi.data()))) return die(L.ctx, "rte_source_beam", rc);
+    if ((rc = rte_set_modulation(L.ctx, modulation))) return die(L.ctx, "rte_set_modulation", rc);
+    s.mag /= cols;  // the second GenerateSourceBeam
+    s.modulation = modulation;
+    mutc = cd(mut, modulation / (c.c / c.n));
+    std::vector<rte_cplx> Wk = xi;
+    const int flag = c.g != 0.0 ? 1 : 0;
+    double fi = 1.0;
+    int n = 1;
+    while (!cpu_stop(c, fi, n, Wk, W) && n <= 10000) {
+      if ((rc = rte_prop_abs(L.ctx, Wk.data(), Wn.data(), flag, 1))) return die(L.ctx, "rte_prop_abs", rc);
+      Wk.swap(Wn);
+      for (size_t q = 0; q < N * C; q++) {
+        W[q].re += Wk[q].re;
+        W[q].im += Wk[q].im;
+      }
+      n++;
+    }
+    printf("Neumann series (modulated): %d terms\n", n - 1);
+    if ((rc = rte_prop_abs(L.ctx, xi.data(), out2.data(), 1, 0))) return die(L.ctx, "rte_prop_abs", rc);
+  }
+  if (L.pr.phase_file[0]) {
+    const std::vector<double> ph = cpu_phase_image(L.ctx, c, out2, s, s.mag, mutc);
+    if ((rc = rte_write_phase_image(L.pr.phase_file, c.nx, c.ny, ph.data(), 1))) return die(L.ctx, L.pr.phase_file, rc);
+  }
+  if (modulation != 0.0) {
+    for (size_t q = 0; q < N * C; q++) {  // CombineOuts: out2 = 0.5 out + 0.5 Re(out2) per coefficient
+      W[q].re = 0.5 * W[q].re + 0.5 * out2[q].re;
+      W[q].im = 0.5 * W[q].im;
+    }
+    rte_source si = s;
+    si.mag = s.mag * cols;  // the library divides by the column count itself
+    if ((rc = rte_images(L.ctx, W.data(), &si, tr.data(), rf.data()))) return die(L.ctx, "rte_images", rc);
+  }
+  return write_cpu_faces(L, W, s, mutc);
+}
+
 int main_forward(const char* path) {
   Loaded L;
   if (load(path, true, L)) return 1;
@@ -106,33 +244,30 @@ int main_forward(const char* path) {
   const size_t N = (size_t)c.nx * c.ny * c.nz, C = (size_t)(c.nL + 1) * (c.nL + 1), np = (size_t)c.nx * c.ny;
   std::vector<rte_cplx> W(N * C), tr(np), rf(np);
   rte_report rep;
-  int rc = rte_forward(L.ctx, &L.pr.src, &L.pr.stop, W.data(), tr.data(), rf.data(), &rep);
-  if (rc) return die(L.ctx, "rte_forward", rc);
-  printf("Neumann series: %d terms, %.3f ms on the device\n", rep.terms, rep.ms_device);
+  int rc;
   const int cpu_layout = L.pr.style == 1;
+  if (L.pr.style == 1) {
+    if ((rc = forward_cpu_package(L, W, tr, rf, rep))) return rc;
+  } else {
+    // FisherInfo_IO reads [Source] modulation and does not use it; the exact model solves with it
+    if (c.model == RTE_MODEL_FIM) L.pr.src.modulation = 0.0;
+    rc = rte_forward(L.ctx, &L.pr.src, &L.pr.stop, W.data(), tr.data(), rf.data(), &rep);
+    if (rc) return die(L.ctx, "rte_forward", rc);
+    printf("Neumann series: %d terms, %.3f ms on the device\n", rep.terms, rep.ms_device);
+  }
   if (L.pr.trans_file[0] && (rc = rte_write_image(L.pr.trans_file, c.nx, c.ny, tr.data(), cpu_layout)))
     return die(L.ctx, L.pr.trans_file, rc);
   if (L.pr.ref_file[0] && (rc = rte_write_image(L.pr.ref_file, c.nx, c.ny, rf.data(), cpu_layout)))
     return die(L.ctx, L.pr.ref_file, rc);
-  if (L.pr.style == 1) {  // the CPU package's side-face images and photon number (RTE_uniform.c:184-185)
-    std::vector<rte_cplx> sx0((size_t)c.nz * c.ny), sx1(sx0.size()), sy0((size_t)c.nz * c.nx), sy1(sy0.size());
-    rte_cplx ph{0, 0};
-    rc = rte_cpu_face_outputs(&c, W.data(), &L.pr.src, L.pr.mua[1] + L.pr.mus[1], sx0.data(), sx1.data(), sy0.data(),
-                              sy1.data(), &ph);
-    if (rc) return die(L.ctx, "rte_cpu_face_outputs", rc);
-    const char* names[4] = {"SideFace1(-X).out", "SideFace2(+X).out", "SideFace3(-Y).out", "SideFace4(+Y).out"};
-    std::vector<rte_cplx>* imgs[4] = {&sx0, &sx1, &sy0, &sy1};
-    for (int q = 0; q < 4; q++) {
-      // the package writes these buffers through its z-face writer (nX x nY values read in order)
-      std::vector<rte_cplx> buf(np, rte_cplx{0, 0});
-      for (size_t e = 0; e < np && e < imgs[q]->size(); e++) buf[e] = (*imgs[q])[e];
-      if ((rc = rte_write_image(names[q], c.nx, c.ny, buf.data(), 1))) return die(L.ctx, names[q], rc);
-    }
-    printf("Number of photons total: %f\n", ph.re);
-  }
   if (L.pr.phase_file[0] && L.pr.style == 0) {
-    const std::vector<double> ph = phase_image(L, W);
-    if ((rc = rte_write_phase_image(L.pr.phase_file, c.nx, c.ny, ph.data()))) return die(L.ctx, L.pr.phase_file, rc);
+    std::vector<double> ph;
+    if (L.pr.src.modulation != 0.0) {  // the modulated transmission (ballistic included): its phase delay
+      ph.resize(np);
+      for (size_t q = 0; q < np; q++) ph[q] = std::arg(cd(tr[q].re, tr[q].im));
+    } else {
+      ph = phase_image(L, W);
+    }
+    if ((rc = rte_write_phase_image(L.pr.phase_file, c.nx, c.ny, ph.data(), 0))) return die(L.ctx, L.pr.phase_file, rc);
   }
   if (L.pr.flux_file[0] && L.pr.detector_bins > 0) {  // binned exitant flux on all six faces
     rte_stop st = L.pr.stop;

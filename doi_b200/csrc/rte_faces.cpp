@@ -78,8 +78,8 @@ std::vector<cd> rule_weights(const ShTables& t, int L, const Rule& q, double are
 }  // namespace
 
 extern "C" int rte_cpu_face_outputs(const rte_config* cfg, const rte_cplx* W, const rte_source* src, double mu_t,
-                                    rte_cplx* side_x0, rte_cplx* side_x1, rte_cplx* side_y0, rte_cplx* side_y1,
-                                    rte_cplx* photons) {
+                                    double mu_t_im, rte_cplx* side_x0, rte_cplx* side_x1, rte_cplx* side_y0,
+                                    rte_cplx* side_y1, rte_cplx* photons) {
   if (!cfg || !W || cfg->nL < 0 || cfg->nL > RTE_MAX_L || cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1)
     return RTE_ERR_ARG;
   const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz, L = cfg->nL, C = (L + 1) * (L + 1);
@@ -108,7 +108,7 @@ extern "C" int rte_cpu_face_outputs(const rte_config* cfg, const rte_cplx* W, co
             const double xs = i * dx + cfg->x_min + dx / 2.0, ys = j * dy + cfg->y_min + dy / 2.0;
             const double zs = k * dz + cfg->z_min + dz / 2.0;
             const double rad = sqrt((xs - src->pos_x) * (xs - src->pos_x) + (ys - src->pos_y) * (ys - src->pos_y));
-            if (rad <= (src->diam + 1.0e-16) / 2.0) v = src->mag * exp(-mu_t * (zs + dz / 2.0));
+            if (rad <= (src->diam + 1.0e-16) / 2.0) v = src->mag * std::exp(-cd(mu_t, mu_t_im) * (zs + dz / 2.0));
           }
           total += dot(w, at(i, j, k)) + v;
         }

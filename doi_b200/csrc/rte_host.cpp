@@ -376,6 +376,13 @@ struct rte_ctx {
   double* d_T = nullptr;
   int* d_cidx = nullptr;        // source-column voxels and their source derivative
   double* d_cval = nullptr;
+  // intensity modulation (CPU package/src/RTE_uniform.c:120-176): mu_a -> mu_a + i modulation/(c/n),
+  // so mu_t has the uniform imaginary part kappa; radiance is complex, (real, imaginary) row pairs
+  double modulation = 0.0, kappa = 0.0;
+  double mumax = 0.0;             // max real mu_t of the medium
+  double* d_self_lut_im = nullptr;  // imaginary part of the self-term table
+  size_t lut_im_cap = 0;
+  double* d_fball_im = nullptr;   // imaginary part of the single source's ballistic flux
   size_t qbp_bytes = 0;
   size_t bytes = 0;
   double last_setup_ms = 0.0;
@@ -470,7 +477,8 @@ static void free_all(rte_ctx* c) {
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
                 c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq,
-                c->d_Qbp, c->d_mask, c->d_dmut, c->d_dmus, c->d_T, c->d_cidx, c->d_cval};
+                c->d_Qbp, c->d_mask, c->d_dmut, c->d_dmus, c->d_T, c->d_cidx, c->d_cval, c->d_self_lut_im,
+                c->d_fball_im};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -689,7 +697,7 @@ static int build_self_lut(rte_ctx* c) {
     idx[r] = it->second;
   }
   const int C = c->C, K = c->K;
-  std::vector<double> lut(vals.size() * C * C, 0.0), dlut(vals.size() * C * C, 0.0);
+  std::vector<double> lut(vals.size() * C * C, 0.0), dlut(vals.size() * C * C, 0.0), lut_im;
   for (size_t q = 0; q < vals.size(); q++) {
     double* D = &lut[q * C * C];
     double* dD = &dlut[q * C * C];
@@ -697,6 +705,32 @@ static int build_self_lut(rte_ctx* c) {
       for (int e = 0; e < C * C; e++) D[e] = D[e] * vals[q] + c->h_mom[(size_t)k * C * C + e];
     for (int k = K - 1; k >= 1; k--)  // d/dmu
       for (int e = 0; e < C * C; e++) dD[e] = dD[e] * vals[q] + (double)k * c->h_mom[(size_t)k * C * C + e];
+  }
+  if (c->kappa != 0.0) {  // D(mu_t + i kappa): Horner in the complex mu
+    lut_im.assign(vals.size() * C * C, 0.0);
+    for (size_t q = 0; q < vals.size(); q++) {
+      double* Dr = &lut[q * C * C];
+      double* Di = &lut_im[q * C * C];
+      for (int e = 0; e < C * C; e++) Dr[e] = 0.0;
+      for (int k = K - 1; k >= 0; k--)
+        for (int e = 0; e < C * C; e++) {
+          const double nr = Dr[e] * vals[q] - Di[e] * c->kappa + c->h_mom[(size_t)k * C * C + e];
+          Di[e] = Dr[e] * c->kappa + Di[e] * vals[q];
+          Dr[e] = nr;
+        }
+    }
+    if (lut_im.size() > c->lut_im_cap) {
+      if (c->d_self_lut_im) {
+        cudaFree(c->d_self_lut_im);
+        c->bytes -= c->lut_im_cap * sizeof(double);
+        c->d_self_lut_im = nullptr;
+      }
+      const size_t cap = std::max(lut_im.size(), (size_t)16 * C * C);
+      CUDA_TRY(c, dalloc(c, &c->d_self_lut_im, cap));
+      c->lut_im_cap = cap;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_self_lut_im, lut_im.data(), sizeof(double) * lut_im.size(),
+                                cudaMemcpyHostToDevice, c->st));
   }
   {
     int rc = 0;
@@ -741,7 +775,8 @@ static int medium_from_device(rte_ctx* c, const double* d_mua, const double* d_m
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->K_valid = false;
   c->medium_set = true;
-  int rc = ensure_moments(c, mumax);
+  c->mumax = mumax;
+  int rc = ensure_moments(c, std::hypot(mumax, c->kappa));
   if (rc) return rc;
   return build_self_lut(c);
 }
@@ -876,6 +911,7 @@ static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in3
   a.cstride = (c->C + 1) / 2 * 2;
   a.cpad = (nb * a.cstride + 3) / 4 * 4;
   a.err = c->d_err;
+  a.kappa = c->kappa;
   return a;
 }
 
@@ -934,7 +970,8 @@ static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<
 }
 
 static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
-  const int key = ((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0);
+  const int cplx = c->kappa != 0.0 ? 1 : 0;
+  const int key = (((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0)) * 2 + cplx;
   for (auto& e : c->splits)
     if (e[0] == key) {
       *S_out = e[1];
@@ -944,7 +981,7 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
   const int table = c->model == RTE_MODEL_FIM ? 1 : 0;
   int occ = 0;
   const int cpad = (nb * ((c->C + 1) / 2 * 2) + 3) / 4 * 4;
-  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, table, stored, nb, cpad, &occ));
+  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, table, stored, nb, cpad, &occ, cplx));
   int sms = 0;
   CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
   const long long slots = (long long)std::max(occ, 1) * sms;
@@ -971,7 +1008,7 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
   if (forced) {
     bestS = std::max(1, std::min(c->max_split, atoi(forced)));
   } else if (tune) {
-    const TuneKey tk{c->cfg.device, c->N, LA, stored, nb, c->precision, table};
+    const TuneKey tk{c->cfg.device, c->N, LA, stored, nb, c->precision, table + 2 * cplx};
     bool have = false;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1012,7 +1049,7 @@ static const int kMaxBatch = 4;  // right-hand sides of one batched solve
 // capture (the transforms plan and synchronise); RTE_NO_FFT=1 keeps the pair kernels.
 static bool fft_eligible(const rte_ctx* c) {
   static const bool off = getenv("RTE_NO_FFT") && getenv("RTE_NO_FFT")[0] == '1';
-  return c->uniform && c->kernel_mode == RTE_KERNEL_AUTO && !off;
+  return c->uniform && c->kernel_mode == RTE_KERNEL_AUTO && !off && c->kappa == 0.0;
 }
 
 // inside a graph capture only when the recording prepared the transforms beforehand
@@ -1071,6 +1108,9 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   sa.scale = c->dV / c->cm;
   sa.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
   sa.out = c->d_selfp;
+  sa.kappa = c->kappa;
+  sa.lut_im = c->d_self_lut_im;
+  if (c->kappa != 0.0 && nb % 2) return fail(c, RTE_ERR_STATE, "a modulated term needs (real, imaginary) row pairs");
   if (LA < c->L) CUDA_TRY(c, cudaMemsetAsync(c->d_selfp, 0, (size_t)c->N * nb * c->C * sizeof(double), c->st));
   {
     ProfScope ps(c, 2);
@@ -1097,6 +1137,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   e.cpad = (nb * e.cstride + 3) / 4 * 4;
   e.sum = sum;
   e.red = c->d_red;
+  e.cplx = c->kappa != 0.0 ? 1 : 0;
   CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
   {
     ProfScope ps(c, 2);
@@ -1211,10 +1252,139 @@ static int download_cplx(rte_ctx* c, const double* u1, const double* u2, rte_cpl
   return RTE_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// Intensity modulation (CPU package/src/RTE_uniform.c:120-176): mu_a -> mu_a + i modulation/(c/n)
+// in every voxel, so mu_t gains the uniform imaginary part kappa and the radiance is complex.  A
+// complex distribution w = w1 + i w2 (w1, w2 coefficient sets of real functions) lives on the
+// device as (real, imaginary) row pairs per voxel, [N][2][C] in the batch buffers; the pair kernels
+// apply k exp(-i kappa r) to the pair, the self term D(mu_t + i kappa), the scatter acts on both rows.
+static int ensure_batch(rte_ctx* c, int nb);
+
+static int upload_pair(rte_ctx* c, const rte_cplx* h, double* d_pair) {
+  const size_t NC = (size_t)c->N * c->C;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_cplx, h, NC * sizeof(rte_cplx), cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, (c->launches++, rte_launch_to_real(c->d_cplx, d_pair, d_pair + c->C, c->N, c->L, nullptr, c->st,
+                                                 2 * c->C)));
+  return RTE_OK;
+}
+
+static int download_pair(rte_ctx* c, const double* d_pair, rte_cplx* h) {
+  const size_t NC = (size_t)c->N * c->C;
+  CUDA_TRY(c, (c->launches++, rte_launch_to_cplx(d_pair, d_pair + c->C, c->d_cplx, c->N, c->L, c->st, 2 * c->C)));
+  CUDA_TRY(c, cudaMemcpyAsync(h, c->d_cplx, NC * sizeof(rte_cplx), cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  return RTE_OK;
+}
+
+// Neumann series of one complex right-hand side: first term in d_bW, initial running sum in d_bsum
+// (row pairs); A * sum to d_bres.  Stop rules as neumann_real (the reference rule on the real parts
+// of the complex-basis layer sums, as StopIteration takes creal, Kernels_selfsub.c:1184-1220).
+static int neumann_cplx(rte_ctx* c, int flag, const rte_stop* stop, int* nterms, double* last_rel) {
+  const int vs = 2 * c->C, cp = (2 * c->cstride + 3) / 4 * 4;
+  const bool mixed = c->precision == RTE_PREC_MIXED;
+  int terms = 0;
+  double rel = 0.0;
+  if (flag) {
+    if (mixed)
+      CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, vs, cp, c->C,
+                                                          c->cstride, c->st)));
+    const int flag_l = c->cfg.g != 0.0 ? 1 : 0;
+    const int rule = stop->rule;
+    const int maxt = rule == RTE_STOP_REFERENCE ? 10000 : stop->max_terms;
+    int n = c->model == RTE_MODEL_CPU ? 1 : 2;
+    double fi = 1.0;
+    double hred[4] = {0, 0, 0, 0};
+    if (rule == RTE_STOP_REFERENCE) {
+      CUDA_TRY(c, cudaMemsetAsync(c->d_red, 0, 4 * sizeof(double), c->st));
+      CUDA_TRY(c, (c->launches++, rte_launch_layer_sums(c->d_bW, c->d_bsum, c->N, c->nx, c->ny, c->nz, c->C, c->d_red,
+                                                        c->st, 1)));
+      CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CUDA_TRY(c, cudaStreamSynchronize(c->st));
+    }
+    for (;;) {
+      if (rule == RTE_STOP_REFERENCE) {
+        const double sumW = hred[2], sumOut = hred[3];
+        double hi = 0.0;
+        bool stopnow = false;
+        if (n > 1) {
+          if (sumOut == 0.0) {
+            stopnow = true;
+          } else {
+            hi = 1.0 - (sumW / sumOut) * (1.0 / (1.0 - (sumW / sumOut) / fi));
+            fi = sumW / sumOut;
+            if (hi > 1.0 || hi < 0.0) hi = 0.0;
+          }
+        }
+        if (stopnow || hi > 0.9999 || terms >= maxt) break;
+      } else if (terms >= maxt) {
+        break;
+      }
+      n++;
+      int rc = apply_term(c, c->d_bW, c->d_bWf, c->d_bWn, mixed ? c->d_bWf : nullptr, c->d_bsum, flag_l, 1, 2);
+      if (rc) return rc;
+      std::swap(c->d_bW, c->d_bWn);
+      terms++;
+      if (rule != RTE_STOP_FIXED) {
+        CUDA_TRY(c, cudaMemcpyAsync(hred, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CUDA_TRY(c, cudaStreamSynchronize(c->st));
+        rel = hred[1] > 0 ? sqrt(hred[0] / hred[1]) : 0.0;
+        if (rule == RTE_STOP_REL_L2 && rel < stop->tol) break;
+      }
+    }
+  }
+  if (mixed)
+    CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bsum, c->d_bWf, c->d_islot, c->N, vs, cp, c->C,
+                                                        c->cstride, c->st)));
+  int rc = apply_term(c, c->d_bsum, c->d_bWf, c->d_bres, nullptr, nullptr, 1, 0, 2);
+  if (!rc) rc = check_kernel_err(c);
+  if (rc) return rc;
+  if (nterms) *nterms = terms;
+  if (last_rel) *last_rel = rel;
+  return RTE_OK;
+}
+
+extern "C" int rte_set_modulation(rte_ctx* c, double modulation) {
+  if (!c) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!std::isfinite(modulation)) return fail(c, RTE_ERR_ARG, "modulation must be finite");
+  if (modulation != 0.0 && c->model == RTE_MODEL_FIM)
+    return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation takes the exact or the CPU-package model");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  const double kappa = modulation / c->cm;  // mu_a + i modulation / (c/n), RTE_uniform.c:129
+  if (kappa != 0.0 && !c->d_fball_im) {
+    const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+    CUDA_TRY(c, dalloc(c, &c->d_fball_im, npix));
+  }
+  const bool changed = kappa != c->kappa;
+  c->modulation = modulation;
+  c->kappa = kappa;
+  if (changed && c->medium_set) {
+    int rc = ensure_moments(c, std::hypot(c->mumax, c->kappa));
+    if (!rc) rc = build_self_lut(c);
+    if (rc) return rc;
+  }
+  return RTE_OK;
+}
+
+static int unsupported_modulated(rte_ctx* c, const char* what) {
+  return fail(c, RTE_ERR_UNSUPPORTED, "%s is not available under intensity modulation (rte_set_modulation 0)", what);
+}
+
 extern "C" int rte_prop_abs(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int flag, int flag_scat) {
   if (!c || !in || !out) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  if (c->kappa != 0.0) {  // complex operator on the (real, imaginary) pair
+    int rc = ensure_batch(c, 2);
+    if (!rc) rc = upload_pair(c, in, c->d_bW);
+    if (rc) return rc;
+    if (c->precision == RTE_PREC_MIXED)
+      CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_bW, c->d_bWf, c->d_islot, c->N, 2 * c->C,
+                                                          (2 * c->cstride + 3) / 4 * 4, c->C, c->cstride, c->st)));
+    rc = apply_term(c, c->d_bW, c->d_bWf, c->d_bres, nullptr, nullptr, flag, flag_scat, 2);
+    if (!rc) rc = check_kernel_err(c);
+    if (rc) return rc;
+    return download_pair(c, c->d_bres, out);
+  }
   bool has2 = false;
   int rc = upload_cplx(c, in, c->d_aux1, c->d_aux2, &has2);
   if (rc) return rc;
@@ -1239,6 +1409,17 @@ extern "C" int rte_neumann(rte_ctx* c, const rte_cplx* src, rte_cplx* out, int f
   if (!c || !out || (flag && (!src || !stop))) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  if (c->kappa != 0.0) {  // one complex series: src -> first term, out -> initial sum
+    int rc = ensure_batch(c, 2);
+    if (!rc) rc = upload_pair(c, out, c->d_bsum);
+    if (!rc && flag) rc = upload_pair(c, src, c->d_bW);
+    int terms = 0;
+    if (!rc) rc = neumann_cplx(c, flag, stop, &terms, nullptr);
+    if (!rc) rc = download_pair(c, c->d_bres, out);
+    if (rc) return rc;
+    if (nterms) *nterms = terms;
+    return RTE_OK;
+  }
   // real parts: src -> (aux1, aux2), out -> (aux3, aux4); each Neumann copies its inputs
   // into its own work buffers first, so the result of part k overwrites the input sum of part k.
   bool o_has2 = false, s_has2 = false;
@@ -1347,19 +1528,27 @@ static void beam_coefs(const rte_ctx* c, int face, double scale, double* coef) {
     }
 }
 
+// Under intensity modulation (c->kappa != 0) the attenuation is complex: d_dst holds (real, imaginary)
+// row pairs (vstride >= 2 C) and the ballistic flux's imaginary part goes to d_fball_im.
 static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vstride = 0, double* d_fball = nullptr,
-                         bool zero = true, double* d_q = nullptr) {
-  if (s->modulation != 0.0) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation is not supported");
+                         bool zero = true, double* d_q = nullptr, double* d_fball_im = nullptr) {
+  if (s->modulation != 0.0 && s->modulation != c->modulation)
+    return fail(c, RTE_ERR_STATE, "source modulation %g differs from the context's %g (rte_set_modulation)",
+                s->modulation, c->modulation);
   std::vector<int> cols;
   double scale;
   if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source kind %d / face %d", s->kind, s->face);
   if ((int)cols.size() > RTE_MAX_SRC_COLS) return fail(c, RTE_ERR_UNSUPPORTED, "beam covers more than %d columns", RTE_MAX_SRC_COLS);
   if (vstride <= 0) vstride = c->C;
+  const bool cplx = c->kappa != 0.0;
+  if (cplx && vstride < 2 * c->C) return fail(c, RTE_ERR_STATE, "a modulated source needs (real, imaginary) row pairs");
   const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
   if (!d_fball) d_fball = c->d_fball;
+  if (cplx && !d_fball_im) d_fball_im = c->d_fball_im;
   if (zero) {
     CUDA_TRY(c, cudaMemsetAsync(d_dst, 0, (size_t)c->N * vstride * sizeof(double), c->st));
     CUDA_TRY(c, cudaMemsetAsync(d_fball, 0, npix * sizeof(double), c->st));
+    if (cplx) CUDA_TRY(c, cudaMemsetAsync(d_fball_im, 0, npix * sizeof(double), c->st));
   }
   if (cols.empty()) return RTE_OK;
   if (s->kind == RTE_SRC_POINT) {
@@ -1393,6 +1582,8 @@ static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vst
   a.mus = c->d_mus;
   a.W = d_dst;
   a.fball = d_fball;
+  a.kappa = c->kappa;
+  a.fball_im = cplx ? d_fball_im : nullptr;
   CUDA_TRY(c, (c->launches++, rte_launch_source(a, c->st)));
   return RTE_OK;
 }
@@ -1445,7 +1636,8 @@ static int image_weights(rte_ctx* c, const rte_source* s, ImgArgs& a) {
 // images of a real-basis distribution on the device; with_ball adds the ballistic term left in
 // d_ball by the last launch_source.
 static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool with_ball, rte_cplx* trans,
-                      rte_cplx* ref, int vstride = 0, const double* d_fball = nullptr) {
+                      rte_cplx* ref, int vstride = 0, const double* d_fball = nullptr, const double* d_out_im = nullptr,
+                      const double* d_fball_im = nullptr) {
   ImgArgs a;
   memset(&a, 0, sizeof a);
   a.nx = c->nx;
@@ -1459,6 +1651,8 @@ static int run_images(rte_ctx* c, const double* d_out, const rte_source* s, bool
   if (rc) return rc;
   const size_t np = (size_t)c->nx * c->ny;
   a.fball = with_ball ? (d_fball ? d_fball : c->d_fball) : nullptr;
+  a.fball_im = with_ball ? d_fball_im : nullptr;
+  a.out_im = d_out_im;
   a.trans = c->d_img;
   a.ref = c->d_img + 2 * np;
   CUDA_TRY(c, (c->launches++, rte_launch_images(a, c->st)));
@@ -1472,6 +1666,12 @@ extern "C" int rte_source_beam(rte_ctx* c, const rte_source* s, rte_cplx* xi) {
   if (!c || !s || !xi) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  if (c->kappa != 0.0) {
+    int rc = ensure_batch(c, 2);
+    if (!rc) rc = launch_source(c, s, c->d_bW, 2 * c->C);
+    if (rc) return rc;
+    return download_pair(c, c->d_bW, xi);
+  }
   int rc = launch_source(c, s, c->d_aux1);
   if (rc) return rc;
   return download_cplx(c, c->d_aux1, nullptr, xi);
@@ -1482,6 +1682,14 @@ extern "C" int rte_images(rte_ctx* c, const rte_cplx* out, const rte_source* s, 
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   int rc;
+  if (c->kappa != 0.0) {  // complex ballistic term and both parts of the distribution in one pass
+    rc = ensure_batch(c, 2);
+    if (!rc && s) rc = launch_source(c, s, c->d_bW, 2 * c->C, nullptr, true, c->d_bq);
+    bool has2 = false;
+    if (!rc) rc = upload_cplx(c, out, c->d_aux1, c->d_aux2, &has2);
+    if (rc) return rc;
+    return run_images(c, c->d_aux1, s, s != nullptr, trans, ref, 0, nullptr, c->d_aux2, c->d_fball_im);
+  }
   if (s) {  // ballistic term of this source (the source itself goes to scratch)
     rc = launch_source(c, s, c->d_aux3, 0, nullptr, true, c->d_aux4);
     if (rc) return rc;
@@ -1523,11 +1731,61 @@ static int series_start(rte_ctx* c, double* d_xi, double* d_q, double* d_w0, int
   return RTE_OK;
 }
 
+// Modulated forward solve: source with complex attenuation, complex series, complex images.
+static int forward_cplx(rte_ctx* c, const rte_source* s, const rte_stop* stop, rte_cplx* W_out, rte_cplx* trans,
+                        rte_cplx* ref, int* terms, double* rel) {
+  int rc = ensure_batch(c, 2);
+  if (rc) return rc;
+  const size_t NC = (size_t)c->N * c->C;
+  const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bsum, 0, 2 * NC * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bq, 0, 2 * NC * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_bball, 0, 2 * npix * sizeof(double), c->st));
+  c->has_point = false;
+  rc = launch_source(c, s, c->d_bsum, 2 * c->C, c->d_bball, false, c->d_bq, c->d_bball + npix);
+  // W0 -> d_bW, S0 -> d_bsum
+  if (!rc) rc = series_start(c, c->d_bsum, c->d_bq, c->d_bW, 2, c->d_bWf, (2 * c->cstride + 3) / 4 * 4);
+  if (!rc) rc = neumann_cplx(c, 1, stop, terms, rel);
+  if (!rc && (trans || ref))
+    rc = run_images(c, c->d_bres, s, true, trans, ref, 2 * c->C, c->d_bball, c->d_bres + c->C, c->d_bball + npix);
+  if (!rc && W_out) rc = download_pair(c, c->d_bres, W_out);
+  return rc;
+}
+
 extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop, rte_cplx* W_out, rte_cplx* trans,
                            rte_cplx* ref, rte_report* rep) {
   if (!c || !s || !stop) return fail(c, RTE_ERR_ARG, "null argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  if (s->modulation != c->modulation) {  // a solve runs at its source's modulation
+    int rc = rte_set_modulation(c, s->modulation);
+    if (rc) return rc;
+  }
+  if (c->kappa != 0.0) {
+    cudaEvent_t t0, t1;
+    CUDA_TRY(c, cudaEventCreate(&t0));
+    CUDA_TRY(c, cudaEventCreate(&t1));
+    CUDA_TRY(c, cudaEventRecord(t0, c->st));
+    int terms = 0;
+    double rel = 0.0;
+    int rc = forward_cplx(c, s, stop, W_out, trans, ref, &terms, &rel);
+    float ms = 0;
+    if (!rc) {
+      CUDA_TRY(c, cudaEventRecord(t1, c->st));
+      CUDA_TRY(c, cudaEventSynchronize(t1));
+      cudaEventElapsedTime(&ms, t0, t1);
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    if (rep) {
+      rep->terms = terms;
+      rep->last_rel = rel;
+      rep->ms_device = ms;
+      rep->ms_setup = c->last_setup_ms;
+    }
+    return RTE_OK;
+  }
   cudaEvent_t t0, t1;
   CUDA_TRY(c, cudaEventCreate(&t0));
   CUDA_TRY(c, cudaEventCreate(&t1));
@@ -1713,7 +1971,9 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   if (stop->rule == RTE_STOP_REFERENCE)
     return fail(c, RTE_ERR_UNSUPPORTED, "batched solves take a fixed or relative-L2 stop rule");
   const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
-  if (c->precision != RTE_PREC_MIXED || nsrc == 1) {  // one source at a time
+  bool modulated = c->kappa != 0.0;
+  for (int b = 0; b < nsrc; b++) modulated = modulated || srcs[b].modulation != 0.0;
+  if (c->precision != RTE_PREC_MIXED || nsrc == 1 || modulated) {  // one source at a time
     double ms = 0;
     rte_report r1;
     for (int b = 0; b < nsrc; b++) {
@@ -1934,6 +2194,7 @@ static int forward_with_flux(rte_ctx* c, const rte_source* s, const rte_stop* st
 }
 
 static int check_detector(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* d) {
+  if (c && c->kappa != 0.0) return unsupported_modulated(c, "binned detectors");
   if (!srcs || !stop || !d || nsrc < 1) return fail(c, RTE_ERR_ARG, "null argument");
   if (d->nbins < 1 || d->nbins > 1024 || d->faces <= 0 || d->faces > 63) return fail(c, RTE_ERR_ARG, "bad detector");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
@@ -2022,6 +2283,7 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
                             const rte_detector* d, const double* target, double* loss, double* g_mua,
                             double* g_mus) {
   if (!c || !target || !g_mua || !g_mus) return fail(c, RTE_ERR_ARG, "null argument");
+  if (c->kappa != 0.0) return unsupported_modulated(c, "the adjoint gradient");
   for (int q = 0; q < nsrc && srcs; q++)
     if (srcs[q].kind != RTE_SRC_COLUMN && srcs[q].kind != RTE_SRC_FIM &&
         !(srcs[q].kind == RTE_SRC_BEAM && srcs[q].face == 0))
@@ -2351,6 +2613,9 @@ extern "C" int rte_forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, i
                                  rte_cplx* ref, rte_report* rep) {
   if (!c || !srcs || nsrc < 1 || nsrc > kMaxBatch || nterms < 0) return fail(c, RTE_ERR_ARG, "bad argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (c->kappa != 0.0) return unsupported_modulated(c, "graph replay");
+  for (int b = 0; b < nsrc; b++)
+    if (srcs[b].modulation != 0.0) return unsupported_modulated(c, "graph replay");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   float ms = 0;
   int rc = forward_graph(c, nsrc, srcs, nterms, trans, ref, &ms);
@@ -2398,6 +2663,7 @@ extern "C" int rte_region_gradient(rte_ctx* c, const rte_source* s, const rte_st
                                    double* grads, double* grads2, double* residual, double* residual2) {
   if (!c || !s || !stop || !g || !tiss || ntypes < 2 || !grada || !grada2 || !grads || !grads2)
     return fail(c, RTE_ERR_ARG, "null argument");
+  if (c->kappa != 0.0 || s->modulation != 0.0) return unsupported_modulated(c, "the region gradient");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   const size_t np = (size_t)c->nx * c->ny;
@@ -2458,6 +2724,7 @@ extern "C" int rte_fisher_regions(rte_ctx* c, const rte_source* s, const rte_sto
                                   int image, double* F) {
   if (!c || !s || !stop || P < 1 || !masks || !F || image < 0 || image > 2) return fail(c, RTE_ERR_ARG, "bad argument");
   if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (c->kappa != 0.0 || s->modulation != 0.0) return unsupported_modulated(c, "the Fisher information");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   const size_t np = (size_t)c->nx * c->ny;
   std::vector<rte_cplx> gt(np), gr(np), t(np), rr(np);
@@ -2545,6 +2812,7 @@ static int tangent_dA(rte_ctx* c, const double* d_in, double* d_outT, const std:
   sa.scale = c->dV / c->cm;
   sa.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
   sa.out = c->d_selfp;
+
   sa.dmut = c->d_dmut;
   sa.dlut = c->d_dlut;
   CUDA_TRY(c, (c->launches++, rte_launch_self(sa, c->st)));
@@ -2572,6 +2840,7 @@ static int tangent_dA(rte_ctx* c, const double* d_in, double* d_outT, const std:
 extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* d,
                           int P, const double* dmua, const double* dmus, double* J, double* F) {
   if (!c || P < 1 || !dmua || !dmus || !F) return fail(c, RTE_ERR_ARG, "null argument");
+  if (c->kappa != 0.0) return unsupported_modulated(c, "the Fisher information");
   int rc = check_detector(c, nsrc, srcs, stop, d);
   if (rc) return rc;
   for (int q = 0; q < nsrc; q++)

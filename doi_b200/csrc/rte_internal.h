@@ -34,6 +34,9 @@ struct PairArgs {
   const double* dmut;
   int box_lo[3], box_hi[3];  // (x, y, z) voxel indices
   const int* islot;          // voxel -> slot (row of the stored kernel)
+  // intensity modulation: mu_t has the uniform imaginary part kappa, so every pair kernel gains the
+  // phase exp(-i kappa |r - r'|); the right-hand sides are complex, (real, imaginary) pairs of rows
+  double kappa;
 };
 
 struct EpiArgs {
@@ -49,6 +52,7 @@ struct EpiArgs {
   int cpad, cstride;
   double* sum;          // running sum (null = do not accumulate)
   double* red;          // [0] ||Wout||^2 [1] ||sum||^2 [2] stop-layer sum of Wout [3] of sum
+  int cplx;             // right-hand sides are (real, imaginary) pairs: odd ones are imaginary parts
 };
 
 struct SelfArgs {
@@ -64,6 +68,10 @@ struct SelfArgs {
   // derivative mode: out = scale * dmut(r) * dD/dmu(mu_t(r)) W (dlut rows, or the series' derivative)
   const double* dmut;   // null: the self term itself
   const double* dlut;   // [ndistinct][Cfull][Cfull]
+  // complex mu_t = mu_t + i kappa (intensity modulation): W holds (real, imaginary) pairs of rows,
+  // lut_im the imaginary parts of the table (the power series takes the complex mu_t directly)
+  double kappa;
+  const double* lut_im;
 };
 
 struct ImgArgs {
@@ -72,6 +80,8 @@ struct ImgArgs {
   double wt[RTE_MAX_L + 1];  // transmission weights per l (m = 0 coefficient)
   double wr[RTE_MAX_L + 1];  // reflection weights per l
   const double* fball;       // ballistic flux per face pixel (z- first, z+ next); may be null
+  const double* fball_im;    // its imaginary part under intensity modulation (may be null)
+  const double* out_im;      // imaginary-part distribution, same layout as out (may be null)
   double* trans;  // nx*ny complex (re, im)
   double* ref;
 };
@@ -95,6 +105,10 @@ struct SrcArgs {
   const double* mus;
   double* W;     // N x vstride, zeroed by the caller
   double* fball; // ballistic exitant flux per face pixel (all six faces), zeroed by the caller
+  // intensity modulation: attenuation with mu_t + i kappa; the imaginary part of the source goes to
+  // W + Cfull (the second row of each voxel's pair) and that of the ballistic flux to fball_im
+  double kappa;
+  double* fball_im;
 };
 
 // detector faces and the adjoint gradient
@@ -202,16 +216,18 @@ ShTables make_sh_tables();
 void sh_real_host(const ShTables& t, int L, double x, double y, double z, double* R);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
-cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm);
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm,
+                               int cplx = 0);
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);
 cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st);
 cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st);
+// complex basis -> real parts; u1/u2 rows ostride apart (0: C)
 cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
-                               cudaStream_t st);
+                               cudaStream_t st, int ostride = 0);
 cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx, int N, int L,
                                cudaStream_t st, int ustride = 0);
 cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
-                                  double* red, cudaStream_t st);
+                                  double* red, cudaStream_t st, int cplx = 0);
 cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
 // FP64 [N][vstride] (voxel order) -> FP32 [slot][cpad] (slot order)
 cudaError_t rte_launch_to_f32_slots(const double* a, float* b, const int* islot, int N, int vstride, int cpad,

@@ -219,28 +219,35 @@ __device__ __forceinline__ A path_sum(int i, int j, int k, int ip, int jp, int k
 }
 
 // ---------------------------------------------------------------------------------------------
-// Plain FP64 method: every pair recomputed in FP64 (path integral, SH, projections).
-template <int LA, bool TABLE>
+// Plain FP64 method: every pair recomputed in FP64 (path integral, SH, projections).  CPLX: one
+// complex right-hand side stored as (real, imaginary) rows per voxel, and the pair kernel carries the
+// modulation phase exp(-i kappa |r - r'|) (complex mu_t = mu_t + i kappa, uniform imaginary part).
+template <int LA, bool TABLE, bool CPLX>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
-  __shared__ double sW[RTE_PAIR_TS * C];
+  constexpr int NP = CPLX ? 2 : 1;        // rows per voxel
+  constexpr int TS = RTE_PAIR_TS / NP;    // sources per shared-memory tile
+  __shared__ double sW[TS * NP * C];
   const int tid = threadIdx.x;
   const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
   const bool act = slot < a.N;
   const int r = act ? a.perm[slot] : 0;
   const int plane = a.nx * a.ny;
   const int i = r / plane, j = (r / a.nx) % a.ny, k = r % a.nx;
-  double acc[C];
+  const int vs = NP * a.Cfull;
+  double acc[NP][C];
 #pragma unroll
-  for (int c = 0; c < C; ++c) acc[c] = 0.0;
+  for (int p = 0; p < NP; ++p)
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[p][c] = 0.0;
   const int sb = blockIdx.y * a.chunk;
   const int se = min(a.N, sb + a.chunk);
-  for (int s0 = sb; s0 < se; s0 += RTE_PAIR_TS) {
-    const int ns = min(RTE_PAIR_TS, se - s0);
+  for (int s0 = sb; s0 < se; s0 += TS) {
+    const int ns = min(TS, se - s0);
     __syncthreads();
-    for (int q = tid; q < ns * C; q += RTE_PAIR_THREADS) {
-      const int sv = q / C, c = q - sv * C;
-      sW[q] = a.Win[(size_t)(s0 + sv) * a.Cfull + c];
+    for (int q = tid; q < ns * NP * C; q += RTE_PAIR_THREADS) {
+      const int sv = q / (NP * C), e = q - sv * NP * C, p = e / C, c = e - p * C;
+      sW[q] = a.Win[(size_t)(s0 + sv) * vs + (size_t)p * a.Cfull + c];
     }
     __syncthreads();
     if (!act) continue;
@@ -263,15 +270,31 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
           }
           double R[C];
           sh_eval<LA, double>(ux, uy, uz, R);
-          double S = 0.0;
+          double S[NP];
 #pragma unroll
-          for (int c = 0; c < C; ++c) S = fma(R[c], sW[sv * C + c], S);
+          for (int p = 0; p < NP; ++p) {
+            S[p] = 0.0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) S[p] = fma(R[c], sW[(sv * NP + p) * C + c], S[p]);
+          }
           int Q;
           const double ps = path_sum<double, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q);
           const double tau = ps * dist / (double)Q;
-          const double t = exp(-tau) * a.kscale / d2 * S;
+          const double kk = exp(-tau) * a.kscale / d2;
+          if (CPLX) {  // kk exp(-i kappa dist) (S0 + i S1)
+            double sn, cs;
+            sincos(a.kappa * dist, &sn, &cs);
+            const double t0 = kk * (cs * S[0] + sn * S[NP - 1]), t1 = kk * (cs * S[NP - 1] - sn * S[0]);
 #pragma unroll
-          for (int c = 0; c < C; ++c) acc[c] = fma(R[c], t, acc[c]);
+            for (int c = 0; c < C; ++c) {
+              acc[0][c] = fma(R[c], t0, acc[0][c]);
+              acc[NP - 1][c] = fma(R[c], t1, acc[NP - 1][c]);
+            }
+          } else {
+            const double t = kk * S[0];
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[0][c] = fma(R[c], t, acc[0][c]);
+          }
         }
       }
       if (++kp == a.nx) {
@@ -284,9 +307,11 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
     }
   }
   if (act) {
-    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * a.Cfull;
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * vs;
 #pragma unroll
-    for (int c = 0; c < C; ++c) o[c] = acc[c];
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+      for (int c = 0; c < C; ++c) o[(size_t)p * a.Cfull + c] = acc[p][c];
   }
 }
 
@@ -477,8 +502,11 @@ struct MixedLayout {
   }
 };
 
-template <int LA, bool TABLE, bool STORED, int NB>
+// CPLX (NB = 2): the two right-hand sides are the real and imaginary parts of one complex one and the
+// pair kernel carries the modulation phase exp(-i kappa |r - r'|).
+template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
+  static_assert(!CPLX || NB == 2, "a complex right-hand side is a (real, imaginary) pair");
   constexpr int C = (LA + 1) * (LA + 1), TS = RTE_PAIR_TS, T = RTE_PAIR_THREADS;
   const int CP = a.cpad;  // FP32 source row: nb * Cfull floats, padded to a multiple of 4
   const MixedLayout Sh(CP, NB * C);
@@ -588,6 +616,32 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
           f2_t R2[C2];
 #pragma unroll
           for (int c = 0; c < C2; ++c) R2[c] = f2_pack((float)R[2 * c], 2 * c + 1 < C ? (float)R[2 * c + 1] : 0.f);
+          if constexpr (CPLX) {
+            float Sv[2];
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+              const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+              f2_t Sa = 0ull, Sb = 0ull;
+#pragma unroll
+              for (int c = 0; c < C2; c += 2) {
+                Sa = f2_fma(R2[c], w[c], Sa);
+                if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+              }
+              float a0, a1, b0, b1;
+              f2_unpack(Sa, a0, a1);
+              f2_unpack(Sb, b0, b1);
+              Sv[b] = (a0 + a1) + (b0 + b1);
+            }
+            float sn, cs;
+            sincosf((float)a.kappa * sqrtf(d2), &sn, &cs);
+            const float t0 = kk * (cs * Sv[0] + sn * Sv[1]), t1 = kk * (cs * Sv[1] - sn * Sv[0]);
+            const f2_t T0 = f2_pack(t0, t0), T1 = f2_pack(t1, t1);
+#pragma unroll
+            for (int c = 0; c < C2; ++c) {
+              acc[0][c] = f2_fma(R2[c], T0, acc[0][c]);
+              acc[NB - 1][c] = f2_fma(R2[c], T1, acc[NB - 1][c]);
+            }
+          } else {
 #pragma unroll
           for (int b = 0; b < NB; ++b) {
             const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
@@ -604,6 +658,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
             const f2_t T2 = f2_pack(tb, tb);
 #pragma unroll
             for (int c = 0; c < C2; ++c) acc[b][c] = f2_fma(R2[c], T2, acc[b][c]);
+          }
           }
         }
       }
@@ -693,6 +748,18 @@ __global__ void __launch_bounds__(RTE_KT) k_store_kernel(PairArgs a) {
   }
 }
 
+// Weight of real coefficient c in the reference stop rule's layer sum, sum over m of Re(w_lm) in the
+// complex basis (dist.cu:1143-1152): for a real function R_l0 + sqrt2 R_l,m (even m > 0); for the
+// imaginary part f2 of a complex function (w = w1 + i w2, Re(i w2_lm) = -Im(w2_lm)) sqrt2 R_l,-m for
+// odd m > 0.
+__device__ __forceinline__ double stop_weight(int c, bool imag) {
+  int l = 0;
+  while ((l + 1) * (l + 1) <= c) ++l;
+  const int m = c - l * l - l;
+  if (imag) return (m < 0 && ((-m) & 1)) ? 1.4142135623730951 : 0.0;
+  return m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Epilogue: add split-K partials, self-voxel term, scatter; write the next term (FP64 and FP32),
 // accumulate the running sum and the norms used by the stop rules.
@@ -735,11 +802,7 @@ __global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
           s2 += sv * sv;
         }
         if (stop_layer) {
-          // sum of Re(w_lm) over m in the complex basis = R_l0 + sqrt2 * R_l,m for even m > 0
-          int l = 0;
-          while ((l + 1) * (l + 1) <= c) ++l;
-          const int m = c - l * l - l;
-          const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
+          const double wgt = stop_weight(c, a.cplx && (b & 1));
           lw += wgt * x;
           ls += wgt * sv;
         }
@@ -798,11 +861,56 @@ __global__ void k_self(SelfArgs a) {
   a.out[base + c] = a.scale * u;
 }
 
+// Self-voxel term with the complex mu_t + i kappa of intensity modulation (the CPU package's
+// (1 - exp(-mu_t beta)) / mu_t with complex mu_t, Kernels_selfsub.c:927-946): W holds (real,
+// imaginary) row pairs; D from the complex table (lut, lut_im) or the power series in the complex
+// mu_t.  One thread per voxel, complex right-hand side and output coefficient.
+__global__ void k_self_cplx(SelfArgs a) {
+  const int npair = a.nb / 2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)a.N * npair * a.Cact;
+  if (t >= total) return;
+  const int c = (int)(t % a.Cact);
+  const int p = (int)((t / a.Cact) % npair);
+  const int r = (int)(t / ((long long)a.Cact * npair));
+  const size_t base = (size_t)r * a.nb * a.Cfull + (size_t)(2 * p) * a.Cfull;
+  const double* w0 = a.W + base;
+  const double* w1 = w0 + a.Cfull;
+  double ur = 0.0, ui = 0.0;
+  if (a.idx) {
+    const size_t row = ((size_t)a.idx[r] * a.Cfull + c) * a.Cfull;
+    const double* Dr = a.lut + row;
+    const double* Di = a.lut_im + row;
+    for (int cp = 0; cp < a.Cact; ++cp) {
+      const double dr = __ldg(Dr + cp), di = __ldg(Di + cp), x0 = __ldg(w0 + cp), x1 = __ldg(w1 + cp);
+      ur = fma(dr, x0, fma(-di, x1, ur));
+      ui = fma(dr, x1, fma(di, x0, ui));
+    }
+  } else {  // Horner in the complex mu: u <- mu u + M_k w
+    const double mr = a.mut[r], mi = a.kappa;
+    for (int kk = a.K - 1; kk >= 0; --kk) {
+      const double* M = a.mom + ((size_t)kk * a.Cfull + c) * a.Cfull;
+      double t0 = 0.0, t1 = 0.0;
+      for (int cp = 0; cp < a.Cact; ++cp) {
+        const double m = __ldg(M + cp);
+        t0 = fma(m, __ldg(w0 + cp), t0);
+        t1 = fma(m, __ldg(w1 + cp), t1);
+      }
+      const double nr = mr * ur - mi * ui + t0, ni = mr * ui + mi * ur + t1;
+      ur = nr;
+      ui = ni;
+    }
+  }
+  a.out[base + c] = a.scale * ur;
+  a.out[base + a.Cfull + c] = a.scale * ui;
+}
+
 // Exitance images of the z = nZ-1 and z = 0 faces from the m = 0 coefficients
 // (FisherInfo_IO/src/dist.cu:103-161, 229-268; the per-l weights come from the host).
-__global__ void k_images(ImgArgs a, const double* out_im) {
+__global__ void k_images(ImgArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.nx * a.ny) return;
+  const double* out_im = a.out_im;
   const size_t rt = (size_t)(a.nz - 1) * a.nx * a.ny + p, rr = (size_t)p;
   double t = 0.0, f = 0.0, ti = 0.0, fi = 0.0;
   for (int l = 0; l <= a.L; ++l) {
@@ -817,6 +925,10 @@ __global__ void k_images(ImgArgs a, const double* out_im) {
   if (a.fball) {
     t += a.fball[(size_t)a.nx * a.ny + p];
     f += a.fball[p];
+  }
+  if (a.fball_im) {
+    ti += a.fball_im[(size_t)a.nx * a.ny + p];
+    fi += a.fball_im[p];
   }
   if (a.trans) {
     a.trans[2 * p] = t;
@@ -857,33 +969,67 @@ __global__ void k_source(SrcArgs a) {
     base = row * plane + col * a.nx;
     stride = 1;
   }
-  double att = 1.0, mt = 0.0;
+  // attenuation with mu_t + i kappa (kappa = 0: the steady state); complex values as (re, im)
+  const double kap = a.kappa;
+  auto cexpm = [kap](double m, double x, double& re, double& im) {  // exp(-(m + i kap) x)
+    const double e = exp(-m * x);
+    double sn = 0.0, cs = 1.0;
+    if (kap != 0.0) sincos(kap * x, &sn, &cs);
+    re = e * cs;
+    im = -e * sn;
+  };
+  double attr = 1.0, atti = 0.0, mt = 0.0;
   for (int t = 0; t < n; ++t) {
     const size_t r = (size_t)base + (size_t)(up ? t : n - 1 - t) * stride;
     mt = a.mut[r];
     const double ms = a.mus[r];
-    double v;
+    double vr, vi, er, ei;
+    cexpm(mt, a.dlen, er, ei);
     if (a.kind == 2) {  // absolute depth of the voxel top (z- entry only)
       const double tz = (double)t * a.dz + a.z_min + a.dz / 2.0 - a.dz / 2.0;
-      v = exp(-mt * tz) - exp(-mt * (tz + a.dz));
-    } else {
-      v = att * (1 - exp(-mt * a.dlen));
+      double e1r, e1i, e2r, e2i;
+      cexpm(mt, tz, e1r, e1i);
+      cexpm(mt, tz + a.dz, e2r, e2i);
+      vr = e1r - e2r;
+      vi = e1i - e2i;
+    } else {  // att * (1 - exp(-mu dlen))
+      vr = attr * (1.0 - er) + atti * ei;
+      vi = atti * (1.0 - er) - attr * ei;
     }
-    att *= exp(-mt * a.dlen);
-    const double amp = ms / mt * v / a.dV;
+    const double nr = attr * er - atti * ei, ni = attr * ei + atti * er;
+    attr = nr;
+    atti = ni;
+    // amp = ms / (mt + i kap) * v / dV
+    double ar, ai = 0.0;
+    if (kap == 0.0) {
+      ar = ms / mt * vr / a.dV;
+    } else {
+      const double den = mt * mt + kap * kap;
+      ar = ms * (mt * vr + kap * vi) / den / a.dV;
+      ai = ms * (mt * vi - kap * vr) / den / a.dV;
+    }
     for (int c = 0; c < a.Cfull; ++c)
-      if (a.coef[c] != 0.0) a.W[r * a.vstride + c] += amp * a.coef[c];
+      if (a.coef[c] != 0.0) {
+        a.W[r * a.vstride + c] += ar * a.coef[c];
+        if (kap != 0.0) a.W[r * a.vstride + a.Cfull + c] += ai * a.coef[c];
+      }
   }
   // exit face = the opposite face, same in-face pixel
   const int ef = a.face ^ 1;
   const size_t a0 = (size_t)a.nx * a.ny, a1 = (size_t)a.nz * a.nx, a2 = (size_t)a.nz * a.ny;
   const size_t off[6] = {0, a0, 2 * a0, 2 * a0 + a1, 2 * a0 + 2 * a1, 2 * a0 + 2 * a1 + a2};
+  double br, bi;
   if (a.kind == 2) {
     const double zs = (double)(a.nz - 1) * a.dz + a.z_min + a.dz / 2.0;
-    a.fball[off[ef] + p] = a.scale * exp(-mt * (zs + a.dz / 2.0));
+    cexpm(mt, zs + a.dz / 2.0, br, bi);
+    br *= a.scale;
+    bi *= a.scale;
   } else {
-    a.fball[off[ef] + p] = a.mag * att;
+    br = a.mag * attr;
+    bi = a.mag * atti;
   }
+  a.fball[off[ef] + p] = br;
+  if (a.fball_im) a.fball_im[off[ef] + p] = bi;
 }
 
 // mu_t = mu_a + mu_s (FP64 and FP32 copies), mu_s copy, and max(mu_t) into red_max (>= 0 values,
@@ -1266,11 +1412,15 @@ __global__ void k_grad_local(GradLocalArgs a) {
 // Complex reference basis <-> real basis.  w = w1 + i w2 with w1, w2 the coefficient sets of
 // real functions (w_{l,-m} = (-1)^m conj(w_{l,m})).  u_l0 = Re(w_l0), u_l,m = sqrt2 Re(w_lm),
 // u_l,-m = -sqrt2 Im(w_lm) (m > 0).  red[0] accumulates ||u2||^2.
-__global__ void k_to_real(const double* __restrict__ w, double* u1, double* u2, int N, int L, double* red) {
+__global__ void k_to_real(const double* __restrict__ w, double* u1, double* u2, int N, int L, double* red,
+                          int ostride) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double n2 = 0.0;
   if (r < N) {
     const int C = (L + 1) * (L + 1);
+    // u1/u2 rows are ostride apart (a complex right-hand side's real and imaginary rows interleaved)
+    u1 += (size_t)r * ostride - (size_t)r * C;
+    if (u2) u2 += (size_t)r * ostride - (size_t)r * C;
     const double s2 = 1.4142135623730951;
     for (int l = 0; l <= L; ++l) {
       const int c0 = l * l + l;
@@ -1340,21 +1490,22 @@ __global__ void k_to_cplx(const double* __restrict__ u1, const double* __restric
   }
 }
 
-// Stop-rule sums of the layer z = nZ-1 (FisherInfo_IO/src/dist.cu:1143-1152) in the real basis.
+// Stop-rule sums of the layer z = nZ-1 (FisherInfo_IO/src/dist.cu:1143-1152) in the real basis;
+// cplx: (real, imaginary) row pairs per voxel.
 __global__ void k_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
-                             double* red) {
+                             double* red, int cplx) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   double lw = 0.0, ls = 0.0;
+  const int np = cplx ? 2 : 1;
   if (p < nx * ny) {
     const size_t r = (size_t)(nz - 1) * nx * ny + p;
-    for (int c = 0; c < Cfull; ++c) {
-      int l = 0;
-      while ((l + 1) * (l + 1) <= c) ++l;
-      const int m = c - l * l - l;
-      const double wgt = m == 0 ? 1.0 : ((m > 0 && (m % 2) == 0) ? 1.4142135623730951 : 0.0);
-      lw += wgt * W[r * Cfull + c];
-      ls += wgt * S[r * Cfull + c];
-    }
+    for (int q = 0; q < np; ++q)
+      for (int c = 0; c < Cfull; ++c) {
+        const double wgt = stop_weight(c, q == 1);
+        const size_t e = (r * np + q) * Cfull + c;
+        lw += wgt * W[e];
+        ls += wgt * S[e];
+      }
   }
   for (int o = 16; o > 0; o >>= 1) {
     lw += __shfl_xor_sync(0xffffffffu, lw, o);
@@ -1382,10 +1533,10 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 
 // ---------------------------------------------------------------------------------------------
 // launchers
-template <int LA, bool TABLE, bool STORED, int NB>
+template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
   const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1)).bytes;
-  void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB>;
+  void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
@@ -1404,8 +1555,19 @@ static cudaError_t launch_mixed_nb(const PairArgs& a, int table, int stored, cud
 template <int LA>
 static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, int stored, int nb, cudaStream_t st,
                                   int* occ) {
+  if (a.kappa != 0.0) {  // one complex right-hand side (exact SH only)
+    if (table || nb != 2) return cudaErrorInvalidValue;
+    if (precision == 0) {
+      void (*kern)(PairArgs) = k_pair_fp64<LA, false, true>;
+      if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, 0);
+      dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+      kern<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+    return stored ? launch_mixed<LA, false, true, 2, true>(a, st, occ) : launch_mixed<LA, false, false, 2, true>(a, st, occ);
+  }
   if (precision == 0) {
-    void (*kern)(PairArgs) = table ? k_pair_fp64<LA, true> : k_pair_fp64<LA, false>;
+    void (*kern)(PairArgs) = table ? k_pair_fp64<LA, true, false> : k_pair_fp64<LA, false, false>;
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, 0);
     dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
     kern<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
@@ -1438,10 +1600,12 @@ cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table,
   return pair_dispatch(a, LA, precision, table, stored, a.nb > 0 ? a.nb : 1, st, nullptr);
 }
 
-cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm) {
+cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm,
+                               int cplx) {
   PairArgs dummy;
   memset(&dummy, 0, sizeof dummy);
   dummy.cpad = cpad;
+  dummy.kappa = cplx ? 1.0 : 0.0;
   return pair_dispatch(dummy, LA, precision, table, stored, nb, nullptr, blocks_per_sm);
 }
 
@@ -1468,6 +1632,12 @@ cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st) {
 }
 
 cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st) {
+  if (a.kappa != 0.0) {
+    if (a.nb % 2 || a.dmut) return cudaErrorInvalidValue;
+    const long long total = (long long)a.N * (a.nb / 2) * a.Cact;
+    k_self_cplx<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   const long long total = (long long)a.N * a.nb * a.Cact;
   k_self<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
   return cudaGetLastError();
@@ -1475,13 +1645,14 @@ cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st) {
 
 cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st) {
   const int n = a.nx * a.ny;
-  k_images<<<(n + 127) / 128, 128, 0, st>>>(a, nullptr);
+  k_images<<<(n + 127) / 128, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t rte_launch_to_real(const double* cplx, double* u1, double* u2, int N, int L, double* red,
-                               cudaStream_t st) {
-  k_to_real<<<(N + 127) / 128, 128, 0, st>>>(cplx, u1, u2, N, L, red);
+                               cudaStream_t st, int ostride) {
+  const int C = (L + 1) * (L + 1);
+  k_to_real<<<(N + 127) / 128, 128, 0, st>>>(cplx, u1, u2, N, L, red, ostride > 0 ? ostride : C);
   return cudaGetLastError();
 }
 
@@ -1493,9 +1664,9 @@ cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx,
 }
 
 cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
-                                  double* red, cudaStream_t st) {
+                                  double* red, cudaStream_t st, int cplx) {
   const int n = nx * ny;
-  k_layer_sums<<<(n + 127) / 128, 128, 0, st>>>(W, S, N, nx, ny, nz, Cfull, red);
+  k_layer_sums<<<(n + 127) / 128, 128, 0, st>>>(W, S, N, nx, ny, nz, Cfull, red, cplx);
   return cudaGetLastError();
 }
 

@@ -310,11 +310,15 @@ int rte_write_image(const char* path, int nx, int ny, const rte_cplx* img, int c
   return ok ? RTE_OK : RTE_ERR_IO;
 }
 
-int rte_write_phase_image(const char* path, int nx, int ny, const double* phase) {
+int rte_write_phase_image(const char* path, int nx, int ny, const double* phase, int cpu_layout) {
   if (!path || !phase || nx < 1 || ny < 1) return RTE_ERR_ARG;
   FILE* f = fopen(path, "wb");
   if (!f) return RTE_ERR_IO;
-  const int hdr[2] = {ny, nx};  // dist.cu:291-314
+  int hdr[2] = {ny, nx};  // dist.cu:291-314
+  if (cpu_layout) {       // Dist.c:54-55
+    hdr[0] = nx;
+    hdr[1] = ny;
+  }
   const size_t np = (size_t)nx * ny;
   bool ok = fwrite(hdr, sizeof(int), 2, f) == 2 && fwrite(phase, sizeof(double), np, f) == np;
   ok = fclose(f) == 0 && ok;

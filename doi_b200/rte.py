@@ -34,7 +34,7 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
            "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
            "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
-           "rte_cpu_face_outputs")
+           "rte_cpu_face_outputs", "rte_set_modulation")
 
 
 class RteError(RuntimeError):
@@ -207,13 +207,14 @@ def load_library():
     L.rte_problem_free.argtypes = [ctypes.POINTER(_Problem)]
     L.rte_problem_free.restype = None
     L.rte_write_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
-    L.rte_write_phase_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp]
+    L.rte_write_phase_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+    L.rte_set_modulation.argtypes = [P, ctypes.c_double]
     L.rte_read_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp]
     L.rte_region_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, ctypes.c_int,
                                       ctypes.c_int, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
-    L.rte_cpu_face_outputs.argtypes = [ctypes.POINTER(_Config), dp, ctypes.POINTER(_Source), ctypes.c_double, dp, dp,
-                                       dp, dp, dp]
+    L.rte_cpu_face_outputs.argtypes = [ctypes.POINTER(_Config), dp, ctypes.POINTER(_Source), ctypes.c_double,
+                                       ctypes.c_double, dp, dp, dp, dp, dp]
     L.rte_fisher.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.POINTER(_Detector),
                              ctypes.c_int, dp, dp, dp, dp]
     L.rte_fisher_regions.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.c_int, dp, ctypes.c_int,
@@ -319,6 +320,11 @@ class Context:
         s = np.ascontiguousarray(mus_tab, np.float64)
         self._check(self.lib.rte_set_medium_tissue(self.h, _ptr(tiss), len(a), _ptr(a), _ptr(s)),
                     "rte_set_medium_tissue")
+
+    def set_modulation(self, modulation):
+        """Intensity modulation: mu_a -> mu_a + i*modulation/(c/n) (the reference's [Source] modulation);
+        0 restores the steady state.  rte_forward solves at its source's own modulation."""
+        self._check(self.lib.rte_set_modulation(self.h, float(modulation)), "rte_set_modulation")
 
     def _dist(self, W):
         W = np.ascontiguousarray(W, np.complex128).reshape(self.N, self.C)
@@ -618,7 +624,8 @@ def read_image(path, nx, ny):
 
 def cpu_face_outputs(W, nx, ny, nz, nL, x_min, x_max, y_min, y_max, z_min, z_max, src, mu_t, c=1.0, n=1.0):
     """The CPU package's side-face images (-x, +x, -y, +y; x faces (nY, nZ), y faces (nX, nZ)) and
-    photon number of a final distribution W (N x C complex, reference layout); host computation."""
+    photon number of a final distribution W (N x C complex, reference layout); host computation.
+    mu_t may be complex (intensity modulation: mu_t + i*modulation/(c/n))."""
     lib = load_library()
     cfg = _Config(nx, ny, nz, x_min, x_max, y_min, y_max, z_min, z_max, nL, 0.0, 1, 0.0, n, c, MODEL_CPU, 0, 0, 0)
     W = np.ascontiguousarray(W, np.complex128)
@@ -628,8 +635,9 @@ def cpu_face_outputs(W, nx, ny, nz, nL, x_min, x_max, y_min, y_max, z_min, z_max
     sy1 = np.zeros(nz * nx, np.complex128)
     ph = np.zeros(1, np.complex128)
     s = src.c()
-    rc = lib.rte_cpu_face_outputs(ctypes.byref(cfg), _ptr(W), ctypes.byref(s), float(mu_t), _ptr(sx0), _ptr(sx1),
-                                  _ptr(sy0), _ptr(sy1), _ptr(ph))
+    mu_t = complex(mu_t)
+    rc = lib.rte_cpu_face_outputs(ctypes.byref(cfg), _ptr(W), ctypes.byref(s), mu_t.real, mu_t.imag, _ptr(sx0),
+                                  _ptr(sx1), _ptr(sy0), _ptr(sy1), _ptr(ph))
     if rc != 0:
         raise RteError(f"rte_cpu_face_outputs failed ({rc})")
     return [sx0.reshape(ny, nz), sx1.reshape(ny, nz), sy0.reshape(nx, nz), sy1.reshape(nx, nz)], ph[0]

@@ -84,7 +84,9 @@ typedef struct {
   double diam;
   double theta, phi; /* read by the reference, unused */
   double mag;
-  double modulation; /* must be 0: the steady-state path only */
+  double modulation; /* intensity modulation (CPU package/src/RTE_uniform.c:120-176): rte_forward and
+                        rte_forward_batch solve at the source's modulation (rte_set_modulation); other
+                        calls take a source whose modulation is 0 or the context's */
   int kind;          /* RTE_SRC_* */
   int face;          /* RTE_SRC_BEAM / RTE_SRC_POINT: 0 z=0, 1 z=nZ-1, 2 y=0, 3 y=nY-1, 4 x=0, 5 x=nX-1;
                         the position on the face comes from the two in-face coordinates of pos_* */
@@ -121,6 +123,17 @@ int rte_set_medium_tissue(rte_ctx* ctx, const uint8_t* tiss, int ntypes, const d
 int rte_set_medium_voxel(rte_ctx* ctx, const double* mua, const double* mus);
 /* Same with DEVICE pointers (on the context's GPU), for callers whose media are already in HBM. */
 int rte_set_medium_device(rte_ctx* ctx, const double* d_mua, const double* d_mus);
+
+/* Intensity modulation, the reference's [Source] modulation (CPU package/src/RTE_uniform.c:120-176):
+ * mu_a -> mu_a + i * modulation / (c/n) in every voxel, so mu_t gains a uniform imaginary part and
+ * every distribution becomes complex (frequency-domain radiance; its phase is the delay).  While it
+ * is non-zero, rte_source_beam, rte_prop_abs, rte_neumann, rte_images and rte_forward work with the
+ * complex mu_t (pair kernels exp(-(tau + i kappa r)), self term and ballistic terms with the complex
+ * mu_t); the uniform-medium convolution path is not used.  Models RTE_MODEL_EXACT and RTE_MODEL_CPU
+ * (RTE_ERR_UNSUPPORTED for FIM, which reads the key and ignores it); detectors, gradients, Fisher
+ * information and graph replay return RTE_ERR_UNSUPPORTED until it is set back to 0.  The self-term
+ * series needs |mu_t + i kappa| * (half voxel diagonal) <= 12. */
+int rte_set_modulation(rte_ctx* ctx, double modulation);
 
 /* ---- reference entry points ----------------------------------------------------- */
 /* generate_source_beam (FisherInfo_IO/src/dist.cu:66-101): xi = D A (collimated beam). */
@@ -313,7 +326,9 @@ void rte_problem_free(rte_problem* pr);
  * rte_read_image reads a measured image (gFile): 2 ints + nX*nY doubles
  * (compute_grad_rte.cu:151-161). */
 int rte_write_image(const char* path, int nx, int ny, const rte_cplx* img, int cpu_layout);
-int rte_write_phase_image(const char* path, int nx, int ny, const double* phase);
+/* phase images: FisherInfo_IO layout (cpu_layout = 0: nY, nX then the values) or the CPU package's
+ * OutputPhaseImage (cpu_layout = 1: nX, nY, then the values x fastest, Dist.c:47-65) */
+int rte_write_phase_image(const char* path, int nx, int ny, const double* phase, int cpu_layout);
 int rte_read_image(const char* path, int nx, int ny, double* out);
 
 /* The CPU package's boundary outputs of a final distribution W (N*C complex, reference layout;
@@ -321,10 +336,10 @@ int rte_read_image(const char* path, int nx, int ny, double* out);
  * 353-532; x faces nZ*nY values at k + j*nZ, y faces nZ*nX at k + i*nZ; each pointer may be NULL) and
  * the photon number of ComputePhotonNumber (Dist.c:538-989: outgoing and "incoming" hemisphere sums
  * on all six faces plus the ballistic beam, with the package's 101 x 101 rectangle rule and its uniform
- * mu_t).  cfg gives the geometry, nL and c / n. */
+ * mu_t, whose imaginary part mu_t_im is the modulation's).  cfg gives the geometry, nL and c / n. */
 int rte_cpu_face_outputs(const rte_config* cfg, const rte_cplx* W, const rte_source* src, double mu_t,
-                         rte_cplx* side_x0, rte_cplx* side_x1, rte_cplx* side_y0, rte_cplx* side_y1,
-                         rte_cplx* photons);
+                         double mu_t_im, rte_cplx* side_x0, rte_cplx* side_x1, rte_cplx* side_y0,
+                         rte_cplx* side_y1, rte_cplx* photons);
 
 /* ---- allocation-free entry point (no counterpart in the reference) ------------------
  * For callers that must not allocate device memory when they run the solver: work recorded

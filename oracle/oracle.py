@@ -23,7 +23,7 @@ class OrcParams(ctypes.Structure):
                 ("x_min", ctypes.c_double), ("y_min", ctypes.c_double), ("z_min", ctypes.c_double),
                 ("L", ctypes.c_int), ("g", ctypes.c_double), ("cm", ctypes.c_double),
                 ("prop_thresh", ctypes.c_double), ("mode", ctypes.c_int), ("ssv", ctypes.c_int),
-                ("nthreads", ctypes.c_int)]
+                ("nthreads", ctypes.c_int), ("kappa", ctypes.c_double)]
 
 
 class OrcSource(ctypes.Structure):
@@ -65,13 +65,14 @@ def _dp(a):
 
 
 def params(nx, ny, nz, dx, dy, dz, L, g, cm, prop_thresh, mode=MODE_EXACT, ssv=1,
-           x_min=None, y_min=None, z_min=0.0, nthreads=0):
+           x_min=None, y_min=None, z_min=0.0, nthreads=0, kappa=0.0):
+    """kappa: imaginary part of mu_t under intensity modulation (modulation * n / c)."""
     if x_min is None:
         x_min = -nx * dx / 2.0
     if y_min is None:
         y_min = -ny * dy / 2.0
     return OrcParams(nx, ny, nz, dx, dy, dz, x_min, y_min, z_min, L, g, cm, prop_thresh, mode, ssv,
-                     nthreads)
+                     nthreads, kappa)
 
 
 def ncoef(L):

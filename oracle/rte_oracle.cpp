@@ -20,6 +20,10 @@
 //   mode 2  CPU   : CPU package (uniform medium): exact SH, exact attenuation,
 //                   200x200 self quadrature with per-axis half widths.
 //
+// Intensity modulation (CPU package/src/RTE_uniform.c:125-129: mu_a -> mu_a + i*modulation/(c/n))
+// enters as kappa, a uniform imaginary part of mu_t: pair attenuation exp(-(tau + i kappa r)), the
+// self-voxel factor (1 - exp(-mu_t beta)) / mu_t with complex mu_t, and complex ballistic terms.
+//
 // Citations are to files of the reference project (paths inside it).
 #include <cmath>
 #include <cstdint>
@@ -49,6 +53,7 @@ typedef struct {
   int mode;                    // 0 exact, 1 fim, 2 cpu
   int ssv;                     // self sub-voxels per axis (reference selfsubVox)
   int nthreads;                // OpenMP threads (0 = default)
+  double kappa;                // imaginary part of mu_t (intensity modulation; 0 = steady state)
 } orc_params;
 
 typedef struct {
@@ -217,12 +222,13 @@ static double mu_int(int si, int sj, int sk, int di, int dj, int dk, T r, const 
 // FisherInfo_IO/src/kernels.cu:175).
 struct SelfKey {
   int quad, L, ssv;
-  double mut, dx, dy, dz;
+  double mut, kappa, dx, dy, dz;
   bool operator<(const SelfKey& o) const {
     if (quad != o.quad) return quad < o.quad;
     if (L != o.L) return L < o.L;
     if (ssv != o.ssv) return ssv < o.ssv;
     if (mut != o.mut) return mut < o.mut;
+    if (kappa != o.kappa) return kappa < o.kappa;
     if (dx != o.dx) return dx < o.dx;
     if (dy != o.dy) return dy < o.dy;
     return dz < o.dz;
@@ -272,8 +278,9 @@ static void cube_exit(FT sx, FT sy, FT sz, float ii, float jj, float kk, int ssv
 }
 
 static const std::vector<cd>* self_matrix(int quad, int L, int ssv, double mut, double dx, double dy,
-                                          double dz) {
-  SelfKey key{quad, L, ssv, mut, dx, dy, dz};
+                                          double dz, double kappa = 0.0) {
+  SelfKey key{quad, L, ssv, mut, kappa, dx, dy, dz};
+  const cd muc(mut, kappa);
   {
     std::lock_guard<std::mutex> lk(g_self_mu);
     auto it = g_self.find(key);
@@ -290,7 +297,7 @@ static const std::vector<cd>* self_matrix(int quad, int L, int ssv, double mut, 
     }
   double dth = th[ang] - th[0], dph = ph[1] - ph[0];
   // weights per omega summed over sub-voxels: f(omega) = sum_sub (1-exp(-mut*beta)) sin(theta)
-  std::vector<double> f(nomega, 0.0);
+  std::vector<cd> f(nomega, 0.0);
   float cx = 0.0f, cy = 0.0f, cz = 0.0f;
   for (float ii = -ssv / 2.0 + 0.5; ii <= ssv / 2.0 - 0.5; ii++)
     for (float jj = -ssv / 2.0 + 0.5; jj <= ssv / 2.0 - 0.5; jj++)
@@ -309,13 +316,13 @@ static const std::vector<cd>* self_matrix(int quad, int L, int ssv, double mut, 
                         pow(jj * 2.0 / ssv - cy, 2.0) * pow(dy / 2.0, 2.0) +
                         pow(kk * 2.0 / ssv - cz, 2.0) * pow(dz / 2.0, 2.0));
           }
-          f[w] += (1 - exp(-mut * dist)) * sin(th[w]);
+          f[w] += (1.0 - std::exp(-muc * dist)) * sin(th[w]);
         }
   std::vector<cd> Y((size_t)nomega * C);
   for (int w = 0; w < nomega; w++) sph_harm_all(L, th[w], ph[w], &Y[(size_t)w * C]);
   std::vector<cd>* D = new std::vector<cd>((size_t)C * C, cd(0, 0));
   double dV = dx * dy * dz;
-  double denom = pow((double)ssv, 3) * mut * dV;
+  const cd denom = pow((double)ssv, 3) * muc * dV;
   for (int c = 0; c < C; c++)
     for (int cp = 0; cp < C; cp++) {
       cd s(0, 0);
@@ -354,7 +361,7 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
       if (p->mode == 1 && mut[r] == 0.0)
         selfm[mut[r]] = nullptr;  // tissue 0 gets no self term (dist.cu:430 loop starts at 1)
       else
-        selfm[mut[r]] = self_matrix(quad, p->L, p->ssv, mut[r], p->dx, p->dy, p->dz);
+        selfm[mut[r]] = self_matrix(quad, p->L, p->ssv, mut[r], p->dx, p->dy, p->dz, p->mode == 1 ? 0.0 : p->kappa);
     }
   const double cm = p->cm;
   const double dV = p->dx * p->dy * p->dz;
@@ -400,7 +407,8 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
           }
           cd S(0, 0);
           for (int cp = 0; cp < C; cp++) S = S + in[rp * Cfull + cp] * Y[cp];
-          double kern = exp(-tau) * (1.0 / (cm * dist * dist));
+          const double kappa = p->mode == 1 ? 0.0 : p->kappa;
+          const cd kern = std::exp(-cd(tau, kappa * dist)) * (1.0 / (cm * dist * dist));
           for (int c = 0; c < C; c++) acc[c] = acc[c] + S * std::conj(Y[c]) * kern;
         }
       }
@@ -497,8 +505,11 @@ int orc_apply(const orc_params* p, const double* mua, const double* mus, const d
 // kind 2: CPU package/src/Dist.c:1077-1128 (columns with |xy - pos| <= diam/2, attenuation
 //   from the absolute z coordinate, normalised by mag / number of columns; uniform medium).
 // kind 0: the column that contains (pos_x, pos_y), product form as kind 1, times mag.
+// With kappa != 0 the attenuation factors take the complex mu_t (the CPU package itself builds its
+// source before it modulates mu_a, RTE_uniform.c:127-129: pass kappa = 0 to reproduce that).
 int orc_source(const orc_params* p, const double* mua, const double* mus, const orc_source_t* s, double* Wd) {
   const int nx = p->nx, ny = p->ny, nz = p->nz, C = ncoef(p->L);
+  const double kap = p->mode == 1 ? 0.0 : p->kappa;
   cd* W = (cd*)Wd;
   size_t N = (size_t)nx * ny * nz;
   for (size_t q = 0; q < N * C; q++) W[q] = 0;
@@ -515,11 +526,11 @@ int orc_source(const orc_params* p, const double* mua, const double* mus, const 
           if (rad <= (s->diam + 1.0e-16) / 2.0) {
             total++;
             size_t r = ((size_t)i * ny + j) * nx + k;
-            double mt = mua[r] + mus[r];
+            const cd mt(mua[r] + mus[r], kap);
             double tz = zs - p->dz / 2.0;
             for (int l = 0; l <= p->L; l++)
               W[r * C + l * l + l] = pow(p->g, (double)l) * (mus[r] / mt) * sqrt(((2.0 * l) + 1.0) / (4.0 * M_PI)) *
-                                     (exp(-mt * tz) - exp(-mt * (tz + p->dz))) / dV;
+                                     (std::exp(-mt * tz) - std::exp(-mt * (tz + p->dz))) / dV;
           }
         }
     if (total == 0) return 0;
@@ -543,15 +554,15 @@ int orc_source(const orc_params* p, const double* mua, const double* mus, const 
   double scale = s->kind == 1 ? 1.0 : s->mag;
   for (int i = 0; i < nz; i++) {
     size_t r = ((size_t)i * ny + cy) * nx + cx;
-    double tmp = 1.0;
+    cd tmp = 1.0;
     for (int ip = 0; ip < i; ip++) {
       size_t rp = ((size_t)ip * ny + cy) * nx + cx;
-      tmp = tmp * exp(-(mus[rp] + mua[rp]) * p->dz);
+      tmp = tmp * std::exp(-cd(mus[rp] + mua[rp], kap) * p->dz);
     }
-    double mt = mus[r] + mua[r];
+    const cd mt(mus[r] + mua[r], kap);
     for (int l = 0; l <= p->L; l++)
       W[r * C + l * l + l] = scale * pow(p->g, l) * mus[r] / mt * sqrt(((2.0 * (double)l) + 1.0) / (4.0 * M_PI)) *
-                             tmp * (1 - exp(-mt * p->dz)) / dV;
+                             tmp * (1.0 - std::exp(-mt * p->dz)) / dV;
   }
   return 0;
 }
@@ -609,6 +620,7 @@ int orc_neumann(const orc_params* p, const double* mua, const double* mus, doubl
 int orc_images(const orc_params* p, const double* mua, const double* mus, const orc_source_t* s, int img_mode,
                int with_ballistic, const double* outd, double* transd, double* refd) {
   const int nx = p->nx, ny = p->ny, nz = p->nz, C = ncoef(p->L);
+  const double kap = img_mode == 1 ? 0.0 : p->kappa;  // ballistic with the complex mu_t
   const cd* out = (const cd*)outd;
   cd* trans = (cd*)transd;
   cd* ref = (cd*)refd;
@@ -699,18 +711,18 @@ int orc_images(const orc_params* p, const double* mua, const double* mus, const 
                   cols++;
               }
             double zs = (double)(nz - 1) * p->dz + p->z_min + p->dz / 2.0;
-            double mt = mua[rt] + mus[rt];
-            vt += (s->mag / cols) * exp(-mt * (zs + p->dz / 2.0));
+            const cd mt(mua[rt] + mus[rt], kap);
+            vt += (s->mag / cols) * std::exp(-mt * (zs + p->dz / 2.0));
           }
         } else {
           int cx = (int)floor((s->pos_x - p->x_min) / p->dx), cy = (int)floor((s->pos_y - p->y_min) / p->dy);
           cx = cx < 0 ? 0 : (cx >= nx ? nx - 1 : cx);
           cy = cy < 0 ? 0 : (cy >= ny ? ny - 1 : cy);
           if (k == cx && j == cy) {
-            double tmp = s->mag;
+            cd tmp = s->mag;
             for (int i = 0; i < nz; i++) {
               size_t r = ((size_t)i * ny + j) * nx + k;
-              tmp *= exp(-(mus[r] + mua[r]) * p->dz);
+              tmp *= std::exp(-cd(mus[r] + mua[r], kap) * p->dz);
             }
             vt += tmp;
           }

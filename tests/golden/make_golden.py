@@ -82,7 +82,8 @@ c = 1.0
 posX = 0
 posY = 0
 diam = {diam}
-magnitude = 1.0
+magnitude = {mag}
+modulation = {modulation}
 """
 
 
@@ -136,19 +137,33 @@ def read_img(path):
     return (v[: nx * ny] + 1j * v[nx * ny: 2 * nx * ny]).reshape(ny, nx)
 
 
-def cpu_case(name, n, nL, mua, mus, g, diam):
+def read_phase(path):
+    """The CPU package's phase image (OutputPhaseImage, Dist.c:47-65): nX, nY, then nX*nY doubles."""
+    b = open(path, "rb").read()
+    nx, ny = np.frombuffer(b[:8], np.int32)
+    return np.frombuffer(b[8:], np.float64)[: nx * ny].reshape(ny, nx)
+
+
+def cpu_case(name, n, nL, mua, mus, g, diam, modulation=0.0, mag=1.0):
     d = tempfile.mkdtemp(prefix="golden_")
-    par = CPU_PAR.format(nL=nL, n=n, lo=-n * 0.05, hi=n * 0.05, zmax=n * 0.1, mua=mua, mus=mus, g=g, diam=diam)
+    par = CPU_PAR.format(nL=nL, n=n, lo=-n * 0.05, hi=n * 0.05, zmax=n * 0.1, mua=mua, mus=mus, g=g, diam=diam,
+                         mag=mag, modulation=modulation)
     open(os.path.join(d, "c.par"), "w").write(par)
     log = run([os.path.join(ROOT, "oracle", "_ref", "rte_cpu"), "c.par"], d)
-    terms = int([l for l in log.splitlines() if l.startswith("Neumann series:")][-1].split()[-1]) - 1
+    # "Neumann series: n" after the steady-state loop (n = terms + 1), after the modulated loop and
+    # once more at the end (RTE_uniform.c:111, 159, 186)
+    counts = [int(l.split()[-1]) for l in log.splitlines() if l.startswith("Neumann series:")]
+    terms = counts[0] - 1
+    terms_mod = counts[1] - 1 if modulation != 0.0 else 0
     photons = float([l for l in log.splitlines() if l.startswith("Number of photons total")][-1].split()[-1])
     # the four side-face images, same file layout as the z-face images (Dist.c:353-532)
     side = {f"side{q}": read_img(os.path.join(d, f"SideFace{q}({ax}).out"))
             for q, ax in ((1, "-X"), (2, "+X"), (3, "-Y"), (4, "+Y"))}
     np.savez_compressed(os.path.join(HERE, name + ".npz"), n=n, nL=nL, mua=mua, mus=mus, g=g, diam=diam,
+                        mag=mag, modulation=modulation,
                         trans=read_img(os.path.join(d, "trans.out")), ref=read_img(os.path.join(d, "ref.out")),
-                        terms=terms, photons=photons, par=par, **side)
+                        phase=read_phase(os.path.join(d, "phase.out")), terms=terms, terms_mod=terms_mod,
+                        photons=photons, par=par, **side)
     print("wrote", name, "terms", terms)
 
 
@@ -162,6 +177,10 @@ def main():
     cpu_case("cpu_uniform_11_L3", 11, 3, 0.01, 1.0, 0.8, 0.1)
     # 5. the CPU package, isotropic scattering (g = 0: only l = 0 propagated), 9^3, L=2
     cpu_case("cpu_isotropic_9_L2", 9, 2, 0.05, 2.0, 0.0, 0.1)
+    # 6. intensity modulation (mu_a + i modulation/(c/n), RTE_uniform.c:120-176), 9^3, L=2
+    cpu_case("cpu_modulated_9_L2", 9, 2, 0.02, 1.5, 0.8, 0.1, modulation=0.5)
+    # 7. a beam over nine columns (the magnitude normalised per column, twice when modulated), L=3
+    cpu_case("cpu_modulated_wide_9_L3", 9, 3, 0.03, 1.2, 0.5, 0.35, modulation=1.0, mag=2.0)
 
 
 def fim_cases():

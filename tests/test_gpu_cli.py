@@ -148,10 +148,12 @@ def test_rte_inv_matches_oracle(rte, oracle, tmp_path):
     assert os.path.getsize(os.path.join(d, "Residual.out")) == 8
 
 
-@pytest.mark.parametrize("case", ["cpu_uniform_11_L3", "cpu_isotropic_9_L2"])
+@pytest.mark.parametrize("case", ["cpu_uniform_11_L3", "cpu_isotropic_9_L2", "cpu_modulated_9_L2",
+                                  "cpu_modulated_wide_9_L3"])
 def test_rte_gpu_on_cpu_package_files(rte, tmp_path, case):
-    """A CPU-package parameter file (uniform medium keys): same images, side-face files and printed
-    photon number as the CPU package itself."""
+    """A CPU-package parameter file (uniform medium keys): same images, phase image, side-face files and
+    printed photon number as the CPU package itself, with intensity modulation (its modulated
+    continuation and CombineOuts, RTE_uniform.c:120-196) and a beam over several columns."""
     g = np.load(os.path.join(GOLD, case + ".npz"))
     d = str(tmp_path)
     text = str(g["par"])
@@ -168,6 +170,12 @@ def test_rte_gpu_on_cpu_package_files(rte, tmp_path, case):
         assert rel(_read_img(os.path.join(d, f"SideFace{q}({ax}).out")), g[f"side{q}"]) < 1e-10
     ph = float(re.search(r"Number of photons total: (\S+)", r.stdout).group(1))
     assert abs(ph - float(g["photons"])) < 2e-6
+    b = open(os.path.join(d, "phase.out"), "rb").read()  # OutputPhaseImage: nX, nY, values x fastest
+    nx, ny = struct.unpack("2i", b[:8])
+    phase = np.frombuffer(b[8:], np.float64).reshape(ny, nx)
+    assert np.abs(phase - g["phase"]).max() < 1e-8
+    if float(g["modulation"]) != 0.0:
+        assert f"Neumann series (modulated): {int(g['terms_mod'])} terms" in r.stdout
 
 
 def test_rte_snr_matches_oracle(rte, oracle, tmp_path):
