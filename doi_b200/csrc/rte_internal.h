@@ -18,7 +18,7 @@ struct PairArgs {
   const double* mut;    // mu_t per voxel, FP64
   const float* mutf;    // mu_t per voxel, FP32
   const double* Win;    // current term, real basis, N x Cfull, FP64
-  const float* Winf;    // current term, FP32 copy
+  const float* Winf;    // current term, FP32 copy in slot order, coefficient c times N_c (sh_eval_monic)
   float* Kmat;          // stored pair kernel [source slot][destination slot], row stride Kld
   size_t Kld;
   double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
@@ -47,7 +47,7 @@ struct EpiArgs {
   int flag_scat;
   double scat[RTE_MAX_L + 1];  // per-l scatter factor (times mu_s of the voxel)
   double* Wout;         // FP64 result (may alias nothing else)
-  float* Woutf;         // FP32 copy in slot order, rows of cpad floats (may be null)
+  float* Woutf;         // FP32 copy in slot order (times N_c), rows of cpad floats (may be null)
   const int* islot;     // voxel -> slot
   int cpad, cstride;
   double* sum;          // running sum (null = do not accumulate)
@@ -229,7 +229,8 @@ cudaError_t rte_launch_to_cplx(const double* u1, const double* u2, double* cplx,
 cudaError_t rte_launch_layer_sums(const double* W, const double* S, int N, int nx, int ny, int nz, int Cfull,
                                   double* red, cudaStream_t st, int cplx = 0);
 cudaError_t rte_launch_f64_to_f32(const double* a, float* b, size_t n, cudaStream_t st);
-// FP64 [N][vstride] (voxel order) -> FP32 [slot][cpad] (slot order)
+// FP64 [N][vstride] (voxel order) -> FP32 [slot][cpad] (slot order), coefficient c scaled by the monic
+// SH normalisation N_c that the mixed pair kernels factor out of their per-pair recurrence
 cudaError_t rte_launch_to_f32_slots(const double* a, float* b, const int* islot, int N, int vstride, int cpad,
                                     int Cfull, int cstride, cudaStream_t st);
 }

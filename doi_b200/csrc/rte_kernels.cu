@@ -161,6 +161,79 @@ __device__ __forceinline__ void sh_eval(T x, T y, T z, T* R) {
   }
 }
 
+// Monic form of the same recurrence for the mixed pair kernel.  With q_l^m = s_lm u_l^m, s_mm = Q0[m]
+// and s_lm = A_lm s_{l-1,m}, the polynomials u satisfy u_l = z u_{l-1} - beta_lm u_{l-2} (beta_lm =
+// B_lm s_{l-2,m} / s_lm), so R_c = N_c U_c with U_{l,+-m} = u_l^m Re/Im((x+iy)^m) and N_c = s_lm.
+// The kernel carries U instead of R: the factors N_c are applied once per source row (the FP32 copy
+// of W holds N_c W_c) and once per destination (the partial sums), not per pair, and a recurrence
+// step costs two operations instead of three.
+struct MonicTab {
+  double beta[64];  // index l*(l+1)/2 + m
+  double N[64];     // index l*l + l + m
+};
+constexpr MonicTab make_monic() {
+  MonicTab t{};
+  const ShConstTab q = make_sh_const();
+  for (int m = 0; m <= RTE_MAX_L; ++m) {
+    double s[RTE_MAX_L + 1] = {};
+    s[m] = q.Q0[m];
+    for (int l = m + 1; l <= RTE_MAX_L; ++l) s[l] = q.A[l * (l + 1) / 2 + m] * s[l - 1];
+    for (int l = m; l <= RTE_MAX_L; ++l) {
+      if (l >= m + 2) t.beta[l * (l + 1) / 2 + m] = q.B[l * (l + 1) / 2 + m] * s[l - 2] / s[l];
+      t.N[l * l + l + m] = s[l];
+      t.N[l * l + l - m] = s[l];
+    }
+  }
+  return t;
+}
+__device__ constexpr MonicTab kMonic = make_monic();
+
+template <int L, typename T>
+__device__ __forceinline__ void sh_eval_monic(T x, T y, T z, T* U) {
+  T cmv = T(1), smv = T(0);
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if (m == 1) {
+      cmv = x;
+      smv = y;
+    } else if (m > 1) {
+      const T c2 = cmv * x - smv * y;
+      const T s2 = cmv * y + smv * x;
+      cmv = c2;
+      smv = s2;
+    }
+    T c1 = cmv, s1 = smv, c0 = T(0), s0 = T(0);
+    if (m == 0) {
+      U[0] = T(1);
+    } else {
+      U[m * m + 2 * m] = cmv;
+      U[m * m] = smv;
+    }
+#pragma unroll
+    for (int l = m + 1; l <= L; ++l) {
+      T cn, sn = T(0);
+      if (l == m + 1) {
+        cn = m == 0 ? z : z * c1;
+        if (m > 0) sn = z * s1;
+      } else {
+        const T b = (T)kMonic.beta[l * (l + 1) / 2 + m];
+        cn = fma(z, c1, -b * c0);
+        if (m > 0) sn = fma(z, s1, -b * s0);
+      }
+      c0 = c1;
+      c1 = cn;
+      s0 = s1;
+      s1 = sn;
+      if (m == 0) {
+        U[l * l + l] = cn;
+      } else {
+        U[l * l + l + m] = cn;
+        U[l * l + l - m] = sn;
+      }
+    }
+  }
+}
+
 // Direction snapped to the reference's 100x100 SH table cell (FisherInfo_IO/src/defines.h:53-56
 // and kernels.cu:326-333: theta = acos(dz/dist), phi = atan2(dy,dx) NOT wrapped to [0,2pi), so a
 // negative phi index reads the previous theta row of the flat table).
@@ -603,10 +676,10 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
                          ez = (double)(i - (int)q.z) * a.dz;
             double ux, uy, uz;
             table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
-            sh_eval<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
+            sh_eval_monic<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
           } else {
             const float inv = FLAT ? (d2 > 0.f ? rsqrtf(d2) : 0.f) : rsqrtf(d2);
-            sh_eval<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+            sh_eval_monic<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
           }
           if (!STORED) {
             int Q;
@@ -680,7 +753,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
 #pragma unroll
     for (int b = 0; b < NB; ++b)
 #pragma unroll
-      for (int c = 0; c < C; ++c) o[b * a.Cfull + c] = (double)sAcc[(b * C + c) * T + tid];
+      for (int c = 0; c < C; ++c) o[b * a.Cfull + c] = (double)sAcc[(b * C + c) * T + tid] * kMonic.N[c];
   }
 }
 
@@ -793,7 +866,8 @@ __global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
       for (int c = 0; c < a.Cfull; ++c) {
         const double x = c < C ? v[c] : 0.0;
         a.Wout[base + c] = x;
-        if (a.Woutf) a.Woutf[(size_t)a.islot[r] * a.cpad + (size_t)b * a.cstride + c] = (float)x;
+        // the mixed pair kernels read N_c W_c (monic SH, sh_eval_monic)
+        if (a.Woutf) a.Woutf[(size_t)a.islot[r] * a.cpad + (size_t)b * a.cstride + c] = (float)(x * kMonic.N[c]);
         w2 += x * x;
         double sv = 0.0;
         if (a.sum) {
@@ -1523,7 +1597,7 @@ __global__ void k_to_f32_slots(const double* a, float* b, const int* islot, int 
   if (t >= (long long)N * vstride) return;
   const int r = (int)(t / vstride), e = (int)(t % vstride);
   const int rhs = e / Cfull, c = e - rhs * Cfull;
-  b[(size_t)islot[r] * cpad + (size_t)rhs * cstride + c] = (float)a[t];
+  b[(size_t)islot[r] * cpad + (size_t)rhs * cstride + c] = (float)(a[t] * kMonic.N[c]);  // N_c W_c, see sh_eval_monic
 }
 
 __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
