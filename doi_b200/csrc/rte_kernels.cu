@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
       // stored kernel with exact SH: no per-pair branch (the diagonal and pairs beyond the coupling
       // distance carry k = 0), so two sources' SH recurrences can interleave
       constexpr bool FLAT = STORED && !TABLE;
-      constexpr int UNR = FLAT ? 2 : 1;
+      constexpr int UNR = FLAT ? 3 : 1;
 #pragma unroll UNR
       for (int sv = 0; sv < ns; ++sv) {
         float kk = 0.f;
