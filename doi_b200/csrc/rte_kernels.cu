@@ -564,12 +564,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// shared memory: [2][TS] float4 | [2][TS][cpad] float | [NB*C][T] float | 2 mbarriers
+// shared memory: [2][TS] float4 | [2][TS][cpad] float | [NB*C][T] float | 2 mbarriers (TS sources per tile)
 struct MixedLayout {
   size_t off_w, off_acc, off_bar, bytes;
-  __host__ __device__ MixedLayout(int cpad, int nbc) {
-    off_w = sizeof(float4) * 2 * RTE_PAIR_TS;
-    off_acc = off_w + sizeof(float) * 2 * RTE_PAIR_TS * (size_t)cpad;
+  __host__ __device__ MixedLayout(int cpad, int nbc, int ts = RTE_PAIR_TS) {
+    off_w = sizeof(float4) * 2 * ts;
+    off_acc = off_w + sizeof(float) * 2 * ts * (size_t)cpad;
     off_bar = (off_acc + sizeof(float) * (size_t)nbc * RTE_PAIR_THREADS + 15) / 16 * 16;
     bytes = off_bar + 2 * sizeof(uint64_t);
   }
@@ -580,9 +580,10 @@ struct MixedLayout {
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
   static_assert(!CPLX || NB == 2, "a complex right-hand side is a (real, imaginary) pair");
-  constexpr int C = (LA + 1) * (LA + 1), TS = RTE_PAIR_TS, T = RTE_PAIR_THREADS;
+  // 4 right-hand sides: 32-source tiles, so that two CTAs (their register limit) fit the shared memory
+  constexpr int C = (LA + 1) * (LA + 1), TS = NB == 4 ? 32 : RTE_PAIR_TS, T = RTE_PAIR_THREADS;
   const int CP = a.cpad;  // FP32 source row: nb * Cfull floats, padded to a multiple of 4
-  const MixedLayout Sh(CP, NB * C);
+  const MixedLayout Sh(CP, NB * C, TS);
   typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sP = reinterpret_cast<float4*>(smem_raw);
@@ -1609,7 +1610,7 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
-  const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1)).bytes;
+  const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1), NB == 4 ? 32 : RTE_PAIR_TS).bytes;
   void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
