@@ -580,8 +580,9 @@ struct MixedLayout {
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
   static_assert(!CPLX || NB == 2, "a complex right-hand side is a (real, imaginary) pair");
-  // 4 right-hand sides: 32-source tiles, so that two CTAs (their register limit) fit the shared memory
-  constexpr int C = (LA + 1) * (LA + 1), TS = NB == 4 ? 32 : RTE_PAIR_TS, T = RTE_PAIR_THREADS;
+  // wide rows (NB * C >= 128: 4 RHS at L = 5, 2 RHS at L = 7): 32-source tiles, so that two CTAs (their
+  // register limit) fit the shared memory
+  constexpr int C = (LA + 1) * (LA + 1), TS = NB * C >= 128 ? 32 : RTE_PAIR_TS, T = RTE_PAIR_THREADS;
   const int CP = a.cpad;  // FP32 source row: nb * Cfull floats, padded to a multiple of 4
   const MixedLayout Sh(CP, NB * C, TS);
   typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
@@ -1610,7 +1611,7 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
-  const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1), NB == 4 ? 32 : RTE_PAIR_TS).bytes;
+  const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1), NB * (LA + 1) * (LA + 1) >= 128 ? 32 : RTE_PAIR_TS).bytes;
   void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
