@@ -136,10 +136,11 @@ def test_neumann_reference_stop_rule_fim(rte, oracle):
     ctx.close()
 
 
-def test_forward_batch_matches_single(rte, oracle):
+@pytest.mark.parametrize("n,L", [(9, 3), (7, 5), (7, 7)])
+def test_forward_batch_matches_single(rte, oracle, n, L):
     """Four sources on one medium in one batched solve == four single solves (mixed precision), and
-    each within 1e-5 of the FP64 oracle."""
-    n, L = 9, 3
+    each within 1e-5 of the FP64 oracle; L = 5 and 7 take the 32-source-tile kernels of wide rows
+    (4 right-hand sides at L = 5, 2 and 4 at L = 7) and, at L = 7, the FP64 SH recurrence."""
     mua, mus, _ = rte.sphere_phantom(n, nspheres=2, seed=8, rmin=0.15, rmax=0.25)
     srcs = [rte.Source(pos_x=x, pos_y=y) for x, y in ((-0.2, -0.2), (0.2, -0.2), (-0.2, 0.2), (0.0, 0.0))]
     stop = rte.Stop(rte.STOP_FIXED, 12)
