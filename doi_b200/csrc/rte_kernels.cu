@@ -576,9 +576,11 @@ struct MixedLayout {
 };
 
 // CPLX (NB = 2): the two right-hand sides are the real and imaginary parts of one complex one and the
-// pair kernel carries the modulation phase exp(-i kappa |r - r'|).
+// pair kernel carries the modulation phase exp(-i kappa |r - r'|).  L = 7 with one right-hand side is
+// held to three CTAs per SM (168 registers): 33^3 launch 38.3 -> 33.9 ms (the same bound made L = 6
+// slower, so it applies to L = 7 alone).
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
-__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
+__global__ void __launch_bounds__(RTE_PAIR_THREADS, (LA == 7 && NB == 1) ? 3 : 1) k_pair_mixed(PairArgs a) {
   static_assert(!CPLX || NB == 2, "a complex right-hand side is a (real, imaginary) pair");
   // wide rows (NB * C >= 128: 4 RHS at L = 5, 2 RHS at L = 7): 32-source tiles, so that two CTAs (their
   // register limit) fit the shared memory
