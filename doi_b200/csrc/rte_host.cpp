@@ -1971,6 +1971,20 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   if (stop->rule == RTE_STOP_REFERENCE)
     return fail(c, RTE_ERR_UNSUPPORTED, "batched solves take a fixed or relative-L2 stop rule");
   const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  if (c->L >= 6 && nsrc > 2 && c->precision == RTE_PREC_MIXED) {
+    // four right-hand sides of 49-64 coefficients exceed the registers (spills): two batches of two
+    rte_report r1, r2;
+    int rc = rte_forward_batch(c, 2, srcs, stop, W_out, trans, ref, &r1);
+    if (!rc)
+      rc = rte_forward_batch(c, nsrc - 2, srcs + 2, stop, W_out ? W_out + 2 * NC : nullptr, trans ? trans + 2 * np : nullptr,
+                             ref ? ref + 2 * np : nullptr, &r2);
+    if (rc) return rc;
+    if (rep) {
+      *rep = r2;
+      rep->ms_device = r1.ms_device + r2.ms_device;
+    }
+    return RTE_OK;
+  }
   bool modulated = c->kappa != 0.0;
   for (int b = 0; b < nsrc; b++) modulated = modulated || srcs[b].modulation != 0.0;
   if (c->precision != RTE_PREC_MIXED || nsrc == 1 || modulated) {  // one source at a time
@@ -2616,6 +2630,19 @@ extern "C" int rte_forward_graph(rte_ctx* c, int nsrc, const rte_source* srcs, i
   if (c->kappa != 0.0) return unsupported_modulated(c, "graph replay");
   for (int b = 0; b < nsrc; b++)
     if (srcs[b].modulation != 0.0) return unsupported_modulated(c, "graph replay");
+  if (c->L >= 6 && nsrc > 2 && c->precision == RTE_PREC_MIXED) {  // as rte_forward_batch: two graphs of two
+    const size_t np = (size_t)c->nx * c->ny;
+    rte_report r1, r2;
+    int rc = rte_forward_graph(c, 2, srcs, nterms, trans, ref, &r1);
+    if (!rc) rc = rte_forward_graph(c, nsrc - 2, srcs + 2, nterms, trans ? trans + 2 * np : nullptr,
+                                    ref ? ref + 2 * np : nullptr, &r2);
+    if (rc) return rc;
+    if (rep) {
+      *rep = r2;
+      rep->ms_device = r1.ms_device + r2.ms_device;
+    }
+    return RTE_OK;
+  }
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   float ms = 0;
   int rc = forward_graph(c, nsrc, srcs, nterms, trans, ref, &ms);

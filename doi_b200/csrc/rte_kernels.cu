@@ -576,11 +576,11 @@ struct MixedLayout {
 };
 
 // CPLX (NB = 2): the two right-hand sides are the real and imaginary parts of one complex one and the
-// pair kernel carries the modulation phase exp(-i kappa |r - r'|).  L = 7 with one right-hand side is
-// held to three CTAs per SM (168 registers): 33^3 launch 38.3 -> 33.9 ms (the same bound made L = 6
-// slower, so it applies to L = 7 alone).
+// pair kernel carries the modulation phase exp(-i kappa |r - r'|).  L = 7 with one right-hand side runs
+// under a three-CTA register bound (168 registers, k_pair_mixed_3): 33^3 launch 38.3 -> 33.9 ms (the
+// same bound made L = 6 slower, so it applies to L = 7 alone).
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
-__global__ void __launch_bounds__(RTE_PAIR_THREADS, (LA == 7 && NB == 1) ? 3 : 1) k_pair_mixed(PairArgs a) {
+__device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
   static_assert(!CPLX || NB == 2, "a complex right-hand side is a (real, imaginary) pair");
   // wide rows (NB * C >= 128: 4 RHS at L = 5, 2 RHS at L = 7): 32-source tiles, so that two CTAs (their
   // register limit) fit the shared memory
@@ -759,6 +759,18 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS, (LA == 7 && NB == 1) ? 3 : 1
 #pragma unroll
       for (int c = 0; c < C; ++c) o[b * a.Cfull + c] = (double)sAcc[(b * C + c) * T + tid] * kMonic.N[c];
   }
+}
+
+// Launch wrappers.  k_pair_mixed_3 carries a 3-CTA register bound and is used for L = 7 with one
+// right-hand side only; an explicit minimum-block count on the others makes ptxas take more registers
+// (L = 5, 2 RHS: 218 instead of 164, two CTAs per SM instead of three, 13.2 -> 17.0 ms per launch).
+template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed(PairArgs a) {
+  pair_mixed_body<LA, TABLE, STORED, NB, CPLX>(a);
+}
+template <int LA, bool TABLE, bool STORED, int NB, bool CPLX>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS, 3) k_pair_mixed_3(PairArgs a) {
+  pair_mixed_body<LA, TABLE, STORED, NB, CPLX>(a);
 }
 
 // Pair-kernel precompute K[s][d] = exp(-tau) dV/(cm |r_d - r_s|^2) over destination slots d and
@@ -1614,7 +1626,11 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
   const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1), NB * (LA + 1) * (LA + 1) >= 128 ? 32 : RTE_PAIR_TS).bytes;
-  void (*kern)(PairArgs) = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
+  void (*kern)(PairArgs);
+  if constexpr (LA == 7 && NB == 1)
+    kern = k_pair_mixed_3<LA, TABLE, STORED, NB, CPLX>;
+  else
+    kern = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
