@@ -1354,13 +1354,24 @@ extern "C" int rte_set_modulation(rte_ctx* c, double modulation) {
     const size_t npix = 2 * ((size_t)c->nx * c->ny + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
     CUDA_TRY(c, dalloc(c, &c->d_fball_im, npix));
   }
-  const bool changed = kappa != c->kappa;
+  if (kappa == c->kappa) {
+    c->modulation = modulation;
+    return RTE_OK;
+  }
+  const double old_mod = c->modulation, old_kappa = c->kappa;
   c->modulation = modulation;
   c->kappa = kappa;
-  if (changed && c->medium_set) {
+  if (c->medium_set) {
     int rc = ensure_moments(c, std::hypot(c->mumax, c->kappa));
     if (!rc) rc = build_self_lut(c);
-    if (rc) return rc;
+    if (rc) {  // keep the context consistent: back to the previous modulation and its self-term table
+      const std::string msg = c->err;
+      c->modulation = old_mod;
+      c->kappa = old_kappa;
+      if (build_self_lut(c) != RTE_OK) c->medium_set = false;
+      c->err = msg;
+      return rc;
+    }
   }
   return RTE_OK;
 }

@@ -163,6 +163,9 @@ def test_modulation_back_to_zero_and_limits(rte):
         ctx.gradient([src], stop, rte.Detector(4, 63), np.zeros((1, 6, 4, 4)))
     with pytest.raises(rte.RteError):
         ctx.forward_graph([src], 4)
+    with pytest.raises(rte.RteError):  # |mu_t + i kappa| beyond the self-term series: refused, state kept
+        ctx.set_modulation(1e5)
+    assert rel(ctx.forward(src, stop)["W"], a["W"]) < 1e-14
     ctx.close()
     fim = rte.Context(8, 8, 8, dx=DX, nL=2, model=rte.MODEL_FIM, precision=0)
     with pytest.raises(rte.RteError):
