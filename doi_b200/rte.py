@@ -614,6 +614,15 @@ def write_image(path, img, cpu_layout=False):
         raise RteError(f"rte_write_image failed ({rc})")
 
 
+def write_phase_image(path, phase, cpu_layout=False):
+    """Phase image: FisherInfo_IO layout (nY, nX header) or the CPU package's (nX, nY header)."""
+    phase = np.ascontiguousarray(phase, np.float64)
+    ny, nx = phase.shape
+    rc = load_library().rte_write_phase_image(os.fsencode(path), nx, ny, _ptr(phase), int(bool(cpu_layout)))
+    if rc != 0:
+        raise RteError(f"rte_write_phase_image failed ({rc})")
+
+
 def read_image(path, nx, ny):
     out = np.zeros(nx * ny)
     rc = load_library().rte_read_image(os.fsencode(path), nx, ny, _ptr(out))

@@ -132,12 +132,14 @@ n = 1.0
 diam = 0.1
 Kind = point
 Face = 3
+modulation = 0.25
 """
     pr = rte.rte.ParFile(_write(tmp_path, "c.par", text)).problem()
     assert pr["style"] == 1 and pr["model"] == rte.MODEL_CPU and pr["c"] == 2.9979e10
     assert pr["x_min"] == -0.55 and pr["self_sub_vox"] == 1 and pr["precision"] == rte.PREC_MIXED
     assert pr["stop"] == {"rule": rte.STOP_REL_L2, "max_terms": 30, "tol": 1e-7} and pr["detector_bins"] == 11
     assert pr["source"]["kind"] == rte.SRC_POINT and pr["source"]["face"] == 3
+    assert pr["source"]["modulation"] == 0.25
     assert (pr["tiss"] == 1).all() and list(pr["mua_tab"]) == [0.0, 0.01]
 
 
@@ -153,6 +155,12 @@ def test_image_files(rte, tmp_path):
         assert np.array_equal(v[:24], img.real.ravel()) and np.array_equal(v[24:], img.imag.ravel())
     g = rte.rte.read_image(str(tmp_path / "i0.out"), 6, 4)  # a measured image: the real plane
     assert np.array_equal(g, img.real)
+    for cpu in (False, True):  # phase images: dist.cu:291-314 (nY, nX) and Dist.c:47-65 (nX, nY)
+        p = str(tmp_path / f"p{int(cpu)}.out")
+        rte.rte.write_phase_image(p, img.real, cpu_layout=cpu)
+        b = open(p, "rb").read()
+        assert struct.unpack("2i", b[:8]) == ((6, 4) if cpu else (4, 6)) and len(b) == 8 + 24 * 8
+        assert np.array_equal(np.frombuffer(b[8:], np.float64), img.real.ravel())
 
 
 def test_cli_usage_without_device(rte):
