@@ -337,4 +337,26 @@ int rte_read_image(const char* path, int nx, int ny, double* out) {
   return ok ? RTE_OK : RTE_ERR_IO;
 }
 
+// FisherInfo_IO/src/dist.cu:271-289 (downsample_image): sums of ds x ds pixel blocks.  The index
+// arithmetic is the reference's: output (i, j), i < nX/ds, j < nY/ds, is out[i*(nY/ds) + j] and adds
+// img[(i*ds + a)*nY + j*ds + b] for a, b < ds; on the square images the callers pass this is the block
+// sum of the y*nX + x image layout.  The reference accumulates into an uninitialised malloc block; the
+// sums here start at zero.  Rows and columns beyond the last whole block are dropped, as there.
+int rte_downsample_image(const rte_cplx* img, int nx, int ny, int ds, rte_cplx* out) {
+  if (!img || !out || nx < 1 || ny < 1 || ds < 1 || ds > nx || ds > ny) return RTE_ERR_ARG;
+  const int mx = nx / ds, my = ny / ds;
+  for (int i = 0; i < mx; i++)
+    for (int j = 0; j < my; j++) {
+      double re = 0.0, im = 0.0;
+      for (int a = 0; a < ds; a++)
+        for (int b = 0; b < ds; b++) {
+          const rte_cplx& v = img[(size_t)(i * ds + a) * ny + (size_t)j * ds + b];
+          re += v.re;
+          im += v.im;
+        }
+      out[(size_t)i * my + j] = rte_cplx{re, im};
+    }
+  return RTE_OK;
+}
+
 }  // extern "C"

@@ -34,7 +34,7 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
            "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
            "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
-           "rte_cpu_face_outputs", "rte_set_modulation")
+           "rte_cpu_face_outputs", "rte_set_modulation", "rte_downsample_image")
 
 
 class RteError(RuntimeError):
@@ -210,6 +210,7 @@ def load_library():
     L.rte_write_phase_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
     L.rte_set_modulation.argtypes = [P, ctypes.c_double]
     L.rte_read_image.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, dp]
+    L.rte_downsample_image.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
     L.rte_region_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, ctypes.c_int,
                                       ctypes.c_int, dp, dp, dp, dp, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(ctypes.c_double)]
@@ -629,6 +630,20 @@ def read_image(path, nx, ny):
     if rc != 0:
         raise RteError(f"rte_read_image failed ({rc})")
     return out.reshape(ny, nx)
+
+
+def downsample_image(img, ds):
+    """Block sums of an nY x nX image (the reference's downsample_image, FisherInfo_IO/src/dist.cu:271-289):
+    returns an (nX//ds) x (nY//ds) complex array; rows/columns beyond the last whole block are dropped."""
+    img = np.ascontiguousarray(img, np.complex128)
+    ny, nx = img.shape
+    if ds < 1 or ds > nx or ds > ny:
+        raise RteError(f"rte_downsample_image: bad factor {ds} for a {nx} x {ny} image")
+    out = np.zeros((nx // ds, ny // ds), np.complex128)
+    rc = load_library().rte_downsample_image(_ptr(img), nx, ny, int(ds), _ptr(out))
+    if rc != 0:
+        raise RteError(f"rte_downsample_image failed ({rc})")
+    return out
 
 
 def cpu_face_outputs(W, nx, ny, nz, nL, x_min, x_max, y_min, y_max, z_min, z_max, src, mu_t, c=1.0, n=1.0):

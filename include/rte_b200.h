@@ -330,6 +330,11 @@ int rte_write_image(const char* path, int nx, int ny, const rte_cplx* img, int c
  * OutputPhaseImage (cpu_layout = 1: nX, nY, then the values x fastest, Dist.c:47-65) */
 int rte_write_phase_image(const char* path, int nx, int ny, const double* phase, int cpu_layout);
 int rte_read_image(const char* path, int nx, int ny, double* out);
+/* Detector downsampling of an nX x nY image by ds (replaces downsample_image,
+ * FisherInfo_IO/src/dist.cu:271-289): out[i*(nY/ds) + j] = sum over a, b < ds of
+ * img[(i*ds + a)*nY + j*ds + b], i < nX/ds, j < nY/ds; the caller provides (nX/ds)*(nY/ds) values.
+ * Sums start at zero (the reference's start from uninitialised memory).  Host-only. */
+int rte_downsample_image(const rte_cplx* img, int nx, int ny, int ds, rte_cplx* out);
 
 /* The CPU package's boundary outputs of a final distribution W (N*C complex, reference layout;
  * host code, no context): the side-face images of ComputeSideFaceImages (CPU package/src/Dist.c:

@@ -167,3 +167,19 @@ def self_matrix(quad, L, ssv, mut, dx, dy, dz):
     out = np.zeros((C, C), np.complex128)
     lib().orc_self_matrix(quad, L, ssv, mut, dx, dy, dz, _dp(out.view(np.float64)))
     return out
+
+
+def downsample_image(img, nx, ny, ds):
+    """Pure-Python restatement of downsample_image (FisherInfo_IO/src/dist.cu:271-289) on a flat
+    nX*nY image: out[i*(nY//ds) + j] += img[(i*ds + a)*nY + j*ds + b], loops in the reference's
+    order (i, j, a, b), sums from zero (the reference's malloc block is not cleared).  Returns the
+    (nX//ds)*(nY//ds) values the reference's loops write."""
+    img = np.asarray(img, np.complex128).ravel()
+    mx, my = nx // ds, ny // ds
+    out = [0j] * (nx * ny // (ds * ds))
+    for i in range(mx):
+        for j in range(my):
+            for a in range(ds):
+                for b in range(ds):
+                    out[i * my + j] += img[(i * ds + a) * ny + j * ds + b]
+    return np.array(out[:mx * my], np.complex128)

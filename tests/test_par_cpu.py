@@ -163,6 +163,32 @@ def test_image_files(rte, tmp_path):
         assert np.array_equal(np.frombuffer(b[8:], np.float64), img.real.ravel())
 
 
+@pytest.mark.parametrize("nx,ny,ds", [(20, 20, 2), (20, 20, 5), (21, 21, 4), (12, 18, 3), (7, 9, 1), (5, 5, 5)])
+def test_downsample_image(rte, oracle, nx, ny, ds):
+    """downsample_image (FisherInfo_IO/src/dist.cu:271-289) through the C ABI: bit-exact against the
+    oracle's loop restatement, including the reference's row-length-nY indexing on non-square images
+    and the dropped ragged edge; on square images whose side ds divides, the block sums keep the total."""
+    rng = np.random.default_rng(nx * 100 + ny * 10 + ds)
+    img = rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx))
+    got = rte.downsample_image(img, ds)
+    ref = oracle.downsample_image(img, nx, ny, ds)
+    assert got.shape == (nx // ds, ny // ds)
+    assert np.array_equal(got.ravel(), ref)
+    if nx == ny and nx % ds == 0:
+        blocks = img.reshape(ny // ds, ds, nx // ds, ds).sum(axis=(1, 3))
+        assert np.allclose(got, blocks, rtol=1e-13, atol=1e-13)
+        assert abs(got.sum() - img.sum()) < 1e-11
+    if ds == 1:
+        assert np.array_equal(got.ravel(), img.ravel())
+
+
+def test_downsample_image_rejects_bad_factor(rte):
+    img = np.ones((4, 6), np.complex128)
+    for ds in (0, -1, 5, 7):
+        with pytest.raises(rte.RteError):
+            rte.downsample_image(img, ds)
+
+
 def test_cli_usage_without_device(rte):
     import subprocess
     exe = os.path.join(os.path.dirname(rte.rte.LIB_PATH), "..", "bin", "rte_gpu")
