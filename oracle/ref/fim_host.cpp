@@ -18,6 +18,13 @@
 //       one prop_abs pass over all slabs (flag = all-L, flag_scat = scatter)
 //   fim_host diag <file.par> <out.bin>
 //       the self-voxel table diag_terms_host (MAX_TISS_NUM*MAX_NL^4 complex, dist.cu:362-533)
+//   fim_host downsample <file.par> <in.bin> <ds> <out.bin>
+//       downsample_image (dist.cu:271-289) of an nX*nY complex image; writes the (nX/ds)*(nY/ds)
+//       values its loops assign.  The function sums into a fresh malloc block without clearing it,
+//       so the allocator is told to hand out zero-filled blocks (M_PERTURB 0xff fills each block
+//       with 0xff ^ 0xff; run with GLIBC_TUNABLES=glibc.malloc.tcache_count=0 so that no block
+//       bypasses the fill), which makes its result the zero-started sum.
+#include <malloc.h>
 #include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -202,6 +209,22 @@ int main(int argc, char** argv) {
       start += tp.num_layers;
     }
     write_dist(argv[6], res.data(), ndist);
+    return 0;
+  }
+  if (!strcmp(argv[1], "downsample") && argc >= 6) {
+    const size_t np = (size_t)geom->nX * geom->nY;
+    std::vector<complex_double> img(np);
+    FILE* f = fopen(argv[3], "rb");
+    if (!f || fread(img.data(), sizeof(complex_double), np, f) != np) {
+      fprintf(stderr, "fim_host: cannot read %s\n", argv[3]);
+      return 2;
+    }
+    fclose(f);
+    const int ds = atoi(argv[4]);
+    if (ds < 1 || ds > geom->nX || ds > geom->nY) return 2;
+    mallopt(M_PERTURB, 0xff);
+    complex_double* res = downsample_image(img.data(), ds);
+    write_dist(argv[5], res, (size_t)(geom->nX / ds) * (geom->nY / ds));
     return 0;
   }
   fprintf(stderr, "fim_host: unknown command %s\n", argv[1]);

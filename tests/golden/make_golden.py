@@ -130,6 +130,33 @@ def fim_case(name, nx, ny, nz, nL, tiss, mua_t, mus_t, g=0.8, n=1.0, prop=10.0, 
     print("wrote", name, "terms", out["terms"])
 
 
+def fim_downsample_case(name, nx, ny, factors, seed):
+    """downsample_image (dist.cu:271-289) of a seeded complex nX x nY image, run by the reference's own
+    function inside fim_host (the geometry comes from a .par file, as there; the solver is not run).
+    tcache off, so that every block the function allocates gets the allocator's zero fill."""
+    d = tempfile.mkdtemp(prefix="golden_")
+    nz = 2
+    np.ones(nx * ny * nz, np.uint8).tofile(os.path.join(d, "tiss.bin"))
+    par = FIM_PAR.format(nL=0, nx=nx, ny=ny, nz=nz, xmin=-nx * 0.05, xmax=nx * 0.05, ymin=-ny * 0.05,
+                         ymax=ny * 0.05, zmax=nz * 0.1, prop=1.0, ntiss=1, tiss="tiss.bin",
+                         tissue_lines="TissAbs1 = 0.01\nTissSc1 = 1.0", g=0.8, n=1.0, mag=1.0)
+    open(os.path.join(d, "t.par"), "w").write(par)
+    rng = np.random.default_rng(seed)
+    img = rng.standard_normal(nx * ny) + 1j * rng.standard_normal(nx * ny)
+    img.tofile(os.path.join(d, "img.bin"))
+    exe = os.path.join(ROOT, "oracle", "_ref", "fim_host")
+    env = dict(os.environ, GLIBC_TUNABLES="glibc.malloc.tcache_count=0")
+    out = dict(nx=nx, ny=ny, img=img, factors=np.array(factors), seed=seed)
+    for ds in factors:
+        r = subprocess.run([exe, "downsample", "t.par", "img.bin", str(ds), f"ds{ds}.bin"], cwd=d, env=env,
+                           stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"fim_host downsample {ds} failed:\n{r.stdout[-2000:]}")
+        out[f"ds{ds}"] = np.fromfile(os.path.join(d, f"ds{ds}.bin"), np.complex128)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name)
+
+
 def read_img(path):
     b = open(path, "rb").read()
     nx, ny = np.frombuffer(b[:8], np.int32)
@@ -199,6 +226,9 @@ def fim_cases():
     # 3. the shipped non-uniform 20^3 tissue map, L=1
     shipped = np.fromfile(os.path.join(REF, "GPU package", "utility", "tiss_map_nonuni.bin"), np.uint8)
     fim_case("fim_shipped_nonuni_20_L1", 20, 20, 20, 1, shipped, [0.0, 0.01, 0.02, 0.03], [0.0, 1.0, 1.2, 0.8])
+    # 4. downsample_image on a square and on a non-square image (its rows are nY long), ragged factors
+    fim_downsample_case("fim_downsample_20x20", 20, 20, [1, 2, 3, 4, 5, 7], 31)
+    fim_downsample_case("fim_downsample_24x18", 24, 18, [2, 3, 4, 5], 32)
 
 
 if __name__ == "__main__":

@@ -6,6 +6,7 @@ the reference stop rule, the source, the self-voxel table and both exitance imag
 CPU fixtures: the CPU package (oracle/_ref/rte_cpu) images and term count; oracle CPU mode.
 Modulated CPU fixtures pin the oracle's complex mu_t (kappa): the package's whole modulated main
 (RTE_uniform.c:120-196) is restated on the oracle below and must reproduce every output file.
+Downsample fixtures: the reference's downsample_image (dist.cu:271-289) on seeded images.
 """
 import os
 
@@ -195,3 +196,17 @@ def test_cpu_package_main_with_modulation(rte, oracle, case):
     for q in range(4):
         assert rel(sides[q].ravel(), g[f"side{q + 1}"].ravel()) < 1e-12, q
     assert abs(ph.real - float(g["photons"])) < 5e-7
+
+
+@pytest.mark.parametrize("case", ["fim_downsample_20x20", "fim_downsample_24x18"])
+def test_fim_downsample_image(rte, oracle, case):
+    """downsample_image as the reference's own function computed it (run inside fim_host with the
+    allocator's zero fill), bit-exact: the oracle's loop restatement and the library's
+    rte_downsample_image, on a square and a non-square image and factors that leave a ragged edge."""
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    nx, ny, img = int(g["nx"]), int(g["ny"]), g["img"]
+    for ds in (int(v) for v in g["factors"]):
+        ref = g[f"ds{ds}"]
+        assert np.array_equal(oracle.downsample_image(img, nx, ny, ds), ref)
+        # the library takes the image as the (nY, nX) array of the y*nX + x layout
+        assert np.array_equal(rte.downsample_image(img.reshape(ny, nx), ds).ravel(), ref)
