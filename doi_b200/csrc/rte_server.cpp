@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -259,7 +260,10 @@ int rte_server_wait(rte_server* s, long long ticket, double timeout_s, rte_cplx*
   auto it = s->reqs.find(ticket);
   if (it == s->reqs.end()) return RTE_ERR_ARG;
   Req* r = it->second.get();
-  const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeout_s));
+  // negative or NaN: poll; +inf or beyond 1e8 s (about three years): 1e8 s, which keeps the
+  // deadline inside the clock's range
+  const double wait_s = std::isfinite(timeout_s) ? std::min(std::max(timeout_s, 0.0), 1e8) : (timeout_s > 0 ? 1e8 : 0.0);
+  const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(wait_s));
   if (!s->cv_done.wait_until(lk, deadline, [&] { return r->done; })) return RTE_ERR_TIMEOUT;
   if (info) {
     info->status = r->status;

@@ -268,8 +268,9 @@ typedef struct rte_server rte_server;
 /* hbm_budget_gb <= 0: 85% of the free memory; nworkers = requests in flight at most. */
 int rte_server_create(int device, double hbm_budget_gb, int nworkers, rte_server** out);
 int rte_server_submit(rte_server* srv, const rte_request* req, long long* ticket);
-/* Waits up to timeout_s; trans/ref get nsrc*n*n complex values.  Returns the request status
- * (RTE_ERR_TIMEOUT if it is still running).  A ticket can be waited for once. */
+/* Waits up to timeout_s (0, negative or NaN: poll; +inf or anything above 1e8 s: 1e8 s); trans/ref
+ * get nsrc*n*n complex values.  Returns the request status (RTE_ERR_TIMEOUT if it is still running,
+ * and the ticket stays valid).  A finished ticket can be waited for once. */
 int rte_server_wait(rte_server* srv, long long ticket, double timeout_s, rte_cplx* trans, rte_cplx* ref,
                     rte_result_info* info);
 int rte_server_cancel(rte_server* srv, long long ticket); /* only before it starts */
