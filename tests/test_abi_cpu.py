@@ -57,3 +57,38 @@ def test_noalloc_rejects_bad_arguments_without_device(rte):
     # too large for the built-in scratch: rejected before any device work
     assert f(128, 128, 128, 0.1, 0.1, 0.1, 7, 1.0, 1.0, 1, 1, 1, None) == 6
     assert b"scratch" in lib.rte_last_error(None)
+
+
+NULL_IS_ERROR = ["rte_set_medium_tissue", "rte_set_medium_voxel", "rte_set_medium_device", "rte_set_modulation",
+                 "rte_source_beam", "rte_prop_abs", "rte_neumann", "rte_images", "rte_forward",
+                 "rte_detector_flux", "rte_gradient", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
+                 "rte_forward_batch", "rte_forward_graph", "rte_server_submit", "rte_server_wait",
+                 "rte_server_cancel", "rte_server_stats", "rte_set_profiling", "rte_get_stats", "rte_par_load",
+                 "rte_par_problem", "rte_write_image", "rte_write_phase_image", "rte_read_image",
+                 "rte_downsample_image", "rte_cpu_face_outputs", "rte_server_create", "rte_attenuate_noalloc",
+                 "rte_measure_fma_peak"]
+NULL_IS_NOOP = ["rte_destroy", "rte_device_bytes", "rte_server_destroy", "rte_get_stream", "rte_par_free",
+                "rte_problem_free", "rte_last_error"]
+
+
+def test_null_arguments_give_status_codes(rte):
+    """Every entry point given null pointers (and zero sizes) returns an error status or does nothing;
+    none dereferences them.  Run in a child process so that a crash is a test failure."""
+    import subprocess
+    import sys
+    lib_path = rte.rte.LIB_PATH
+    code = f"""
+import ctypes
+lib = ctypes.CDLL({lib_path!r})
+for name in {NULL_IS_ERROR + NULL_IS_NOOP!r}:
+    f = getattr(lib, name)
+    f.restype = ctypes.c_longlong
+    print(name, f(*([None] * 12)))
+"""
+    r = subprocess.run([sys.executable, "-c", code], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stdout[-2000:]
+    got = dict(line.split() for line in r.stdout.split("\n") if line.strip())
+    for name in NULL_IS_ERROR:
+        assert int(got[name]) != 0, name
+    assert all(name in got for name in NULL_IS_NOOP)
