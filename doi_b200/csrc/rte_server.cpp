@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/rte_b200.h"
+#include "rte_internal.h"
 
 namespace {
 
@@ -39,6 +40,7 @@ struct Req {
   std::vector<rte_cplx> trans, ref;
   Clock::time_point t_submit, t_start, t_done;
   int status = RTE_OK;
+  std::string msg;  // why the request failed, handed to the waiting thread's rte_last_error(NULL)
   bool started = false, done = false, cancelled = false;
   double device_ms = 0.0;
 };
@@ -153,6 +155,10 @@ static void worker_main(rte_server* s) {
       for (auto it = s->pending.begin(); it != s->pending.end();) {
         Slot* q = admit(s, *it);
         if (q == (Slot*)1) {  // larger than the whole budget: it can never run
+          char m[160];
+          snprintf(m, sizeof m, "request needs %.2f GB of HBM, the server's budget is %.2f GB",
+                   estimate_bytes(key_of((*it)->rq), (*it)->rq.nsrc) / 1e9, s->budget / 1e9);
+          (*it)->msg = m;
           (*it)->status = RTE_ERR_NOMEM;
           (*it)->done = true;
           (*it)->t_done = Clock::now();
@@ -179,6 +185,7 @@ static void worker_main(rte_server* s) {
     lk.unlock();
     int rc = RTE_OK;
     if (!sl->ctx) sl->ctx = make_ctx(s, sl->key, &rc);
+    if (rc != RTE_OK) r->msg = rte_last_error(nullptr);  // rte_create's message (this thread's)
     if (rc == RTE_OK) rc = rte_set_medium_voxel(sl->ctx, r->mua.data(), r->mus.data());
     if (rc == RTE_OK) {
       rte_report rep;
@@ -190,6 +197,7 @@ static void worker_main(rte_server* s) {
     lk.lock();
     if (rc != RTE_OK && sl->ctx) {  // a failed context is not reused
       s->err = rte_last_error(sl->ctx);
+      r->msg = s->err;
       rte_destroy(sl->ctx);
       sl->ctx = nullptr;
     }
@@ -214,11 +222,18 @@ static void worker_main(rte_server* s) {
 extern "C" {
 
 int rte_server_create(int device, double hbm_budget_gb, int nworkers, rte_server** out) {
-  if (!out || nworkers < 1 || nworkers > 64) return RTE_ERR_ARG;
+  if (!out || nworkers < 1 || nworkers > 64) {
+    rte_set_global_error("rte_server_create: null output or nworkers outside 1..64");
+    return RTE_ERR_ARG;
+  }
   *out = nullptr;
-  if (cudaSetDevice(device) != cudaSuccess) return RTE_ERR_DEVICE;
+  cudaError_t e = cudaSetDevice(device);
   size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return RTE_ERR_DEVICE;
+  if (e == cudaSuccess) e = cudaMemGetInfo(&fr, &tot);
+  if (e != cudaSuccess) {
+    rte_set_global_error(cudaGetErrorString(e));
+    return RTE_ERR_DEVICE;
+  }
   rte_server* s = new rte_server;
   s->device = device;
   s->budget = hbm_budget_gb > 0 ? (size_t)(hbm_budget_gb * 1e9) : (size_t)(0.85 * (double)fr);
@@ -228,10 +243,15 @@ int rte_server_create(int device, double hbm_budget_gb, int nworkers, rte_server
 }
 
 int rte_server_submit(rte_server* s, const rte_request* rq, long long* ticket) {
-  if (!s || !rq || !ticket || !rq->mua || !rq->mus) return RTE_ERR_ARG;
-  if (rq->n < 2 || rq->n > 256 || rq->nL < 0 || rq->nL > 7 || rq->nsrc < 1 || rq->nsrc > 4 || rq->terms < 0 ||
-      !(rq->dx > 0))
+  if (!s || !rq || !ticket || !rq->mua || !rq->mus) {
+    rte_set_global_error("rte_server_submit: null argument");
     return RTE_ERR_ARG;
+  }
+  if (rq->n < 2 || rq->n > 256 || rq->nL < 0 || rq->nL > 7 || rq->nsrc < 1 || rq->nsrc > 4 || rq->terms < 0 ||
+      !(rq->dx > 0)) {
+    rte_set_global_error("rte_server_submit: n outside 2..256, nL outside 0..7, nsrc outside 1..4, terms < 0 or dx <= 0");
+    return RTE_ERR_ARG;
+  }
   std::unique_ptr<Req> r(new Req);
   r->rq = *rq;
   const size_t N = (size_t)rq->n * rq->n * rq->n;
@@ -273,6 +293,7 @@ int rte_server_wait(rte_server* s, long long ticket, double timeout_s, rte_cplx*
     info->service_ms = r->started ? std::chrono::duration<double, std::milli>(r->t_done - r->t_start).count() : 0.0;
     info->device_ms = r->device_ms;
   }
+  if (r->status != RTE_OK) rte_set_global_error(r->msg.empty() ? "request cancelled" : r->msg.c_str());
   if (r->status == RTE_OK) {
     if (trans) memcpy(trans, r->trans.data(), r->trans.size() * sizeof(rte_cplx));
     if (ref) memcpy(ref, r->ref.data(), r->ref.size() * sizeof(rte_cplx));

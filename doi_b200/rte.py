@@ -485,7 +485,7 @@ class Server:
         h = ctypes.c_void_p()
         rc = self.lib.rte_server_create(device, float(hbm_budget_gb), int(workers), ctypes.byref(h))
         if rc != 0:
-            raise RteError(f"rte_server_create failed ({rc})")
+            raise RteError(f"rte_server_create failed ({rc}): {self.lib.rte_last_error(None).decode()}")
         self.h = h
         self._shape = {}
 
@@ -505,7 +505,7 @@ class Server:
         t = ctypes.c_longlong(0)
         rc = self.lib.rte_server_submit(self.h, ctypes.byref(rq), ctypes.byref(t))
         if rc != 0:
-            raise RteError(f"rte_server_submit failed ({rc})")
+            raise RteError(f"rte_server_submit failed ({rc}): {self.lib.rte_last_error(None).decode()}")
         self._shape[t.value] = (len(srcs), n)
         return t.value
 
@@ -519,7 +519,7 @@ class Server:
             raise TimeoutError(f"request {ticket} still running")
         del self._shape[ticket]
         if rc != 0:
-            raise RteError(f"request {ticket} failed ({rc})")
+            raise RteError(f"request {ticket} failed ({rc}): {self.lib.rte_last_error(None).decode()}")
         return tr, rf, {k: getattr(info, k) for k, _ in _ResultInfo._fields_}
 
     def cancel(self, ticket):

@@ -265,7 +265,9 @@ typedef struct {
 
 typedef struct rte_server rte_server;
 
-/* hbm_budget_gb <= 0: 85% of the free memory; nworkers = requests in flight at most. */
+/* hbm_budget_gb <= 0: 85% of the free memory; nworkers = requests in flight at most.  A failed
+ * rte_server_create / rte_server_submit / rte_server_wait leaves its reason for rte_last_error(NULL)
+ * on the calling thread (for a failed request: the admission or context error that stopped it). */
 int rte_server_create(int device, double hbm_budget_gb, int nworkers, rte_server** out);
 int rte_server_submit(rte_server* srv, const rte_request* req, long long* ticket);
 /* Waits up to timeout_s (0, negative or NaN: poll; +inf or anything above 1e8 s: 1e8 s); trans/ref

@@ -92,3 +92,17 @@ for name in {NULL_IS_ERROR + NULL_IS_NOOP!r}:
     for name in NULL_IS_ERROR:
         assert int(got[name]) != 0, name
     assert all(name in got for name in NULL_IS_NOOP)
+
+
+def test_server_errors_carry_messages(rte):
+    """rte_server_create failures (bad worker count; no device here) leave a reason for
+    rte_last_error(NULL), which the Python mirror puts in its exception."""
+    import torch
+    with pytest.raises(rte.RteError) as e:
+        rte.Server(device=0, workers=0)
+    assert "nworkers" in str(e.value)
+    if not torch.cuda.is_available():
+        with pytest.raises(rte.RteError) as e:
+            rte.Server(device=0, workers=2)
+        msg = str(e.value).split("):", 1)[1].strip()
+        assert msg
