@@ -3,7 +3,8 @@
 SH orthonormality (the check in GPU package/src/dist.cu:545-672), the exact radiological path in a
 uniform medium and against an independent crossing-sort computation, the collimated source closed
 form (JOSAA GPU Eq. 23, dist.cu:66-101), g = 0 keeps only l = 0 after scatter (prop_scat_dev),
-linearity, and the Neumann series against a dense direct solve of (I - DA) x = xi on a tiny grid.
+linearity, the Neumann series against a dense direct solve of (I - DA) x = xi on a tiny grid, and
+photon conservation without absorption (ComputePhotonNumber).
 """
 import numpy as np
 import pytest
@@ -192,3 +193,24 @@ def test_exitance_weights_closed_form(oracle, l):
         m = (-1) ** (k + 1) * factorial(l - 2) / (2 ** l * factorial(k - 1) * factorial(k + 1))
     expect = 2 * np.pi * 0.1 * 0.1 * np.sqrt((2 * l + 1) / (4 * np.pi)) * m
     assert abs(tr[1, 1].real - expect) < 1e-15
+
+
+@pytest.mark.parametrize("L", [1, 3])
+def test_photon_number_without_absorption(rte, oracle, L):
+    """ComputePhotonNumber (CPU package/src/Dist.c:538-989, the library's rte_cpu_face_outputs) on the
+    oracle's converged CPU-package solve: with mu_a = 0 every photon of the unit beam leaves through
+    the faces, up to the discretisation error of the angular truncation and the face quadratures
+    (within 10 %); absorption lowers the count monotonically."""
+    n = 9
+    N, lo, hi = n ** 3, -0.45, 0.45
+    p = oracle.params(n, n, n, 0.1, 0.1, 0.1, L, 0.8, 1.0, 10.0, mode=oracle.MODE_CPU, x_min=lo, y_min=lo)
+    src = rte.Source(diam=0.1, kind=rte.SRC_CPU)
+    counts = []
+    for mua in (0.0, 0.01, 0.1, 0.5):
+        r = oracle.forward(p, np.full(N, mua), np.full(N, 1.0), src_kind=oracle.SRC_CPU, img_mode=2,
+                           stop_rule=oracle.STOP_REL_L2, max_terms=200, tol=1e-12, diam=0.1)
+        _, ph = rte.rte.cpu_face_outputs(r["out"], n, n, n, L, lo, hi, lo, hi, 0.0, n * 0.1, src, mua + 1.0)
+        assert abs(ph.imag) < 1e-12
+        counts.append(ph.real)
+    assert abs(counts[0] - 1.0) < 0.1
+    assert all(b < a for a, b in zip(counts, counts[1:]))
