@@ -226,7 +226,11 @@ def fim_cases():
     # 3. the shipped non-uniform 20^3 tissue map, L=1
     shipped = np.fromfile(os.path.join(REF, "GPU package", "utility", "tiss_map_nonuni.bin"), np.uint8)
     fim_case("fim_shipped_nonuni_20_L1", 20, 20, 20, 1, shipped, [0.0, 0.01, 0.02, 0.03], [0.0, 1.0, 1.2, 0.8])
-    # 4. downsample_image on a square and on a non-square image (its rows are nY long), ragged factors
+    # 4. two tissues at L = 4, the highest order the reference's diag_terms indexing allows (MAX_NL 5)
+    tiss4 = np.random.default_rng(77).integers(1, 3, 2000).astype(np.uint8)
+    fim_case("fim_tissues_10x10x20_L4", 10, 10, 20, 4, tiss4, [0.0, 0.02, 0.08], [0.0, 1.0, 2.0], g=0.8, prop=10.0,
+             apply_seed=4)
+    # 5. downsample_image on a square and on a non-square image (its rows are nY long), ragged factors
     fim_downsample_case("fim_downsample_20x20", 20, 20, [1, 2, 3, 4, 5, 7], 31)
     fim_downsample_case("fim_downsample_24x18", 24, 18, [2, 3, 4, 5], 32)
 

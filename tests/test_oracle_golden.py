@@ -16,7 +16,9 @@ import pytest
 from conftest import rel
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FIM_CASES = ["fim_uniform_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_shipped_nonuni_20_L1"]
+FIM_CASES = ["fim_uniform_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_shipped_nonuni_20_L1",
+             "fim_tissues_10x10x20_L4"]
+FIM_APPLY_CASES = [c for c in FIM_CASES if c != "fim_shipped_nonuni_20_L1"]
 CPU_CASES = ["cpu_uniform_11_L3", "cpu_isotropic_9_L2"]
 MOD_CASES = ["cpu_modulated_9_L2", "cpu_modulated_wide_9_L3"]
 
@@ -45,7 +47,7 @@ def test_fim_forward(oracle, case):
     assert rel(rf, g["ref"]) < 1e-12
 
 
-@pytest.mark.parametrize("case", FIM_CASES[:2])
+@pytest.mark.parametrize("case", FIM_APPLY_CASES)
 def test_fim_single_pass(oracle, case):
     """One prop_abs pass of the reference kernels on a random complex input."""
     g = np.load(os.path.join(GOLD, case + ".npz"))
