@@ -204,6 +204,8 @@ def main():
     cpu_case("cpu_uniform_11_L3", 11, 3, 0.01, 1.0, 0.8, 0.1)
     # 5. the CPU package, isotropic scattering (g = 0: only l = 0 propagated), 9^3, L=2
     cpu_case("cpu_isotropic_9_L2", 9, 2, 0.05, 2.0, 0.0, 0.1)
+    # 5b. the benchmark's order L = 5 on a 9^3 uniform medium
+    cpu_case("cpu_uniform_9_L5", 9, 5, 0.01, 1.0, 0.8, 0.1)
     # 6. intensity modulation (mu_a + i modulation/(c/n), RTE_uniform.c:120-176), 9^3, L=2
     cpu_case("cpu_modulated_9_L2", 9, 2, 0.02, 1.5, 0.8, 0.1, modulation=0.5)
     # 7. a beam over nine columns (the magnitude normalised per column, twice when modulated), L=3

@@ -19,7 +19,7 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FIM_CASES = ["fim_uniform_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_shipped_nonuni_20_L1",
              "fim_tissues_10x10x20_L4"]
 FIM_APPLY_CASES = [c for c in FIM_CASES if c != "fim_shipped_nonuni_20_L1"]
-CPU_CASES = ["cpu_uniform_11_L3", "cpu_isotropic_9_L2"]
+CPU_CASES = ["cpu_uniform_11_L3", "cpu_isotropic_9_L2", "cpu_uniform_9_L5"]
 MOD_CASES = ["cpu_modulated_9_L2", "cpu_modulated_wide_9_L3"]
 
 
