@@ -4,6 +4,9 @@
 #   oracle/liboracle.so        FP64 restatement (rte_oracle.cpp)
 #   oracle/_ref/rte_cpu        CPU package built from its own sources (link order fixed)
 #   oracle/_ref/fim_host       FisherInfo_IO forward path compiled as host C++ (fim_emu.h)
+#   oracle/_ref/fim_fisher     the same with the Fisher main (rte_fim.cu) as its "program"
+#   oracle/_ref/fim_snr        the same with the SNR main (rte_snr.cu) as its "program"
+#   oracle/_ref/fim_grad       the same with the region-gradient main (compute_grad_rte.cu)
 # The reference sources are compiled where they lie; nothing is copied into the repo.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -19,7 +22,7 @@ if [ ! -d "$REF" ]; then
 fi
 
 OUT="$HERE/_ref"
-mkdir -p "$OUT/cpu" "$OUT/fim"
+mkdir -p "$OUT/cpu" "$OUT/fim" "$OUT/main"
 
 # CPU package: its Makefile puts -lm before the objects, which modern ld rejects; build the
 # same objects with the same flags and link with the libraries last.
@@ -37,9 +40,16 @@ FLAGS=(-O2 -std=c++17 -fopenmp -w -x c++ -D__CUDACC__ -include "$HERE/ref/fim_em
 for f in dist sph_harm inits neumann iniparser dictionary; do
   "$CXX" "${FLAGS[@]}" -c "$FIM/$f.cu" -o "$OUT/fim/$f.o"
 done
-"$CXX" "${FLAGS[@]}" -Dmain=fim_rte_main -c "$FIM/rte.cu" -o "$OUT/fim/rte.o"
+# the mains, each with main renamed to fim_prog_main (fim_host's "program" command runs it)
+for f in rte rte_fim rte_snr compute_grad_rte; do
+  "$CXX" "${FLAGS[@]}" -Dmain=fim_prog_main -c "$FIM/$f.cu" -o "$OUT/main/$f.o"
+done
+rm -f "$OUT/fim/rte.o"
 sed -n '1,418p' "$FIM/kernels.cu" | "$CXX" "${FLAGS[@]}" -c - -o "$OUT/fim/kernels.o"
 "$CXX" -O2 -std=c++17 -fopenmp -w -D__CUDACC__ -include "$HERE/ref/fim_emu.h" -I "$HERE/ref/include" -I "$FIM" \
   -c "$HERE/ref/fim_host.cpp" -o "$OUT/fim/fim_host.o"
-"$CXX" -fopenmp -o "$OUT/fim_host" "$OUT"/fim/*.o -lpthread -lm
-echo "oracle/build.sh: built liboracle.so, _ref/rte_cpu, _ref/fim_host"
+"$CXX" -fopenmp -o "$OUT/fim_host" "$OUT"/fim/*.o "$OUT/main/rte.o" -lpthread -lm
+"$CXX" -fopenmp -o "$OUT/fim_fisher" "$OUT"/fim/*.o "$OUT/main/rte_fim.o" -lpthread -lm
+"$CXX" -fopenmp -o "$OUT/fim_snr" "$OUT"/fim/*.o "$OUT/main/rte_snr.o" -lpthread -lm
+"$CXX" -fopenmp -o "$OUT/fim_grad" "$OUT"/fim/*.o "$OUT/main/compute_grad_rte.o" -lpthread -lm
+echo "oracle/build.sh: built liboracle.so, _ref/rte_cpu, _ref/fim_host, _ref/fim_fisher, _ref/fim_snr, _ref/fim_grad"

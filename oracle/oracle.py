@@ -47,6 +47,8 @@ def lib():
         L.orc_source.argtypes = [P, dp, dp, S, dp]
         L.orc_neumann.argtypes = [P, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.orc_neumann_split.argtypes = [P, dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.orc_images.argtypes = [P, dp, dp, S, ctypes.c_int, ctypes.c_int, dp, dp, dp]
         L.orc_sh_complex.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
         L.orc_assoc_legendre.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int]
@@ -117,15 +119,20 @@ def source(p, mua, mus, pos_x=0.0, pos_y=0.0, diam=0.1, mag=1.0, kind=SRC_COLUMN
     return W
 
 
-def neumann(p, mua, mus, W, out, flag=1, stop_rule=STOP_FIXED, max_terms=20, tol=1e-7, n0=2):
-    """Neumann(W, out, flag) of the reference; returns (A*sum, last term, number of terms)."""
+def neumann(p, mua, mus, W, out, flag=1, stop_rule=STOP_FIXED, max_terms=20, tol=1e-7, n0=2, mut_self=None):
+    """Neumann(W, out, flag) of the reference; returns (A*sum, last term, number of terms).
+    mut_self: per-voxel mu_t of the self-voxel term when it differs from mua + mus (the path
+    integrals and the scatter keep mua, mus), as in the FisherInfo_IO mains whose device tissue
+    table goes stale (rte_snr.cu:239, rte_fim.cu:231, compute_grad_rte.cu:431)."""
     mua = np.ascontiguousarray(mua, np.float64).ravel()
     mus = np.ascontiguousarray(mus, np.float64).ravel()
     W = np.array(W, np.complex128, copy=True)
     out = np.array(out, np.complex128, copy=True)
     nt = ctypes.c_int(0)
-    lib().orc_neumann(ctypes.byref(p), _dp(mua), _dp(mus), _dp(W.view(np.float64)),
-                      _dp(out.view(np.float64)), flag, stop_rule, max_terms, tol, n0, ctypes.byref(nt))
+    ms = None if mut_self is None else np.ascontiguousarray(mut_self, np.float64).ravel()
+    lib().orc_neumann_split(ctypes.byref(p), _dp(mua), _dp(mus), None if ms is None else _dp(ms),
+                            _dp(W.view(np.float64)), _dp(out.view(np.float64)), flag, stop_rule, max_terms, tol, n0,
+                            ctypes.byref(nt))
     return out, W, nt.value
 
 

@@ -18,6 +18,11 @@
 //       one prop_abs pass over all slabs (flag = all-L, flag_scat = scatter)
 //   fim_host diag <file.par> <out.bin>
 //       the self-voxel table diag_terms_host (MAX_TISS_NUM*MAX_NL^4 complex, dist.cu:362-533)
+//   fim_host program <file.par>
+//       the reference main linked into this binary (rte.cu in fim_host, rte_fim.cu in fim_fisher,
+//       rte_snr.cu in fim_snr, compute_grad_rte.cu in fim_grad; oracle/build.sh renames each main
+//       to fim_prog_main), run as
+//       `<main> file.par`, so it reads the file and writes its outputs as the program does
 //   fim_host downsample <file.par> <in.bin> <ds> <out.bin>
 //       downsample_image (dist.cu:271-289) of an nX*nY complex image; writes the (nX/ds)*(nY/ds)
 //       values its loops assign.  The function sums into a fresh malloc block without clearing it,
@@ -145,7 +150,10 @@ static void setup(const char* par) {
   generate_diag_terms_host();
 }
 
+int fim_prog_main(int argc, char** argv);
+
 int main(int argc, char** argv) {
+  if (argc >= 3 && !strcmp(argv[1], "program")) return fim_prog_main(argc - 1, argv + 1);
   if (argc < 4) {
     fprintf(stderr, "usage: fim_host forward <par> <prefix> | apply <par> <in> <flag> <flag_scat> <out>\n");
     return 1;

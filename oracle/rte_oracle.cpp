@@ -343,8 +343,12 @@ static const std::vector<cd>* self_matrix(int quad, int L, int ssv, double mut, 
 // One application of the attenuation operator A (and optionally the scatter D).
 // FisherInfo_IO/src/kernels.cu: compute_diagonal_abs :151-178, compute_propabs :289-366,
 // scale_dist_dev :368-383, prop_scat_dev :385-418; host sequence prop_abs :704-808.
+// mut_self (nullable): mu_t of each voxel for the self-voxel term when it differs from the mu_t of the
+// path integrals (the FisherInfo_IO mains that change tissue values rebuild the self-term table from
+// the new values but never refresh the device table the kernels read, e.g. rte_snr.cu:239,
+// compute_grad_rte.cu:431: `populate_info_dev();` with its result dropped).
 static void apply_op(const orc_params* p, const double* mua, const double* mus, const cd* in, cd* out, int flag,
-                     int flag_scat, const int* dests = nullptr, long ndest = -1) {
+                     int flag_scat, const int* dests = nullptr, long ndest = -1, const double* mut_self = nullptr) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   const size_t N = (size_t)nx * ny * nz;
   const int Cfull = ncoef(p->L);
@@ -352,16 +356,17 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
   const int C = ncoef(Lact);
   std::vector<double> mut(N);
   for (size_t r = 0; r < N; r++) mut[r] = mua[r] + mus[r];
+  const double* mts = mut_self ? mut_self : mut.data();
   const ShTable* tab = p->mode == 1 ? get_table(p->L) : nullptr;
   const int quad = p->mode == 1 ? 0 : 1;
   // self matrices for every distinct mu_t (the reference keeps one per tissue type)
   std::map<double, const std::vector<cd>*> selfm;
   for (size_t r = 0; r < N; r++)
-    if (!selfm.count(mut[r])) {
-      if (p->mode == 1 && mut[r] == 0.0)
-        selfm[mut[r]] = nullptr;  // tissue 0 gets no self term (dist.cu:430 loop starts at 1)
+    if (!selfm.count(mts[r])) {
+      if (p->mode == 1 && mts[r] == 0.0)
+        selfm[mts[r]] = nullptr;  // tissue 0 gets no self term (dist.cu:430 loop starts at 1)
       else
-        selfm[mut[r]] = self_matrix(quad, p->L, p->ssv, mut[r], p->dx, p->dy, p->dz, p->mode == 1 ? 0.0 : p->kappa);
+        selfm[mts[r]] = self_matrix(quad, p->L, p->ssv, mts[r], p->dx, p->dy, p->dz, p->mode == 1 ? 0.0 : p->kappa);
     }
   const double cm = p->cm;
   const double dV = p->dx * p->dy * p->dz;
@@ -375,7 +380,7 @@ static void apply_op(const orc_params* p, const double* mua, const double* mus, 
     int i = (int)(r / ((size_t)nx * ny)), j = (int)((r / nx) % ny), k = (int)(r % nx);
     std::vector<cd> acc(Cfull, cd(0, 0)), Y(Cfull);
     // self voxel
-    const std::vector<cd>* D = selfm[mut[r]];
+    const std::vector<cd>* D = selfm[mts[r]];
     if (D) {
       for (int c = 0; c < C; c++) {
         cd s(0, 0);
@@ -571,8 +576,17 @@ int orc_source(const orc_params* p, const double* mua, const double* mus, const 
 // sum) are inputs, as in the reference; on return out = A * sum.  stop_rule 0: reference
 // lambda rule (n starts at n0); 1: exactly max_terms terms; 2: ||W_k||_2 < tol*||sum||_2 or
 // max_terms.  W is left holding the last term.
+int orc_neumann_split(const orc_params* p, const double* mua, const double* mus, const double* mut_self, double* Wd,
+                      double* outd, int flag, int stop_rule, int max_terms, double tol, int n0, int* nterms);
+
 int orc_neumann(const orc_params* p, const double* mua, const double* mus, double* Wd, double* outd, int flag,
                 int stop_rule, int max_terms, double tol, int n0, int* nterms) {
+  return orc_neumann_split(p, mua, mus, nullptr, Wd, outd, flag, stop_rule, max_terms, tol, n0, nterms);
+}
+
+// Neumann (neumann.cu:23-120) whose self-voxel term takes mut_self (nullable) instead of mua + mus.
+int orc_neumann_split(const orc_params* p, const double* mua, const double* mus, const double* mut_self, double* Wd,
+                      double* outd, int flag, int stop_rule, int max_terms, double tol, int n0, int* nterms) {
   const size_t N = (size_t)p->nx * p->ny * p->nz;
   const int C = ncoef(p->L);
   cd* W = (cd*)Wd;
@@ -591,7 +605,7 @@ int orc_neumann(const orc_params* p, const double* mua, const double* mus, doubl
         break;
       }
       n++;
-      apply_op(p, mua, mus, W, Wn.data(), flag_l, 1);
+      apply_op(p, mua, mus, W, Wn.data(), flag_l, 1, nullptr, -1, mut_self);
       double nw = 0, ns = 0;
       for (size_t q = 0; q < N * C; q++) {
         out[q] = Wn[q] + out[q];
@@ -603,7 +617,7 @@ int orc_neumann(const orc_params* p, const double* mua, const double* mus, doubl
       if (stop_rule == 2 && sqrt(nw) < tol * sqrt(ns)) break;
     }
   }
-  apply_op(p, mua, mus, out, tmp.data(), 1, 0);
+  apply_op(p, mua, mus, out, tmp.data(), 1, 0, nullptr, -1, mut_self);
   memcpy(out, tmp.data(), sizeof(cd) * N * C);
   if (nterms) *nterms = terms;
   return 0;

@@ -88,7 +88,8 @@ modulation = {modulation}
 
 
 def run(cmd, cwd):
-    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    # errors="replace": compute_grad_rte.cu:155 prints a FILE* with %s
+    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, errors="replace")
     if r.returncode != 0:
         raise RuntimeError(f"{cmd} failed:\n{r.stdout[-2000:]}")
     return r.stdout
@@ -155,6 +156,61 @@ def fim_downsample_case(name, nx, ny, factors, seed):
         out[f"ds{ds}"] = np.fromfile(os.path.join(d, f"ds{ds}.bin"), np.complex128)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print("wrote", name)
+
+
+def fim_program_case(name, base, exe_name, files=(), measured_scale=0.0, runtime_keys=""):
+    """Run one of the reference's FisherInfo_IO mains (rte_fim.cu in fim_fisher, rte_snr.cu in
+    fim_snr, compute_grad_rte.cu in fim_grad), compiled for the host, on the .par file and tissue map
+    of the fixture `base`.  The measured image (gFile) these mains read is the base fixture's
+    transmission image times measured_scale (0: zeros).  Stores the program's standard output and
+    the binary files it writes."""
+    g = np.load(os.path.join(HERE, base + ".npz"))
+    d = tempfile.mkdtemp(prefix="golden_")
+    nx, ny = int(g["nx"]), int(g["ny"])
+    g["tiss"].astype(np.uint8).tofile(os.path.join(d, "tiss.bin"))
+    meas = (g["trans"].real.reshape(ny, nx) * measured_scale).astype(np.float64)
+    with open(os.path.join(d, "g.out"), "wb") as f:
+        f.write(np.array([ny, nx], np.int32).tobytes() + meas.tobytes())
+    par = str(g["par"]).replace("[Runtime]", "[Runtime]\ngFile = g.out\n" + runtime_keys, 1)
+    open(os.path.join(d, "t.par"), "w").write(par)
+    stdout = run([os.path.join(ROOT, "oracle", "_ref", exe_name), "program", "t.par"], d)
+    out = dict(base=base, par=par, stdout=stdout, measured_scale=measured_scale)
+    for f in files:
+        out[f.replace(".", "_")] = np.fromfile(os.path.join(d, f), np.float64)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name)
+
+
+def fim_snr_first_depth(name, base):
+    """The reference's SNR main (rte_snr.cu) never leaves its first depth: its loop step
+    `loc_indz = loc_indz++` (rte_snr.cu:219) leaves the index unchanged as gcc, the host compiler,
+    evaluates it, so the program prints the SNR^2 of depth 2 again and again and never writes
+    snr_terms.dat.  Run it with line-buffered output until the first value is printed, then stop it,
+    and store that line."""
+    g = np.load(os.path.join(HERE, base + ".npz"))
+    d = tempfile.mkdtemp(prefix="golden_")
+    nx, ny = int(g["nx"]), int(g["ny"])
+    g["tiss"].astype(np.uint8).tofile(os.path.join(d, "tiss.bin"))
+    with open(os.path.join(d, "g.out"), "wb") as f:
+        f.write(np.array([ny, nx], np.int32).tobytes() + np.zeros(nx * ny).tobytes())
+    par = str(g["par"]).replace("[Runtime]", "[Runtime]\ngFile = g.out", 1)
+    open(os.path.join(d, "t.par"), "w").write(par)
+    exe = os.path.join(ROOT, "oracle", "_ref", "fim_snr")
+    proc = subprocess.Popen(["stdbuf", "-oL", exe, "program", "t.par"], cwd=d, stdout=subprocess.PIPE,
+                            stderr=subprocess.STDOUT, text=True)
+    line = None
+    try:
+        for ln in proc.stdout:
+            if "is snr_sq for" in ln:
+                line = ln.strip()
+                break
+    finally:
+        proc.kill()
+        proc.wait()
+    if line is None:
+        raise RuntimeError("fim_snr printed no SNR value")
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), base=base, par=par, first_line=line)
+    print("wrote", name, line)
 
 
 def read_img(path):
@@ -232,7 +288,12 @@ def fim_cases():
     tiss4 = np.random.default_rng(77).integers(1, 3, 2000).astype(np.uint8)
     fim_case("fim_tissues_10x10x20_L4", 10, 10, 20, 4, tiss4, [0.0, 0.02, 0.08], [0.0, 1.0, 2.0], g=0.8, prop=10.0,
              apply_seed=4)
-    # 5. downsample_image on a square and on a non-square image (its rows are nY long), ragged factors
+    # 5. the Fisher, SNR and region-gradient mains on the random-tissue case
+    fim_program_case("fim_fisher_main_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_fisher")
+    fim_snr_first_depth("fim_snr_main_10x10x20_L2", "fim_tissues_10x10x20_L2")
+    fim_program_case("fim_grad_main_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_grad", files=("Residual.out",),
+                     measured_scale=1.05, runtime_keys="numIterations = 1\n")
+    # 6. downsample_image on a square and on a non-square image (its rows are nY long), ragged factors
     fim_downsample_case("fim_downsample_20x20", 20, 20, [1, 2, 3, 4, 5, 7], 31)
     fim_downsample_case("fim_downsample_24x18", 24, 18, [2, 3, 4, 5], 32)
 

@@ -9,6 +9,7 @@ Modulated CPU fixtures pin the oracle's complex mu_t (kappa): the package's whol
 Downsample fixtures: the reference's downsample_image (dist.cu:271-289) on seeded images.
 """
 import os
+import re
 
 import numpy as np
 import pytest
@@ -212,3 +213,139 @@ def test_fim_downsample_image(rte, oracle, case):
         assert np.array_equal(oracle.downsample_image(img, nx, ny, ds), ref)
         # the library takes the image as the (nY, nX) array of the y*nX + x layout
         assert np.array_equal(rte.downsample_image(img.reshape(ny, nx), ds).ravel(), ref)
+
+
+def _fim_main_setup(oracle, g, mua_t, mus_t, tiss, stale=None):
+    """Forward solve of a FisherInfo_IO main on the oracle (FIM model, reference stop rule).
+    stale: the tissue tables (mua, mus) the device kernels still hold.  The SNR and gradient mains
+    change tissue values on the host and call populate_info_dev() without keeping its result
+    (rte_snr.cu:239, compute_grad_rte.cu:431), so the path integrals and the scatter read the .par
+    values while the source, the self-voxel table and the images use the new ones."""
+    p = _fim_params(oracle, g)
+    mua, mus = np.asarray(mua_t)[tiss], np.asarray(mus_t)[tiss]
+    src = oracle.source(p, mua, mus, kind=oracle.SRC_FIM)
+    if stale is None:
+        out, _, _ = oracle.neumann(p, mua, mus, src, src, 1, oracle.STOP_REFERENCE, n0=2)
+        return p, mua, mus, out, mua, mus
+    ka, ks = np.asarray(stale[0])[tiss], np.asarray(stale[1])[tiss]
+    out, _, _ = oracle.neumann(p, ka, ks, src, src, 1, oracle.STOP_REFERENCE, n0=2, mut_self=mua + mus)
+    return p, mua, mus, out, ka, ks
+
+
+def _fim_axes(g):
+    """The mains' voxel-centre coordinates: every axis built from the x extent
+    (rte_fim.cu:160-170, rte_snr.cu likewise)."""
+    nx, ny, nz = (int(g[k]) for k in ("nx", "ny", "nz"))
+    fov = nx * float(g["delX"])
+    X = np.arange(nx) * fov / nx - fov / 2 + fov / (2 * nx)
+    Y = np.arange(ny) * fov / ny - fov / 2 + fov / (2 * ny)
+    Z = np.arange(nz) * fov / nz + fov / (2 * nz)
+    return fov, X, Y, Z
+
+
+def test_fim_fisher_main(oracle):
+    """The reference's Fisher main (rte_fim.cu, run in fim_fisher) against its restatement on the oracle:
+    tissue map ignored (every voxel tissue 1, mu_a 0.01, mu_s 1), one region of radius fov/(2 nX)
+    (a float, squared in float) about (nX/2, nY/2, z index 1), tangent source -C mask(out), Poisson
+    F = sum dg^2 / g over the reflection image.  The main prints F with 7 significant digits."""
+    run = np.load(os.path.join(GOLD, "fim_fisher_main_10x10x20_L2.npz"))
+    g = np.load(os.path.join(GOLD, str(run["base"]) + ".npz"))
+    F_ref = float(re.search(r"(\S+) is fisher abs", str(run["stdout"])).group(1))
+    nx, ny, nz = (int(g[k]) for k in ("nx", "ny", "nz"))
+    tiss = np.ones(nx * ny * nz, np.int64)
+    p, mua, mus, out, _, _ = _fim_main_setup(oracle, g, [0.0, 0.01, 0.01, 0.01], [0.0, 1.0, 1.0, 1.0], tiss)
+    mag = float(g["mag"])
+    _, gref = oracle.images(p, mua, mus, out, 1, mag=mag)
+    fov, X, Y, Z = _fim_axes(g)
+    rad = np.float32(fov / (2 * nx))
+    d2 = (X[None, None, :] - X[nx // 2]) ** 2 + (Y[None, :, None] - Y[ny // 2]) ** 2 + (Z[:, None, None] - Z[1]) ** 2
+    mask = ~(d2 > float(rad * rad)).ravel()
+    src = np.where(mask[:, None], -out, 0)
+    o, _, _ = oracle.neumann(p, mua, mus, src, src, 1, oracle.STOP_REFERENCE, n0=2)
+    _, dref = oracle.images(p, mua, mus, o, 1, mag=mag, with_ballistic=0)
+    gr, dr = gref.real.ravel(), dref.real.ravel()
+    nzp = gr != 0
+    F = float(np.sum(dr[nzp] ** 2 / gr[nzp]))
+    assert abs(F - F_ref) <= 1e-6 * abs(F_ref), (F, F_ref)
+
+
+def test_fim_snr_main(oracle):
+    """The reference's SNR main (rte_snr.cu, run in fim_snr) against its restatement on the oracle at the
+    first lesion depth: a lesion (tissue 2, radius 3 fov/(2 nX) in float) at (nX/2, nY/2, z index 2),
+    mu_a 0.35 (signal present) or 0.25 (absent), mu_s 1, on the stale device tissue table;
+    SNR^2 = sum (g1 - g0)^2 / g0 over the reflection image, printed with 7 digits.  Two more quirks:
+    the z coordinate array is filled only below nX (rte_snr.cu:175-179; the rest read as 0 in this
+    run, which puts the deep part of the centre column inside the lesion), and the program never
+    reaches the next depth (its loop step `loc_indz = loc_indz++`, rte_snr.cu:219, leaves the index
+    unchanged under gcc)."""
+    run = np.load(os.path.join(GOLD, "fim_snr_main_10x10x20_L2.npz"))
+    g = np.load(os.path.join(GOLD, str(run["base"]) + ".npz"))
+    m = re.match(r"(\S+) is snr_sq for (\d+) as z index", str(run["first_line"]))
+    snr_ref, lz = float(m.group(1)), int(m.group(2))
+    assert lz == 2
+    nx, ny = int(g["nx"]), int(g["ny"])
+    fov, X, Y, Z = _fim_axes(g)
+    Z[nx:] = 0.0
+    rad = np.float32(3 * fov / (2 * nx))
+    mua_t, mus_t = np.array(g["mua_t"], float), np.array(g["mus_t"], float)
+    d2 = (X[None, None, :] - X[nx // 2]) ** 2 + (Y[None, :, None] - Y[ny // 2]) ** 2 + (Z[:, None, None] - Z[lz]) ** 2
+    tiss = np.where(d2 < float(rad * rad), 2, 1).ravel()
+    imgs = []
+    for hyp in (1, 0):
+        a, s = mua_t.copy(), mus_t.copy()
+        a[2], s[2] = 0.25 + 0.1 * hyp, 1.0
+        p, mua, mus, out, _, _ = _fim_main_setup(oracle, g, a, s, tiss, stale=(mua_t, mus_t))
+        imgs.append(oracle.images(p, mua, mus, out, 1, mag=float(g["mag"]))[1].real.ravel())
+    snr = float(np.sum((imgs[0] - imgs[1]) ** 2 / imgs[1]))
+    assert abs(snr - snr_ref) <= 1e-6 * abs(snr_ref), (snr, snr_ref)
+
+
+def test_fim_region_gradient_main(oracle):
+    """The reference's region-gradient main (compute_grad_rte.cu, run in fim_grad, one iteration) against
+    its restatement on the oracle: iteration 0 sets tissue 1 to mu_a 0.008, mu_s 0.8; per tissue a tangent
+    solve of -C mask(out) (mu_a) and of mask((g^l - 1) out) with the stale-index mask (mu_s) projected to
+    the transmission image without the ballistic term, all on the stale device tissue table (the
+    .par values; the source, the self-voxel table and the images take the new ones); grad1 = -2 av sum dg/(g - gbar), grad2 = -2 av
+    sum (g - gbar) dg over pixels with g or gbar non-zero (av 0.01 as a float for mu_a, 1 for mu_s);
+    Residual.out = sum log((gbar - g)^2).  Printed values carry 7 digits; Residual.out is binary."""
+    run = np.load(os.path.join(GOLD, "fim_grad_main_10x10x20_L2.npz"))
+    g = np.load(os.path.join(GOLD, str(run["base"]) + ".npz"))
+    text = str(run["stdout"])
+    got1 = [tuple(float(x) for x in m) for m in re.findall(r"mua grad1 = (\S+) musgrad1 = (\S+)", text)]
+    got2 = [tuple(float(x) for x in m) for m in re.findall(r"mua grad2 = (\S+) musgrad2 = (\S+)", text)]
+    nx, ny = int(g["nx"]), int(g["ny"])
+    meas = g["trans"].real.reshape(ny, nx) * float(run["measured_scale"])
+    mua_t, mus_t = np.array(g["mua_t"], float), np.array(g["mus_t"], float)
+    mua_t[1], mus_t[1] = 0.008, 0.8
+    tiss = g["tiss"].astype(np.int64)
+    p, mua, mus, out, ka, ks = _fim_main_setup(oracle, g, mua_t, mus_t, tiss,
+                                               stale=(np.array(g["mua_t"], float), np.array(g["mus_t"], float)))
+    mag = float(g["mag"])
+    gbar, _ = oracle.images(p, mua, mus, out, 1, mag=mag)
+    gb, gm = gbar.real.ravel(), meas.ravel()
+    use = (gm != 0) | (gb != 0)
+    L = int(g["nL"])
+    lof = np.array([int(np.floor(np.sqrt(c))) for c in range((L + 1) ** 2)])
+
+    def tangent(src):
+        o, _, _ = oracle.neumann(p, ka, ks, src, src, 1, oracle.STOP_REFERENCE, n0=2, mut_self=mua + mus)
+        return oracle.images(p, mua, mus, o, 1, mag=mag, with_ballistic=0)[0].real.ravel()
+
+    assert len(got1) == len(got2) == len(mua_t) - 1
+    for t in range(1, len(mua_t)):
+        m = tiss == t
+        dga = tangent(np.where(m[:, None], -out, 0))
+        resid = gm[use] - gb[use]
+        ga = float(np.sum(-2 * np.float32(0.01) * dga[use] / resid))
+        ga2 = float(np.sum(-2 * np.float32(0.01) * resid * dga[use]))
+        ms = np.ones_like(m)
+        if not m.all():
+            ms[-1] = False  # the stale-index mu_s mask (compute_grad_rte.cu:356-363)
+        dgs = tangent(np.where(ms[:, None], out * (-1.0 + float(g["g"]) ** lof)[None, :], 0))
+        gs = float(np.sum(-2 * dgs[use] / resid))
+        gs2 = float(np.sum(-2 * resid * dgs[use]))
+        for got, want in ((got1[t - 1][0], ga), (got1[t - 1][1], gs), (got2[t - 1][0], ga2), (got2[t - 1][1], gs2)):
+            assert abs(got - want) <= 1e-6 * abs(want), (t, got, want)
+    diff = gb - gm
+    res = float(np.sum(np.log(diff[diff != 0] ** 2)))
+    assert abs(run["Residual_out"][0] - res) <= 1e-12 * abs(res)
