@@ -181,6 +181,22 @@ def fim_program_case(name, base, exe_name, files=(), measured_scale=0.0, runtime
     print("wrote", name)
 
 
+def fim_forward_main_files(name, bases):
+    """The reference's forward main (rte.cu, run in fim_host) on each base fixture's .par file: the raw
+    bytes of the TransFile and ReflectFile it writes (dist.cu:316-345 layout)."""
+    out = {}
+    for base in bases:
+        g = np.load(os.path.join(HERE, base + ".npz"))
+        d = tempfile.mkdtemp(prefix="golden_")
+        g["tiss"].astype(np.uint8).tofile(os.path.join(d, "tiss.bin"))
+        open(os.path.join(d, "t.par"), "w").write(str(g["par"]))
+        run([os.path.join(ROOT, "oracle", "_ref", "fim_host"), "program", "t.par"], d)
+        for f, k in (("trans.out", "trans"), ("ref.out", "ref")):
+            out[f"{base}__{k}"] = np.frombuffer(open(os.path.join(d, f), "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name)
+
+
 def fim_snr_first_depth(name, base):
     """The reference's SNR main (rte_snr.cu) never leaves its first depth: its loop step
     `loc_indz = loc_indz++` (rte_snr.cu:219) leaves the index unchanged as gcc, the host compiler,
@@ -288,7 +304,10 @@ def fim_cases():
     tiss4 = np.random.default_rng(77).integers(1, 3, 2000).astype(np.uint8)
     fim_case("fim_tissues_10x10x20_L4", 10, 10, 20, 4, tiss4, [0.0, 0.02, 0.08], [0.0, 1.0, 2.0], g=0.8, prop=10.0,
              apply_seed=4)
-    # 5. the Fisher, SNR and region-gradient mains on the random-tissue case
+    # 5. the forward main itself (rte.cu): the image files it writes for the first three cases
+    fim_forward_main_files("fim_forward_main_files", ["fim_uniform_10x10x20_L2", "fim_tissues_10x10x20_L2",
+                                                      "fim_shipped_nonuni_20_L1"])
+    # 5b. the Fisher, SNR and region-gradient mains on the random-tissue case
     fim_program_case("fim_fisher_main_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_fisher")
     fim_snr_first_depth("fim_snr_main_10x10x20_L2", "fim_tissues_10x10x20_L2")
     fim_program_case("fim_grad_main_10x10x20_L2", "fim_tissues_10x10x20_L2", "fim_grad", files=("Residual.out",),

@@ -349,3 +349,23 @@ def test_fim_region_gradient_main(oracle):
     diff = gb - gm
     res = float(np.sum(np.log(diff[diff != 0] ** 2)))
     assert abs(run["Residual_out"][0] - res) <= 1e-12 * abs(res)
+
+
+@pytest.mark.parametrize("case", FIM_CASES[:3])
+def test_fim_forward_main_files(rte, tmp_path, case):
+    """The image files the reference's forward main (rte.cu, run in fim_host) writes for each case: the
+    fixture's images are exactly these (so the GPU program tests compare against the main's own
+    output), and rte_write_image produces the same bytes from them (header nY, nX, then the real and
+    the imaginary plane, dist.cu:316-345)."""
+    files = np.load(os.path.join(GOLD, "fim_forward_main_files.npz"))
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    nx, ny = int(g["nx"]), int(g["ny"])
+    for k in ("trans", "ref"):
+        raw = files[f"{case}__{k}"].tobytes()
+        assert np.frombuffer(raw[:8], np.int32).tolist() == [ny, nx]
+        v = np.frombuffer(raw[8:], np.float64)
+        assert v.size == 2 * nx * ny
+        assert np.array_equal(v[:nx * ny] + 1j * v[nx * ny:], g[k].ravel())
+        path = str(tmp_path / f"{k}.out")
+        rte.rte.write_image(path, g[k].reshape(ny, nx))
+        assert open(path, "rb").read() == raw
