@@ -141,8 +141,12 @@ def cpu_baseline(seconds=10.0, seed=0):
     solve_s = per_app * (TERMS + 1)
     cores = os.cpu_count()
     return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": f"operator D*A for {nd2} random destination voxels x all {N} sources of the 33^3 L=5 "
-                      f"phantom ({dt:.1f} s), extrapolated x{N / nd2:.0f} voxels x{TERMS + 1} applications",
+            "sample": f"operator D*A for {nd2} random destination voxels ({100.0 * nd2 / N:.1f} % of the {N}) x all "
+                      f"sources of the 33^3 L=5 phantom ({dt:.1f} s), extrapolated x{N / nd2:.0f} voxels x{TERMS + 1} "
+                      "applications",
+            "what": "the unoptimised FP64 oracle port (a restatement of the reference algorithm in the complex "
+                    "SH basis, OpenMP over destination voxels): a reported baseline, not a target; the reference "
+                    "has no CPU code for non-uniform media (the CPU package's own run is config1_plain_fp64)",
             "seconds_per_solve": solve_s}
 
 
@@ -196,54 +200,81 @@ def serve_requests(count, seed):
     return out
 
 
+def serve_stream(srv, reqs, gaps):
+    """Submit reqs (n, L, mua, mus, src) at the given inter-arrival gaps, wait for all; returns (wall s,
+    latencies ms, summed device ms)."""
+    t0 = time.perf_counter()
+    tickets, t_next = [], t0
+    for (n, Lq, mua, mus, src), gap in zip(reqs, gaps):
+        t_next += gap
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        tickets.append(srv.submit(mua, mus, [src], n, dx=DX, nL=Lq, g=0.8, terms=TERMS))
+    lat, dev_ms = [], 0.0
+    for t in tickets:
+        _, _, info = srv.wait(t, timeout=3600)
+        lat.append(info["latency_ms"])
+        dev_ms += info["device_ms"]
+    return time.perf_counter() - t0, np.array(lat), dev_ms
+
+
+def serve_measure(srv, reqs, rate, seed):
+    """Saturated capacity (every request submitted at once: completed / wall), then the same requests
+    with seeded Poisson arrivals at `rate` (0: 0.7 x the capacity) for p50 / p99 latency."""
+    wall_sat, _, _ = serve_stream(srv, reqs, np.zeros(len(reqs)))
+    capacity = len(reqs) / wall_sat
+    rate = rate if rate > 0 else 0.7 * capacity
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(reqs))
+    wall, lat, dev_ms = serve_stream(srv, reqs, gaps)
+    return {"requests": len(reqs), "capacity_solves_per_s": capacity, "saturated_wall_s": wall_sat,
+            "arrival_rate_per_s": rate, "solves_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "wall_s": wall,
+            "device_ms_sum": dev_ms}
+
+
 def run_serve(args, dev):
-    """Continuous-batching stream through rte_server_*.  Capacity: every request submitted at once,
-    completed requests / (first submit -> last completion).  Latency: Poisson arrivals at
-    --serve-rate (default 0.7 x the capacity just measured), submit -> completion, p50 / p99."""
+    """Continuous-batching streams through rte_server_*.  (1) BASELINE config 3's request mix (grids
+    {17,25,33,41}^3, orders {3,5,7}, 0-3 inclusions, beam or isotropic point on a random face); (2) the
+    benchmark's own shape: single-source 33^3 L=5 requests, each on a new 3-sphere phantom with a
+    collimated beam at a random z=0 position, the form the >= 5x target is stated for.  Each stream:
+    saturated capacity, then Poisson arrivals at 0.7 x capacity for p50 / p99 latency."""
     import doi_b200 as R
-    reqs = serve_requests(args.serve_requests, seed=17)
-
-    def stream(srv, gaps):
-        t0 = time.perf_counter()
-        tickets, t_next = [], t0
-        for (n, Lq, mua, mus, src), gap in zip(reqs, gaps):
-            t_next += gap
-            d = t_next - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            tickets.append(srv.submit(mua, mus, [src], n, dx=DX, nL=Lq, g=0.8, terms=TERMS))
-        lat, dev_ms = [], 0.0
-        for t in tickets:
-            _, _, info = srv.wait(t, timeout=3600)
-            lat.append(info["latency_ms"])
-            dev_ms += info["device_ms"]
-        return time.perf_counter() - t0, np.array(lat), dev_ms
-
+    from doi_b200.phantoms import sphere_phantom
+    mix = serve_requests(args.serve_requests, seed=17)
+    rng = np.random.default_rng(29)
+    bench_shape = []
+    for q in range(args.serve_requests_33):
+        mua, mus, _ = sphere_phantom(N_SIDE, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=3, seed=50000 + q)
+        a, b = rng.uniform(-N_SIDE * DX / 2, N_SIDE * DX / 2, 2)
+        bench_shape.append((N_SIDE, L, mua, mus, R.Source(pos_x=float(a), pos_y=float(b), kind=R.SRC_COLUMN)))
+    out = {}
     with R.Server(device=dev, workers=args.serve_workers) as srv:
         # one request of every shape first (context creation, self-term tables, graph capture) so the
-        # stream measures steady-state serving; these are not counted
+        # streams measure steady-state serving; these are not counted
         N0 = [(n, Lq) for n in SERVE_GRIDS for Lq in SERVE_ORDERS]
         warm = [srv.submit(np.full(n ** 3, 0.01), np.full(n ** 3, 1.0), [R.Source(kind=R.SRC_BEAM)], n, dx=DX,
                            nL=Lq, g=0.8, terms=TERMS) for n, Lq in N0]
         for t in warm:
             srv.wait(t, timeout=1800)
         st0 = srv.stats()
-        wall_sat, lat_sat, _ = stream(srv, np.zeros(len(reqs)))
-        capacity = len(reqs) / wall_sat
-        rate = args.serve_rate if args.serve_rate > 0 else 0.7 * capacity
-        gaps = np.random.default_rng(23).exponential(1.0 / rate, len(reqs))
-        wall, lat, dev_ms = stream(srv, gaps)
+        if mix:
+            out = serve_measure(srv, mix, args.serve_rate, 23)
+            out["mix"] = ("grid {17,25,33,41}^3, L {3,5,7}, 0-3 inclusions, beam or isotropic point on a random "
+                          "face; warm-up: one uncounted request of every (grid, order) shape")
+            out["subset"] = (f"{len(mix)} of the 2,000 requests of the full stream (the full stream takes ~20 min "
+                             "of device time, beyond the bench's time budget; run it with --serve-requests 2000)")
+        if bench_shape:
+            b = serve_measure(srv, bench_shape, 0.0, 31)
+            b["workload"] = (f"{len(bench_shape)} single-source {N_SIDE}^3 L={L} requests, each a new 3-sphere phantom, "
+                             "collimated z=0 beam at a random position, 20 terms, mixed precision")
+            out["bench_shape"] = b
         st = srv.stats()
-    return {"requests": len(reqs), "workers": args.serve_workers,
-            "capacity_solves_per_s": capacity, "saturated_wall_s": wall_sat,
-            "arrival_rate_per_s": rate, "solves_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "wall_s": wall,
-            "device_ms_sum": dev_ms, "terms": TERMS,
-            "precision": "mixed (stored FP32 pair kernel; FFT convolution for uniform media)",
-            "contexts": st["contexts"], "hbm_reserved_gb": st["hbm_reserved"] / 1e9,
-            "failed": st["failed"] - st0["failed"],
-            "mix": "grid {17,25,33,41}^3, L {3,5,7}, 0-3 inclusions, beam or isotropic point on a random "
-                   "face; warm-up: one uncounted request of every (grid, order) shape"}
+    out.update({"workers": args.serve_workers, "terms": TERMS,
+                "precision": "mixed (stored FP32 pair kernel; FFT convolution for uniform media)",
+                "contexts": st["contexts"], "hbm_reserved_gb": st["hbm_reserved"] / 1e9,
+                "failed": st["failed"] - st0["failed"]})
+    return out
 
 
 CFG1_PAR = """[Runtime]
@@ -330,28 +361,38 @@ def run_cfg1(dev):
     return out
 
 
-def run_grad(dev):
-    """Adjoint gradient at the 33^3, L=5 phantom: 4 collimated z=0 sources at (+-0.825, +-0.825) cm,
-    8x8 bins on each of the 6 faces, target flux from the phantom with every sphere's coefficients
-    scaled by (1 + 0.05 N(0,1)); cost of rte_gradient against the forward solves it differentiates."""
+def grad_problem(dev, n=N_SIDE, prec=None, kernel_mode=None, terms=TERMS):
+    """Config 4: the n^3 L=5 phantom (3 spheres, seed 4), 4 collimated z=0 sources at (+-0.825, +-0.825) cm
+    scaled to the grid, 8x8 bins on each of the 6 faces, target flux from the phantom with every sphere's
+    coefficients scaled by (1 + 0.05 N(0,1))."""
     import doi_b200 as R
     from doi_b200.phantoms import sphere_phantom
-    mua, mus, sph = sphere_phantom(N_SIDE, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=3, seed=4)
+    mua, mus, sph = sphere_phantom(n, dx=DX, mua_bg=0.01, mus_bg=1.0, nspheres=3, seed=4)
     rng = np.random.default_rng(44)
     pa, ps = mua.copy(), mus.copy()
     for sp in sph:  # perturb each inclusion's values
         ka, ks = 1 + 0.05 * rng.standard_normal(2)
         pa[mua == sp["mua"]] *= ka
         ps[mus == sp["mus"]] *= ks
-    ctx = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_MIXED,
-                    kernel_mode=R.KERNEL_STORE, device=dev)
-    srcs = [R.Source(pos_x=x, pos_y=y, kind=R.SRC_COLUMN) for x, y in
-            ((-0.825, -0.825), (0.825, -0.825), (-0.825, 0.825), (0.825, 0.825))]
-    stop = R.Stop(R.STOP_FIXED, TERMS)
+    prec = R.PREC_MIXED if prec is None else prec
+    ctx = R.Context(n, n, n, dx=DX, nL=L, g=0.8, precision=prec, device=dev,
+                    kernel_mode=R.KERNEL_STORE if kernel_mode is None else kernel_mode)
+    off = 0.825 * n / 33.0
+    srcs = [R.Source(pos_x=x, pos_y=y, kind=R.SRC_COLUMN) for x, y in ((-off, -off), (off, -off), (-off, off), (off, off))]
+    stop = R.Stop(R.STOP_FIXED, terms)
     det = R.Detector(nbins=8, faces=63)
     ctx.set_medium_voxel(pa, ps)
     target = ctx.detector_flux(srcs, stop, det)
     ctx.set_medium_voxel(mua, mus)
+    return ctx, srcs, stop, det, target
+
+
+def run_grad(dev):
+    """Adjoint gradient at config 4 (33^3, L=5): cost of the mixed-precision rte_gradient against the
+    forward solves it differentiates, and its error against the FP64 method's gradient (stored FP64 pair
+    kernel) of the same 20-term model."""
+    import doi_b200 as R
+    ctx, srcs, stop, det, target = grad_problem(dev)
     ctx.detector_flux(srcs[:1], stop, det)
     ctx.gradient(srcs[:1], stop, det, target[:1])  # warm-up (autotuner, buffers)
     t = time.perf_counter()
@@ -361,48 +402,98 @@ def run_grad(dev):
     loss, ga, gs = ctx.gradient(srcs, stop, det, target)
     t_grad = time.perf_counter() - t
     ctx.close()
+    c64, srcs, stop, det, target = grad_problem(dev, prec=R.PREC_FP64, kernel_mode=R.KERNEL_STORE)
+    t = time.perf_counter()
+    loss64, ga64, gs64 = c64.gradient(srcs, stop, det, target)
+    t64 = time.perf_counter() - t
+    c64.close()
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
     return {"workload": "33^3 L=5 phantom, 4 z=0 sources, 8x8 bins x 6 faces, 20 terms, mixed precision",
             "forward_s_4src": t_fwd, "gradient_s_4src": t_grad, "ratio_gradient_over_forward": t_grad / t_fwd,
             "loss": loss, "grad_norm_mua": float(np.linalg.norm(ga)), "grad_norm_mus": float(np.linalg.norm(gs)),
-            "check": "central finite differences on 50 voxels (step 1e-4 rel) in tests/test_gpu_gradient.py"}
+            "fp64_rel_err": {"loss": abs(loss - loss64) / loss64, "g_mua": rel(ga, ga64), "g_mus": rel(gs, gs64),
+                             "against": "FP64 method (stored FP64 pair kernel) on the same 20-term model"},
+            "fp64_gradient_s_4src": t64,
+            "check": "central finite differences at this size in FP64 (10 + 10 voxels, 40 terms): "
+                     "tests/test_gpu_fullsize.py::test_gradient_finite_differences_at_config4_size"}
 
 
-def run_fisher(dev, n=25, Lq=5, nbins=16, terms=TERMS):
-    """Fisher information of 8 seeded inclusions x (x, y, z, mu_a contrast) = 32 parameters: background
-    mu_a 0.02, mu_s 2, g 0.9, six collimated beams at the face centres, nbins x nbins bins per face,
-    Poisson noise; J from one forward and 32 tangent solves per source (path integrals of each
-    parameter direction recomputed along every pair).  The full configuration is 49^3, L=7, 16x16."""
+def fisher_problem(dev, n, Lq, prec, kernel_mode):
+    """Config 5's medium at n^3: background mu_a 0.02, mu_s 2, g 0.9, 8 seeded inclusions rasterised with a
+    one-voxel partial-volume ramp (derivatives of x, y, z and mu_a contrast each: 32 parameters), six
+    collimated beams at the face centres."""
     import doi_b200 as R
     sph = R.random_spheres(n, 8, seed=55, dx=DX)
     mua, mus, dmua, dmus = R.smooth_sphere_phantom(n, sph, dx=DX, mua_bg=0.02, mus_bg=2.0)
-    ctx = R.Context(n, n, n, dx=DX, nL=Lq, g=0.9, precision=R.PREC_MIXED, kernel_mode=R.KERNEL_STORE, device=dev)
+    ctx = R.Context(n, n, n, dx=DX, nL=Lq, g=0.9, precision=prec, kernel_mode=kernel_mode, device=dev)
     ctx.set_medium_voxel(mua, mus)
     h = n * DX / 2
     srcs = [R.Source(kind=R.SRC_BEAM, face=0), R.Source(kind=R.SRC_BEAM, face=1, pos_z=n * DX),
             R.Source(kind=R.SRC_BEAM, face=2, pos_z=h), R.Source(kind=R.SRC_BEAM, face=3, pos_z=h),
             R.Source(kind=R.SRC_BEAM, face=4, pos_z=h), R.Source(kind=R.SRC_BEAM, face=5, pos_z=h)]
+    return ctx, srcs, dmua, dmus
+
+
+def run_fisher_case(dev, n, Lq, nbins, terms, nsrc=6, P=32, kernel_mode=None, prec=None, want_J=False):
+    """One rte_fisher call of nsrc sources x P parameters; returns (F, J, seconds, forward seconds of the
+    same sources, stats)."""
+    import doi_b200 as R
+    ctx, srcs, dmua, dmus = fisher_problem(dev, n, Lq, R.PREC_MIXED if prec is None else prec,
+                                           R.KERNEL_RECOMPUTE if kernel_mode is None else kernel_mode)
     stop = R.Stop(R.STOP_FIXED, terms)
     det = R.Detector(nbins=nbins, faces=63)
-    ctx.fisher(srcs[:1], stop, det, dmua[:1], dmus[:1])  # warm-up (pair kernel, buffers)
     ctx.stats()
     ctx.set_profiling(True)
     t = time.perf_counter()
-    F = ctx.fisher(srcs, stop, det, dmua, dmus)
-    wall = time.perf_counter() - t
+    res = ctx.fisher(srcs[:nsrc], stop, det, dmua[:P], dmus[:P], want_J=want_J)
+    sec = time.perf_counter() - t
     st = ctx.stats()
     t = time.perf_counter()
-    ctx.forward_batch(srcs[:2], stop, want_W=False)
-    ctx.forward_batch(srcs[2:4], stop, want_W=False)
-    ctx.forward_batch(srcs[4:], stop, want_W=False)
+    ctx.detector_flux(srcs[:nsrc], stop, det)
     t_fwd = time.perf_counter() - t
     ctx.close()
+    F, J = res if want_J else (res, None)
+    return F, J, sec, t_fwd, st
+
+
+def run_fisher(dev, full_matrix_at_49=False):
+    """Fisher information of 8 seeded inclusions x (x, y, z, mu_a contrast) = 32 parameters (BASELINE config
+    5), Poisson noise, path integrals recomputed along every pair in every term (no stored pair kernel):
+    (1) the full configuration, 49^3, L=7, 16x16 bins, on a bounded leg of 1 source x 2 parameters (one
+    two-right-hand-side tangent series), extrapolated to 6 sources x 32 parameters; (2) the whole 32 x 32
+    matrix at 25^3, L=5; (3) its FP64 error on 1 source x 4 parameters against the FP64 method."""
+    import doi_b200 as R
+    out = {"workload": "8 inclusions x 4 = 32 parameters, 6 face-centre beams, 16x16 bins x 6 faces, 20 terms, "
+                       "mixed precision, path integrals recomputed (no stored pair kernel)"}
+    # (1) the full configuration, bounded
+    run_fisher_case(dev, 49, 7, 16, 2, nsrc=1, P=2)  # warm-up: split autotuning, buffers
+    if full_matrix_at_49:
+        F, _, sec, t_fwd, st = run_fisher_case(dev, 49, 7, 16, TERMS)
+        out["full_49_L7"] = {"seconds": sec, "measured": "6 sources x 32 parameters", "pair_kernel_ms": st["ms_pair"]}
+    else:
+        F, _, sec, t_fwd, st = run_fisher_case(dev, 49, 7, 16, TERMS, nsrc=1, P=2)
+        t_tan = max(sec - t_fwd, 0.0)
+        out["full_49_L7"] = {
+            "measured": "1 source x 2 parameters (the forward solve and one two-right-hand-side tangent series)",
+            "seconds": sec, "forward_s_1src": t_fwd, "tangent_s_2params": t_tan,
+            "extrapolated_s_6src_32params": 6 * t_fwd + 6 * 16 * t_tan,
+            "extrapolation": "6 forward solves + 6 x 16 two-parameter tangent series at the measured rates",
+            "pair_kernel_ms": st["ms_pair"], "launches": st["launches"]}
+    # (2) the whole matrix at 25^3, L=5
+    F, _, sec, t_fwd, st = run_fisher_case(dev, 25, 5, 16, TERMS)
     ev = np.linalg.eigvalsh(F)
-    return {"workload": f"{n}^3 L={Lq}, 8 inclusions x 4 = 32 parameters, 6 face-centre beams, {nbins}x{nbins} bins "
-                        f"x 6 faces, {terms} terms, mixed precision",
-            "seconds": wall, "tangent_solves": 6 * 32, "forward_solves_6src_s": t_fwd,
-            "pair_kernel_ms": st["ms_pair"], "launches": st["launches"],
-            "F_trace": float(np.trace(F)), "F_cond": float(ev.max() / max(ev.min(), 1e-300)),
-            "F_min_eig": float(ev.min())}
+    out["matrix_25_L5"] = {"seconds": sec, "tangent_solves": 6 * 32, "forward_solves_6src_s": t_fwd,
+                           "pair_kernel_ms": st["ms_pair"], "launches": st["launches"], "F_trace": float(np.trace(F)),
+                           "F_cond": float(ev.max() / max(ev.min(), 1e-300)), "F_min_eig": float(ev.min())}
+    # (3) FP64 error of F and J (1 source x 4 parameters at 25^3 L=5)
+    Fm, Jm, _, _, _ = run_fisher_case(dev, 25, 5, 16, TERMS, nsrc=1, P=4, want_J=True)
+    F64, J64, _, _, _ = run_fisher_case(dev, 25, 5, 16, TERMS, nsrc=1, P=4, want_J=True, prec=R.PREC_FP64,
+                                        kernel_mode=R.KERNEL_STORE)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    out["fp64_rel_err"] = {"F": rel(Fm, F64), "J": rel(Jm, J64), "case": "25^3 L=5, 1 source x 4 parameters",
+                           "note": "F weights each bin by 1/flux; bins of near-zero flux amplify the mixed solve's "
+                                   "relative flux error there, so F's error exceeds J's"}
+    return out
 
 
 def run_uniform(dev):
@@ -540,15 +631,27 @@ def run_ours(args):
         r_mixed = ctx.forward_batch(srcs, stop, want_W=True) if B > 1 else ctx.forward(src, stop, want_W=True)
         if B > 1:
             r_mixed = {k: r_mixed[k][0] for k in ("W", "trans", "ref")}
-        ref_err, plain = None, None
+        ref_err, plain, plain_stored = None, None, None
         if prec == R.PREC_MIXED and not args.skip_fp64_check:
+            # the plain FP64 method as the reference computes it (every path integral recomputed every
+            # term), and the same method with its FP64 pair kernel stored (8 N^2 bytes, precompute included)
             c64 = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_FP64, device=dev)
             c64.set_medium_voxel(*media[args.warmup])
             r64 = c64.forward(srcs[0], stop, want_W=True)
             rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
             ref_err = {"W": rel(r_mixed["W"], r64["W"]), "trans": rel(r_mixed["trans"], r64["trans"]),
-                       "ref": rel(r_mixed["ref"], r64["ref"])}
+                       "ref": rel(r_mixed["ref"], r64["ref"]), "against": "plain FP64 method on the same phantom "
+                       "and source (itself within 1e-11 of the FP64 oracle: tests/test_gpu_fullsize.py)"}
             plain = 1e3 / r64["ms_device"]
+            c64.close()
+            c64 = R.Context(N_SIDE, N_SIDE, N_SIDE, dx=DX, nL=L, g=0.8, precision=R.PREC_FP64,
+                            kernel_mode=R.KERNEL_STORE, device=dev)
+            c64.set_medium_voxel(*media[0])
+            c64.forward(srcs[0], stop, want_W=False)  # warm-up on another phantom
+            c64.set_medium_voxel(*media[args.warmup])
+            r64s = c64.forward(srcs[0], stop, want_W=True)
+            ref_err["fp64_stored_vs_recomputed_W"] = rel(r64s["W"], r64["W"])
+            plain_stored = 1e3 / r64s["ms_device"]
             c64.close()
         avg_pair_ms = st["ms_pair"] / max(st["n_pair"], 1)
         nbk = 1 if B == 1 else (2 if B <= 2 else 4)  # right-hand sides per launch
@@ -579,7 +682,10 @@ def run_ours(args):
                          "traffic": traffic, "kernel": "k_pair_mixed<5,stored>" if prec == R.PREC_MIXED
                          else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
                          "flop_per_launch": apply_flop, "rhs_per_launch": nbk,
-                         "peak_source": "measured by rte_measure_fma_peak (8-chain FMA probe) in this run",
+                         "peak_source": ("measured in this run by rte_measure_fma_peak (8 independent FMA chains "
+                                         "per thread on every SM), of measured; theoretical FP32 148 SMs x 128 "
+                                         "FMA/clk x 2 x 1.965 GHz = 74.4 TFLOP/s, FP64 half of it (37.2); "
+                                         "MEASURED_PEAKS.json holds HBM and bf16 only"),
                          "hbm": hbm_line(traffic, avg_pair_ms)},
             "cpu_baseline": None,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -587,6 +693,9 @@ def run_ours(args):
             "clocks": clocks,
             "fp64_rel_err": ref_err,
             "plain_fp64_solves_per_s": plain,
+            "plain_fp64_stored_kernel_solves_per_s": plain_stored,
+            "speedup_over_plain_fp64": {"recomputed": value / plain if plain else None,
+                                        "stored_kernel": value / plain_stored if plain_stored else None},
             "kernel_ms_per_step": {"pair": st["ms_pair"] / args.steps, "store": st["ms_store"] / args.steps,
                                    "epilogue": st["ms_epi"] / args.steps},
             "solve_tflops_canonical": B * counts["solve_flop"] / (ms / args.steps / 1e3) / 1e12,
@@ -597,10 +706,14 @@ def run_ours(args):
         if not args.skip_extras:
             line["config1_plain_fp64"] = run_cfg1(dev)
             line["config4_gradient"] = run_grad(dev)
-            line["config5_fisher"] = run_fisher(dev, **({"n": 49, "Lq": 7} if args.fisher_full else {}))
+            line["config5_fisher"] = run_fisher(dev, full_matrix_at_49=args.fisher_full)
             line["uniform_fft"] = run_uniform(dev)
-        if args.serve_requests > 0:
+        if args.serve_requests > 0 or args.serve_requests_33 > 0:
             line["serve"] = run_serve(args, dev)
+            bs = line["serve"].get("bench_shape")
+            if bs and plain:
+                bs["vs_plain_fp64"] = {"recomputed": bs["capacity_solves_per_s"] / plain,
+                                       "stored_kernel": bs["capacity_solves_per_s"] / plain_stored if plain_stored else None}
         out = line
     ctx.close()
     if ws > 1:
@@ -608,6 +721,23 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if out is not None:
         print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_profile(args):
+    """Small single-purpose runs for ncu captures (no timing line): --profile-grad N runs one mixed-
+    precision gradient of the config-4 problem at N^3 (4 sources, 8x8 bins, 20 terms); --profile-fisher N
+    one mixed-precision Fisher information at N^3, L=5 (1 face beam, 8 parameters, 16x16 bins, path
+    integrals recomputed)."""
+    import doi_b200 as R
+    if args.profile_grad:
+        ctx, srcs, stop, det, target = grad_problem(0, n=args.profile_grad)
+        loss, ga, gs = ctx.gradient(srcs, stop, det, target)
+        ctx.close()
+        print(json.dumps({"profile": "gradient", "n": args.profile_grad, "loss": loss}))
+    if args.profile_fisher:
+        F = run_fisher_case(0, args.profile_fisher, 5, 16, TERMS, nsrc=1, P=8, kernel_mode=R.KERNEL_RECOMPUTE)[0]
+        print(json.dumps({"profile": "fisher", "n": args.profile_fisher, "F_trace": float(np.trace(F))}))
     return 0
 
 
@@ -625,9 +755,14 @@ def main():
     ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
                     help="sources per phantom solved together (1 = one source per solve)")
     ap.add_argument("--skip-extras", action="store_true", help="skip the config-1, gradient and Fisher measurements")
-    ap.add_argument("--fisher-full", action="store_true", help="Fisher at the full 49^3, L=7 size (long)")
+    ap.add_argument("--fisher-full", action="store_true",
+                    help="the whole 32 x 32 Fisher matrix at 49^3, L=7 instead of the bounded leg (long)")
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
+    ap.add_argument("--profile-grad", type=int, default=0, help="one config-4 gradient at this grid side, then exit")
+    ap.add_argument("--profile-fisher", type=int, default=0, help="one Fisher information at this grid side, then exit")
+    ap.add_argument("--serve-requests-33", type=int, default=32,
+                    help="requests in the single-shape 33^3 L=5 serving stream (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="Poisson arrival rate (requests/s); 0 = 0.7 x the capacity measured first")
     ap.add_argument("--serve-workers", type=int, default=4, help="requests in flight at most")
@@ -638,6 +773,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_grad or args.profile_fisher:
+        return run_profile(args)
     return run_ours(args)
 
 

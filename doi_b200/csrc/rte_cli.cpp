@@ -299,13 +299,19 @@ int main_inverse(const char* path) {
   }
   const int nt = L.pr.ntypes;
   std::vector<double> ga(nt), ga2(nt), gs(nt), gs2(nt), mua(L.pr.mua, L.pr.mua + nt), mus(L.pr.mus, L.pr.mus + nt);
+  // [Algorithm] ReferenceQuirks = 1 (default): the main's device tissue table keeps the .par values
+  // (populate_info_dev()'s result is dropped, compute_grad_rte.cu:431), so the path integrals and the
+  // scatter use them while the source, self-voxel term and images take the swept values; 0: the swept
+  // values throughout
+  const int quirks = rte_par_get_int(L.par, "Algorithm:ReferenceQuirks", 1);
   FILE* resf = fopen("Residual.out", "wb");
   // the main sweeps tissue 1 over a fixed grid of values, one gradient evaluation per iteration
   // (compute_grad_rte.cu:207-209); its parameter update is disabled in the reference
   for (int itt = 0; itt < L.pr.num_iterations; itt++) {
     mus[1] = 0.8 + round(itt / 2.0) * 0.05;
     mua[1] = 0.008 + floor(itt / 2.0) * 0.0005;
-    rc = rte_set_medium_tissue(L.ctx, L.pr.tiss, nt, mua.data(), mus.data());
+    rc = quirks ? rte_set_medium_tissue_split(L.ctx, L.pr.tiss, nt, mua.data(), mus.data(), L.pr.mua, L.pr.mus)
+                : rte_set_medium_tissue(L.ctx, L.pr.tiss, nt, mua.data(), mus.data());
     if (rc) return die(L.ctx, "set medium", rc);
     double res = 0, res2 = 0;
     rc = rte_region_gradient(L.ctx, &L.pr.src, &L.pr.stop, g.data(), L.pr.tiss, nt, 1, ga.data(), ga2.data(),
@@ -328,8 +334,13 @@ int main_inverse(const char* path) {
 // rte_snr (FisherInfo_IO/src/rte_snr.cu:80-385): squared detection SNR of a spherical mu_a lesion
 // (radius 3 fov / (2 nX), tissue 2, mu_a 0.35 against 0.25, mu_s 1) at depths z index 2 .. 15 on the
 // reflection image, SNR^2 = sum_j (g1_j - g0_j)^2 / g0_j, written to snr_terms.dat (nZ - 2 doubles).
-// The reference steps its depth loop with `loc_indz = loc_indz++` (undefined in C); here it steps by
-// one and stops at the last layer of small grids.
+// The reference steps its depth loop with `loc_indz = loc_indz++` (undefined in C; under gcc the index
+// never advances); here it steps by one and stops at the last layer of small grids.
+// [Algorithm] ReferenceQuirks = 1 (default) reproduces what the main computes at each depth: its device
+// tissue table keeps the .par values (rte_snr.cu:239 drops populate_info_dev()'s result), so the path
+// integrals and the scatter use them while the source, self-voxel term and images take the lesion's
+// values, and its z coordinate array is filled only for indices below nX (rte_snr.cu:175-179; the rest
+// read as 0).  0: the lesion's values throughout and every z coordinate.
 int main_snr(const char* path) {
   Loaded L;
   if (load(path, false, L)) return 1;
@@ -365,7 +376,8 @@ int main_snr(const char* path) {
   const double fov = c.x_max - c.x_min;
   auto X = [&](int i) { return i * fov / c.nx - fov / 2 + fov / (2 * c.nx); };
   auto Y = [&](int i) { return i * fov / c.ny - fov / 2 + fov / (2 * c.ny); };
-  auto Z = [&](int i) { return i * fov / c.nz + fov / (2 * c.nz); };
+  const int quirks = rte_par_get_int(L.par, "Algorithm:ReferenceQuirks", 1);
+  auto Z = [&](int i) { return (quirks && i >= c.nx) ? 0.0 : i * fov / c.nz + fov / (2 * c.nz); };
   const float rad = (float)(3 * fov / (2 * c.nx));
   const float rad2 = rad * rad;
   const int initz = 2, lx = c.nx / 2, ly = c.ny / 2;
@@ -383,7 +395,9 @@ int main_snr(const char* path) {
     for (int hyp = 1; hyp >= 0; hyp--) {
       ta[2] = 0.25 + 0.1 * hyp;
       ts[2] = 1.0;
-      int rc = rte_set_medium_tissue(L.ctx, tiss.data(), L.pr.ntypes, ta.data(), ts.data());
+      int rc = quirks ? rte_set_medium_tissue_split(L.ctx, tiss.data(), L.pr.ntypes, ta.data(), ts.data(), L.pr.mua,
+                                                    L.pr.mus)
+                      : rte_set_medium_tissue(L.ctx, tiss.data(), L.pr.ntypes, ta.data(), ts.data());
       if (!rc) rc = rte_forward(L.ctx, &L.pr.src, &L.pr.stop, nullptr, tr.data(), hyp ? g1.data() : g0.data(), nullptr);
       if (rc) return die(L.ctx, "rte_forward", rc);
     }
@@ -406,11 +420,13 @@ int main_fisher(const char* path) {
   if (rc) return die(L.ctx, "set medium", rc);
   // region: the voxels within rad_sig[0] = fov/(2 nX) of voxel (nX/2, nY/2, 1), on the main's own
   // coordinate arrays, which use the x extent for every axis (rte_fim.cu:135-206).  The reference
-  // fills its z array only for indices below nX; here every index follows the same formula.
+  // fills its z array only for indices below nX; with ReferenceQuirks (default) the others read as 0, as
+  // in the reference's run (the region about z index 1 is the same either way).
   const double fov = c.x_max - c.x_min;
   auto X = [&](int i) { return i * fov / c.nx - fov / 2 + fov / (2 * c.nx); };
   auto Y = [&](int i) { return i * fov / c.ny - fov / 2 + fov / (2 * c.ny); };
-  auto Z = [&](int i) { return i * fov / c.nz + fov / (2 * c.nz); };
+  const int quirks = rte_par_get_int(L.par, "Algorithm:ReferenceQuirks", 1);
+  auto Z = [&](int i) { return (quirks && i >= c.nx) ? 0.0 : i * fov / c.nz + fov / (2 * c.nz); };
   const float rad = (float)(1 * fov / (2 * c.nx));
   const float rad2 = rad * rad;  // a float product, compared against the double distance
   const int lx = c.nx / 2, ly = c.ny / 2, lz = 1;

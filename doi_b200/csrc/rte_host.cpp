@@ -317,6 +317,7 @@ struct rte_ctx {
   double *d_aux1 = nullptr, *d_aux2 = nullptr, *d_aux3 = nullptr, *d_aux4 = nullptr;  // real-basis staging
   float* d_Wf = nullptr;
   float* d_K = nullptr;
+  double* d_K64 = nullptr;      // FP64 pair kernel (FP64 contexts in RTE_KERNEL_STORE mode)
   bool K_valid = false;
   double* d_cplx = nullptr;
   double* d_red = nullptr;
@@ -365,6 +366,12 @@ struct rte_ctx {
   std::vector<uintptr_t> graph_sig[5];
   void* d_Qbp = nullptr;        // gradient: weight of every unordered voxel pair (N x round32(N))
   uint8_t* d_mask = nullptr;    // region mask of the reference-compatible tangent solves [N]
+  bool transpose = false;       // pair kernels apply A^T (table model: reverse-displacement snapping)
+  // split medium (rte_set_medium_tissue_split): the self-voxel term, the source and its ballistic beam
+  // take d_mut_self / d_mus_src, while the pair kernels and the scatter keep d_mut / d_mus
+  bool split = false;
+  double* d_mut_self = nullptr;
+  double* d_mus_src = nullptr;
   bool uniform = false;         // the medium has one mu_t: the operator is a convolution
   double uniform_mut = 0.0;
   FftState* fft = nullptr;      // its table spectra, buffers and plans
@@ -473,11 +480,11 @@ static void free_all(rte_ctx* c) {
     }
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   void* ps[] = {c->d_perm, c->d_mut, c->d_mus, c->d_mutf, c->d_W, c->d_Wn, c->d_sum, c->d_part, c->d_mom,
-                c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_cplx, c->d_red, c->d_img,
+                c->d_aux1, c->d_aux2, c->d_aux3, c->d_aux4, c->d_Wf, c->d_K, c->d_K64, c->d_cplx, c->d_red, c->d_img,
                 c->d_selfp, c->d_self_idx, c->d_self_lut, c->d_islot, c->d_slot_xyz, c->d_err,
                 c->d_bW, c->d_bWn, c->d_bsum, c->d_bres, c->d_bball, c->d_bWf, c->d_h, c->d_S, c->d_out,
                 c->d_e, c->d_lam, c->d_y, c->d_gt, c->d_gs, c->d_J, c->d_rho, c->d_dlut, c->d_fball, c->d_q, c->d_bq,
-                c->d_Qbp, c->d_mask, c->d_dmut, c->d_dmus, c->d_T, c->d_cidx, c->d_cval, c->d_self_lut_im,
+                c->d_Qbp, c->d_mask, c->d_dmut, c->d_dmus, c->d_mut_self, c->d_mus_src, c->d_T, c->d_cidx, c->d_cval, c->d_self_lut_im,
                 c->d_fball_im};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -673,12 +680,16 @@ static int ensure_moments(rte_ctx* c, double mumax) {
   return RTE_OK;
 }
 
+// mu_t of the self-voxel term and (mu_t, mu_s) of the source: the medium's, or the split table's
+static const double* self_mut(const rte_ctx* c) { return c->split ? c->d_mut_self : c->d_mut; }
+static const double* source_mus(const rte_ctx* c) { return c->split ? c->d_mus_src : c->d_mus; }
+
 // Self-voxel matrices D(mu) = sum_k mu^k M_k for each distinct mu_t of the medium (a handful for
 // tissue maps and sphere phantoms), and the voxel -> matrix index.  Media with more than 4096
 // distinct values use the power series on the device instead.
 static int build_self_lut(rte_ctx* c) {
   std::vector<double> mut(c->N);
-  CUDA_TRY(c, cudaMemcpyAsync(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(mut.data(), self_mut(c), sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   std::unordered_map<double, int> id;
   std::vector<int> idx(c->N);
@@ -761,7 +772,7 @@ static int build_self_lut(rte_ctx* c) {
   CUDA_TRY(c, cudaMemcpyAsync(c->d_self_idx, idx.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice, c->st));
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->self_lut_ok = true;
-  c->uniform = vals.size() == 1;
+  c->uniform = vals.size() == 1 && !c->split;  // a split medium keeps the pair kernels
   c->uniform_mut = vals[0];
   return RTE_OK;
 }
@@ -775,6 +786,7 @@ static int medium_from_device(rte_ctx* c, const double* d_mua, const double* d_m
   CUDA_TRY(c, cudaStreamSynchronize(c->st));
   c->K_valid = false;
   c->medium_set = true;
+  c->split = false;
   c->mumax = mumax;
   int rc = ensure_moments(c, std::hypot(mumax, c->kappa));
   if (rc) return rc;
@@ -809,6 +821,39 @@ extern "C" int rte_set_medium_tissue(rte_ctx* c, const uint8_t* tiss, int ntypes
   return rte_set_medium_voxel(c, a.data(), s.data());
 }
 
+static int unsupported_modulated(rte_ctx* c, const char* what);
+
+// Two tissue tables on one tissue map, as the FisherInfo_IO SNR and region-gradient mains leave them:
+// they change tissue values on the host (self-voxel table, source and images follow) but drop the
+// result of populate_info_dev() (rte_snr.cu:239, compute_grad_rte.cu:431), so the device kernels'
+// path integrals (compute_propabs) and scatter (prop_scat_dev) keep the .par values.
+extern "C" int rte_set_medium_tissue_split(rte_ctx* c, const uint8_t* tiss, int ntypes, const double* mua,
+                                           const double* mus, const double* mua_kernel, const double* mus_kernel) {
+  if (!c || !tiss || !mua || !mus || !mua_kernel || !mus_kernel || ntypes <= 0 || ntypes > 256)
+    return fail(c, RTE_ERR_ARG, "bad tissue arguments");
+  if (c->kappa != 0.0) return unsupported_modulated(c, "a split tissue table");
+  int rc = rte_set_medium_tissue(c, tiss, ntypes, mua_kernel, mus_kernel);
+  if (rc) return rc;
+  std::vector<double> t(c->N), sc(c->N);
+  double mumax = c->mumax;
+  for (int r = 0; r < c->N; r++) {
+    if (!(mua[tiss[r]] >= 0.0) || !(mus[tiss[r]] >= 0.0)) return fail(c, RTE_ERR_ARG, "negative or NaN coefficient");
+    t[r] = mua[tiss[r]] + mus[tiss[r]];
+    sc[r] = mus[tiss[r]];
+    mumax = std::max(mumax, t[r]);
+  }
+  if (!c->d_mut_self) CUDA_TRY(c, dalloc(c, &c->d_mut_self, (size_t)c->N));
+  if (!c->d_mus_src) CUDA_TRY(c, dalloc(c, &c->d_mus_src, (size_t)c->N));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mut_self, t.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_mus_src, sc.data(), sizeof(double) * c->N, cudaMemcpyHostToDevice, c->st));
+  c->split = true;
+  c->mumax = mumax;
+  rc = ensure_moments(c, mumax);
+  if (!rc) rc = build_self_lut(c);
+  if (rc) c->medium_set = false;
+  return rc;
+}
+
 // scatter factor per l (prop_scat_dev, FisherInfo_IO/src/kernels.cu:385-418)
 static void scatter_factors(const rte_ctx* c, int flag, double* s) {
   for (int l = 0; l <= RTE_MAX_L; l++) {
@@ -825,12 +870,15 @@ static void scatter_factors(const rte_ctx* c, int flag, double* s) {
   }
 }
 
+// The stored pair kernel: FP32 for the mixed method (store or automatic mode), FP64 for the FP64
+// method when RTE_KERNEL_STORE asks for it (automatic FP64 contexts keep recomputing: the plain method).
 static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
   *stored = false;
-  if (c->precision != RTE_PREC_MIXED || c->kernel_mode == RTE_KERNEL_RECOMPUTE) return RTE_OK;
+  const bool f64 = c->precision == RTE_PREC_FP64;
+  if (c->kernel_mode == RTE_KERNEL_RECOMPUTE || (f64 && c->kernel_mode != RTE_KERNEL_STORE)) return RTE_OK;
   const size_t ld = ((size_t)c->N + 31) / 32 * 32;  // 128-byte rows
-  const size_t need = (size_t)c->N * ld * sizeof(float);
-  if (!c->d_K) {
+  const size_t need = (size_t)c->N * ld * (f64 ? sizeof(double) : sizeof(float));
+  if (f64 ? !c->d_K64 : !c->d_K) {
     size_t fr = 0, tot = 0;
     CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
     if (need + (1ull << 30) > fr) {
@@ -838,7 +886,10 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
         return fail(c, RTE_ERR_NOMEM, "pair kernel needs %.1f GB, %.1f GB free", need / 1e9, fr / 1e9);
       return RTE_OK;  // auto: recompute
     }
-    CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * ld));
+    if (f64)
+      CUDA_TRY(c, dalloc(c, &c->d_K64, (size_t)c->N * ld));
+    else
+      CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * ld));
     c->Kld = ld;
   }
   if (!c->K_valid || c->capture_store) {
@@ -855,16 +906,18 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     a.prop_thresh = c->prop_thresh;
     a.kscale = c->dV / c->cm;
     a.perm = c->d_perm;
+    a.mut = c->d_mut;
     a.mutf = c->d_mutf;
     a.Kmat = c->d_K;
+    a.Kmat64 = c->d_K64;
     a.Kld = c->Kld;
     if (c->capturing) {
-      CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+      CUDA_TRY(c, rte_launch_store_kernel(a, c->st, f64 ? 1 : 0));
     } else {
       CUDA_TRY(c, cudaEventRecord(c->ev0, c->st));
       {
         ProfScope ps(c, 1);
-        CUDA_TRY(c, rte_launch_store_kernel(a, c->st));
+        CUDA_TRY(c, rte_launch_store_kernel(a, c->st, f64 ? 1 : 0));
       }
       CUDA_TRY(c, cudaEventRecord(c->ev1, c->st));
       CUDA_TRY(c, cudaEventSynchronize(c->ev1));
@@ -902,6 +955,7 @@ static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in3
   a.Win = in64;
   a.Winf = in32;
   a.Kmat = c->d_K;
+  a.Kmat64 = c->d_K64;
   a.Kld = c->Kld;
   a.part = c->d_part;
   a.chunk = chunk;
@@ -912,6 +966,7 @@ static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in3
   a.cpad = (nb * a.cstride + 3) / 4 * 4;
   a.err = c->d_err;
   a.kappa = c->kappa;
+  a.transpose = c->transpose ? 1 : 0;
   return a;
 }
 
@@ -1053,7 +1108,9 @@ static bool fft_eligible(const rte_ctx* c) {
 }
 
 // inside a graph capture only when the recording prepared the transforms beforehand
-static bool fft_active(const rte_ctx* c) { return fft_eligible(c) && (!c->capturing || c->fft_capture_ready); }
+static bool fft_active(const rte_ctx* c) {
+  return fft_eligible(c) && !c->transpose && (!c->capturing || c->fft_capture_ready);
+}
 
 static int ensure_fft(rte_ctx* c) {
   FftTabArgs a;
@@ -1101,7 +1158,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   sa.Cact = (LA + 1) * (LA + 1);
   sa.K = c->K;
   sa.W = in64;
-  sa.mut = c->d_mut;
+  sa.mut = self_mut(c);
   sa.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
   sa.lut = c->d_self_lut;
   sa.mom = c->d_mom;
@@ -1348,6 +1405,7 @@ extern "C" int rte_set_modulation(rte_ctx* c, double modulation) {
   if (!std::isfinite(modulation)) return fail(c, RTE_ERR_ARG, "modulation must be finite");
   if (modulation != 0.0 && c->model == RTE_MODEL_FIM)
     return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation takes the exact or the CPU-package model");
+  if (modulation != 0.0 && c->split) return fail(c, RTE_ERR_UNSUPPORTED, "intensity modulation of a split tissue table");
   CUDA_TRY(c, cudaSetDevice(c->cfg.device));
   const double kappa = modulation / c->cm;  // mu_a + i modulation / (c/n), RTE_uniform.c:129
   if (kappa != 0.0 && !c->d_fball_im) {
@@ -1411,6 +1469,34 @@ extern "C" int rte_prop_abs(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int f
     if (rc) return rc;
   }
   rc = check_kernel_err(c);
+  if (rc) return rc;
+  return download_cplx(c, c->d_W, has2 ? c->d_sum : nullptr, out);
+}
+
+// out = A^H in: the adjoint of prop_abs without scatter.  In the real basis A^T = P A P (P = (-1)^l) for
+// exact directions; the table model applies its transposed pair kernels (see adjoint_series).
+extern "C" int rte_prop_abs_adjoint(rte_ctx* c, const rte_cplx* in, rte_cplx* out, int flag) {
+  if (!c || !in || !out) return fail(c, RTE_ERR_ARG, "null argument");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (c->kappa != 0.0) return unsupported_modulated(c, "the adjoint operator");
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  bool has2 = false;
+  int rc = upload_cplx(c, in, c->d_aux1, c->d_aux2, &has2);
+  if (rc) return rc;
+  const bool mixed = c->precision == RTE_PREC_MIXED, table = c->model == RTE_MODEL_FIM;
+  double* parts[2] = {c->d_aux1, c->d_aux2};
+  double* res[2] = {c->d_W, c->d_sum};
+  for (int k = 0; k < (has2 ? 2 : 1) && !rc; k++) {
+    if (!table) CUDA_TRY(c, (c->launches++, rte_launch_parity(parts[k], c->N, c->L, c->C, c->st)));
+    if (mixed)
+      CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(parts[k], c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C,
+                                                          c->cstride, c->st)));
+    c->transpose = table;
+    rc = apply_term(c, parts[k], c->d_Wf, res[k], nullptr, nullptr, flag, 0);
+    c->transpose = false;
+    if (!rc && !table) CUDA_TRY(c, (c->launches++, rte_launch_parity(res[k], c->N, c->L, c->C, c->st)));
+  }
+  if (!rc) rc = check_kernel_err(c);
   if (rc) return rc;
   return download_cplx(c, c->d_W, has2 ? c->d_sum : nullptr, out);
 }
@@ -1589,8 +1675,8 @@ static int launch_source(rte_ctx* c, const rte_source* s, double* d_dst, int vst
   a.z_min = c->cfg.z_min;
   a.dz = c->dz;
   a.vstride = vstride;
-  a.mut = c->d_mut;
-  a.mus = c->d_mus;
+  a.mut = self_mut(c);
+  a.mus = source_mus(c);
   a.W = d_dst;
   a.fball = d_fball;
   a.kappa = c->kappa;
@@ -2278,6 +2364,7 @@ static BpArgs bp_args(rte_ctx* c, bool accumulate) {
   bp.y = c->d_y;
   bp.S = c->d_S;
   bp.Kmat = c->K_valid && c->d_K ? c->d_K : nullptr;
+  bp.Kmat64 = c->K_valid && c->d_K64 ? c->d_K64 : nullptr;
   bp.Kld = ((size_t)c->N + 31) / 32 * 32;
   bp.g = c->d_gt;
   bp.Q = c->d_Qbp;
@@ -2304,33 +2391,178 @@ static int ensure_bp_buffer(rte_ctx* c) {
   return RTE_OK;
 }
 
+// Adjoint field of one source: lambda = (I - A^T D)^-1 A^T e for the seed e = dL/d(out) in d_e, with
+// A^T = P A P (P = (-1)^l in the real basis: A's kernel is symmetric in (r, r') and R(-w) = P R(w)), so
+// lambda = P A (I - D A)^-1 P e: the forward machinery on P e, the same number of terms as the forward
+// solve it differentiates (`terms`), result in d_lam.
+// The table model (RTE_MODEL_FIM) snaps pair directions to its 100 x 100 table, and snapping does not
+// commute with negation: there A^T is applied directly (pair kernels in transposed mode; the self term
+// and D are symmetric), lambda = (I - A^T D)^-1 A^T e = A^T (I - D A^T)^-1 e.
+static int adjoint_series(rte_ctx* c, const rte_stop* stop, int terms) {
+  const size_t NC = (size_t)c->N * c->C;
+  const bool table = c->model == RTE_MODEL_FIM;
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_aux3, c->d_e, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  if (!table) CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_aux3, c->N, c->L, c->C, c->st)));
+  if (c->precision == RTE_PREC_MIXED)
+    CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_aux3, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C,
+                                                        c->cstride, c->st)));
+  c->transpose = table;
+  int rc = apply_term(c, c->d_aux3, c->d_Wf, c->d_aux4, nullptr, nullptr, 1, 1);
+  if (!rc) {
+    CUDA_TRY(c, (c->launches++, rte_launch_axpy(c->d_aux3, c->d_aux4, 1.0, NC, c->st)));
+    rc = neumann_real(c, c->d_aux4, c->d_aux3, c->d_lam, 1, stop, std::max(terms - 1, 0), nullptr, nullptr);
+  }
+  c->transpose = false;
+  if (rc) return rc;
+  if (!table) CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_lam, c->N, c->L, c->C, c->st)));
+  return RTE_OK;
+}
+
+// Exact derivative of the discrete model for one source, after its forward solve (d_S = running sum,
+// d_out = A S) and with the seed e = dL/d(out) in d_e: the adjoint series, the pair weights of the
+// back-projection (pass 1, summed into the pair-weight buffer; `first` overwrites it), the self-term
+// and scatter parts (into d_gt, d_gs), and on the host the source column and the ballistic beam of a
+// z = 0 collimated source (rho_ball = dL/d(ballistic flux at the z = nZ-1 exit pixel of the column),
+// into ga, gsum).  The walk of pass 2 runs once after all sources (rte_launch_bp_walk).
+static int adjoint_source_terms(rte_ctx* c, const rte_source* s, const rte_stop* stop, int terms, double rho_ball,
+                                bool first, const std::vector<double>& mut, const std::vector<double>& mus,
+                                std::vector<double>& ga, std::vector<double>& gsum) {
+  const bool mixed = c->precision == RTE_PREC_MIXED;
+  double scat[RTE_MAX_L + 1];
+  scatter_factors(c, 1, scat);
+  int rc = adjoint_series(c, stop, terms);
+  if (rc) return rc;
+  CUDA_TRY(c, (c->launches++, rte_launch_y_field(c->d_y, c->d_e, c->d_lam, c->d_mus, scat, c->N, c->L, c->C, c->st)));
+  // back-projection through exp(-tau), pass 1: this source's weight of every unordered pair, summed
+  // over the sources in the pair-weight buffer
+  BpArgs bp = bp_args(c, !first);
+  {
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, (c->launches++, rte_launch_bp_weights(bp, c->L, mixed ? 0 : 1, c->st)));
+  }
+  GradLocalArgs gl;
+  memset(&gl, 0, sizeof gl);
+  gl.N = c->N;
+  gl.Cfull = c->C;
+  gl.Cact = c->C;
+  gl.y = c->d_y;
+  gl.lam = c->d_lam;
+  gl.S = c->d_S;
+  gl.out = c->d_out;
+  gl.mus = c->d_mus;
+  gl.mut = c->d_mut;
+  gl.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
+  gl.dlut = c->d_dlut;
+  gl.mom = c->d_mom;
+  gl.K = c->K;
+  gl.scale = c->dV / c->cm;
+  gl.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
+  for (int l = 0; l <= RTE_MAX_L; l++) gl.scat[l] = scat[l];
+  gl.gt = c->d_gt;
+  gl.gs = c->d_gs;
+  CUDA_TRY(c, (c->launches++, rte_launch_grad_local(gl, c->st)));
+  // source column and ballistic transmission (host; nz voxels)
+  std::vector<int> cols;
+  double scale;
+  if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source");
+  for (int col : cols) {
+    const int nz = c->nz, plane = c->nx * c->ny;
+    std::vector<double> lamc((size_t)nz * c->C);
+    for (int i = 0; i < nz; i++)
+      CUDA_TRY(c, cudaMemcpyAsync(&lamc[(size_t)i * c->C], c->d_lam + ((size_t)i * plane + col) * c->C,
+                                  c->C * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CUDA_TRY(c, cudaStreamSynchronize(c->st));
+    std::vector<double> X(nz), Lam(nz), Tt(nz), E(nz);
+    double att = 1.0;
+    for (int i = 0; i < nz; i++) {
+      const int r = i * plane + col;
+      E[i] = exp(-mut[r] * c->dz);
+      Tt[i] = att;
+      att *= E[i];
+      double lam = 0.0, gl2 = 1.0;
+      for (int l = 0; l <= c->L; l++) {
+        lam += lamc[(size_t)i * c->C + l * l + l] * scale * gl2 * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) / c->dV;
+        gl2 *= c->cfg.g;
+      }
+      Lam[i] = lam;
+      X[i] = (mus[r] / mut[r]) * Tt[i] * (1 - E[i]);
+    }
+    double tail = 0.0;  // sum_{i' > i} Lam X
+    const double ball = s->mag * att;
+    for (int i = nz - 1; i >= 0; i--) {
+      const int r = i * plane + col;
+      const double mt = mut[r], ms = mus[r], ma = mt - ms;
+      const double common = (ms / mt) * Tt[i] * c->dz * E[i];
+      ga[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (-ms / (mt * mt)) + common) - c->dz * tail - rho_ball * ball * c->dz;
+      gsum[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (ma / (mt * mt)) + common) - c->dz * tail - rho_ball * ball * c->dz;
+      tail += Lam[i] * X[i];
+    }
+  }
+  return RTE_OK;
+}
+
+// Pass 2 of the back-projection, then the per-voxel gradient g_mua = g_t + ga, g_mus = g_t + g_s + gsum.
+static int adjoint_finish(rte_ctx* c, const std::vector<double>& ga, const std::vector<double>& gsum, double* g_mua,
+                          double* g_mus) {
+  {
+    const BpArgs bp = bp_args(c, true);
+    ProfScope ps(c, 0);
+    CUDA_TRY(c, (c->launches++, rte_launch_bp_walk(bp, c->precision == RTE_PREC_MIXED ? 0 : 1, c->st)));
+  }
+  std::vector<double> gt(c->N), gs(c->N);
+  CUDA_TRY(c, cudaMemcpyAsync(gt.data(), c->d_gt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(gs.data(), c->d_gs, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+  CUDA_TRY(c, cudaStreamSynchronize(c->st));
+  int rc = check_kernel_err(c);
+  if (rc) return rc;
+  for (int r = 0; r < c->N; r++) {
+    g_mua[r] = gt[r] + ga[r];
+    g_mus[r] = gt[r] + gs[r] + gsum[r];
+  }
+  return RTE_OK;
+}
+
+static int gradient_sources_ok(rte_ctx* c, int nsrc, const rte_source* srcs) {
+  if (c->split)
+    return fail(c, RTE_ERR_UNSUPPORTED, "the exact derivative needs one tissue table (rte_set_medium_tissue_split)");
+  if (c->model == RTE_MODEL_FIM)
+    return fail(c, RTE_ERR_UNSUPPORTED,
+                "the exact derivative is not available for the table model (RTE_MODEL_FIM): its back-projection "
+                "uses exact directions; use RTE_DERIV_REFERENCE or RTE_MODEL_EXACT");
+  for (int q = 0; q < nsrc && srcs; q++)
+    if (srcs[q].kind != RTE_SRC_COLUMN && srcs[q].kind != RTE_SRC_FIM &&
+        !(srcs[q].kind == RTE_SRC_BEAM && srcs[q].face == 0))
+      return fail(c, RTE_ERR_UNSUPPORTED, "the gradient takes collimated sources on the z = 0 face");
+  return RTE_OK;
+}
+
+static int gradient_setup(rte_ctx* c, std::vector<double>& mut, std::vector<double>& mus) {
+  mut.resize(c->N);
+  mus.resize(c->N);
+  CUDA_TRY(c, cudaMemsetAsync(c->d_gt, 0, sizeof(double) * c->N, c->st));
+  CUDA_TRY(c, cudaMemsetAsync(c->d_gs, 0, sizeof(double) * c->N, c->st));
+  CUDA_TRY(c, cudaMemcpy(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, cudaMemcpy(mus.data(), c->d_mus, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
+  return ensure_bp_buffer(c);
+}
+
 extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const rte_stop* stop,
                             const rte_detector* d, const double* target, double* loss, double* g_mua,
                             double* g_mus) {
   if (!c || !target || !g_mua || !g_mus) return fail(c, RTE_ERR_ARG, "null argument");
   if (c->kappa != 0.0) return unsupported_modulated(c, "the adjoint gradient");
-  for (int q = 0; q < nsrc && srcs; q++)
-    if (srcs[q].kind != RTE_SRC_COLUMN && srcs[q].kind != RTE_SRC_FIM &&
-        !(srcs[q].kind == RTE_SRC_BEAM && srcs[q].face == 0))
-      return fail(c, RTE_ERR_UNSUPPORTED, "the gradient takes collimated sources on the z = 0 face");
-  int rc = check_detector(c, nsrc, srcs, stop, d);
+  int rc = gradient_sources_ok(c, nsrc, srcs);
   if (rc) return rc;
-  const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
+  rc = check_detector(c, nsrc, srcs, stop, d);
+  if (rc) return rc;
+  const size_t np = (size_t)c->nx * c->ny;
   const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
   const int nb = d->nbins;
-  const bool mixed = c->precision == RTE_PREC_MIXED;
   std::vector<double> J(npix), rho(npix), bins(6 * nb * nb), dbins(6 * nb * nb);
-  std::vector<double> ga(c->N, 0.0), gsum(c->N, 0.0);
-  CUDA_TRY(c, cudaMemsetAsync(c->d_gt, 0, sizeof(double) * c->N, c->st));
-  CUDA_TRY(c, cudaMemsetAsync(c->d_gs, 0, sizeof(double) * c->N, c->st));
-  double L2 = 0.0;
-  double scat[RTE_MAX_L + 1];
-  scatter_factors(c, 1, scat);
-  std::vector<double> mut(c->N), mus(c->N);
-  CUDA_TRY(c, cudaMemcpy(mut.data(), c->d_mut, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
-  CUDA_TRY(c, cudaMemcpy(mus.data(), c->d_mus, sizeof(double) * c->N, cudaMemcpyDeviceToHost));
-  rc = ensure_bp_buffer(c);
+  std::vector<double> ga(c->N, 0.0), gsum(c->N, 0.0), mut, mus;
+  rc = gradient_setup(c, mut, mus);
   if (rc) return rc;
+  double L2 = 0.0;
   for (int sidx = 0; sidx < nsrc; sidx++) {
     const rte_source* s = &srcs[sidx];
     int terms = 0;
@@ -2347,7 +2579,7 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
       }
     unbin_faces(c, d, dbins.data(), rho);
     CUDA_TRY(c, cudaMemcpyAsync(c->d_rho, rho.data(), npix * sizeof(double), cudaMemcpyHostToDevice, c->st));
-    CUDA_TRY(c, cudaMemsetAsync(c->d_e, 0, NC * sizeof(double), c->st));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_e, 0, (size_t)c->N * c->C * sizeof(double), c->st));
     FaceArgs fa;
     memset(&fa, 0, sizeof fa);
     fa.nx = c->nx;
@@ -2359,100 +2591,101 @@ extern "C" int rte_gradient(rte_ctx* c, int nsrc, const rte_source* srcs, const 
     fa.rho = c->d_rho;
     fa.e = c->d_e;
     CUDA_TRY(c, (c->launches++, rte_launch_adjoint_seed(fa, c->st)));
-    // adjoint series
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_aux3, c->d_e, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-    CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_aux3, c->N, c->L, c->C, c->st)));
-    if (mixed)
-      CUDA_TRY(c, (c->launches++, rte_launch_to_f32_slots(c->d_aux3, c->d_Wf, c->d_islot, c->N, c->C, c->cpad, c->C,
-                                                          c->cstride, c->st)));
-    rc = apply_term(c, c->d_aux3, c->d_Wf, c->d_aux4, nullptr, nullptr, 1, 1);
-    if (rc) return rc;
-    CUDA_TRY(c, (c->launches++, rte_launch_axpy(c->d_aux3, c->d_aux4, 1.0, NC, c->st)));
-    rc = neumann_real(c, c->d_aux4, c->d_aux3, c->d_lam, 1, stop, std::max(terms - 1, 0), nullptr, nullptr);
-    if (rc) return rc;
-    CUDA_TRY(c, (c->launches++, rte_launch_parity(c->d_lam, c->N, c->L, c->C, c->st)));
-    CUDA_TRY(c, (c->launches++, rte_launch_y_field(c->d_y, c->d_e, c->d_lam, c->d_mus, scat, c->N, c->L, c->C, c->st)));
-    // back-projection through exp(-tau), pass 1: this source's weight of every unordered pair,
-    // summed over the sources in the pair-weight buffer (pass 2, the walk, follows the loop)
-    BpArgs bp = bp_args(c, sidx > 0);
-    {
-      ProfScope ps(c, 0);
-      CUDA_TRY(c, (c->launches++, rte_launch_bp_weights(bp, c->L, mixed ? 0 : 1, c->st)));
-    }
-    GradLocalArgs gl;
-    memset(&gl, 0, sizeof gl);
-    gl.N = c->N;
-    gl.Cfull = c->C;
-    gl.Cact = c->C;
-    gl.y = c->d_y;
-    gl.lam = c->d_lam;
-    gl.S = c->d_S;
-    gl.out = c->d_out;
-    gl.mus = c->d_mus;
-    gl.mut = c->d_mut;
-    gl.idx = c->self_lut_ok ? c->d_self_idx : nullptr;
-    gl.dlut = c->d_dlut;
-    gl.mom = c->d_mom;
-    gl.K = c->K;
-    gl.scale = c->dV / c->cm;
-    gl.air_no_self = c->model == RTE_MODEL_FIM ? 1 : 0;
-    for (int l = 0; l <= RTE_MAX_L; l++) gl.scat[l] = scat[l];
-    gl.gt = c->d_gt;
-    gl.gs = c->d_gs;
-    CUDA_TRY(c, (c->launches++, rte_launch_grad_local(gl, c->st)));
-    // source column and ballistic transmission (host; nz voxels)
     std::vector<int> cols;
     double scale;
-    if (source_columns(c, s, cols, scale)) return fail(c, RTE_ERR_ARG, "bad source");
-    for (int col : cols) {
-      const int nz = c->nz, plane = c->nx * c->ny;
-      std::vector<double> lamc((size_t)nz * c->C);
-      for (int i = 0; i < nz; i++)
-        CUDA_TRY(c, cudaMemcpyAsync(&lamc[(size_t)i * c->C], c->d_lam + ((size_t)i * plane + col) * c->C,
-                                    c->C * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-      CUDA_TRY(c, cudaStreamSynchronize(c->st));
-      std::vector<double> X(nz), Lam(nz), Tt(nz), E(nz);
-      double att = 1.0;
-      for (int i = 0; i < nz; i++) {
-        const int r = i * plane + col;
-        E[i] = exp(-mut[r] * c->dz);
-        Tt[i] = att;
-        att *= E[i];
-        double lam = 0.0, gl2 = 1.0;
-        for (int l = 0; l <= c->L; l++) {
-          lam += lamc[(size_t)i * c->C + l * l + l] * scale * gl2 * sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) / c->dV;
-          gl2 *= c->cfg.g;
-        }
-        Lam[i] = lam;
-        X[i] = (mus[r] / mut[r]) * Tt[i] * (1 - E[i]);
-      }
-      double tail = 0.0;  // sum_{i' > i} Lam X
-      const double ball = s->mag * att;
-      const double rho_b = rho[np + (size_t)col];  // z+ face pixel of this column
-      for (int i = nz - 1; i >= 0; i--) {
-        const int r = i * plane + col;
-        const double mt = mut[r], ms = mus[r], ma = mt - ms;
-        const double common = (ms / mt) * Tt[i] * c->dz * E[i];
-        ga[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (-ms / (mt * mt)) + common) - c->dz * tail - rho_b * ball * c->dz;
-        gsum[r] += Lam[i] * (Tt[i] * (1 - E[i]) * (ma / (mt * mt)) + common) - c->dz * tail - rho_b * ball * c->dz;
-        tail += Lam[i] * X[i];
-      }
-    }
+    source_columns(c, s, cols, scale);
+    const double rho_b = cols.empty() ? 0.0 : rho[np + (size_t)cols[0]];  // z+ face pixel of the column
+    rc = adjoint_source_terms(c, s, stop, terms, rho_b, sidx == 0, mut, mus, ga, gsum);
+    if (rc) return rc;
   }
-  {  // back-projection pass 2: one walk of every unordered pair for all sources together
-    const BpArgs bp = bp_args(c, true);
-    ProfScope ps(c, 0);
-    CUDA_TRY(c, (c->launches++, rte_launch_bp_walk(bp, mixed ? 0 : 1, c->st)));
-  }
-  std::vector<double> gt(c->N), gs(c->N);
-  CUDA_TRY(c, cudaMemcpyAsync(gt.data(), c->d_gt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
-  CUDA_TRY(c, cudaMemcpyAsync(gs.data(), c->d_gs, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
-  CUDA_TRY(c, cudaStreamSynchronize(c->st));
-  rc = check_kernel_err(c);
+  rc = adjoint_finish(c, ga, gsum, g_mua, g_mus);
   if (rc) return rc;
-  for (int r = 0; r < c->N; r++) {
-    g_mua[r] = gt[r] + ga[r];
-    g_mus[r] = gt[r] + gs[r] + gsum[r];
+  if (loss) *loss = L2;
+  return RTE_OK;
+}
+
+// Gradient of the reference's image misfit sum_j (gbar_j - g_j)^2 (compute_grad_rte.cu:314-315,
+// 376-377; GPU package/src/inverse_rte.cu:365, 425) from one forward and one adjoint series.
+extern "C" int rte_image_gradient(rte_ctx* c, const rte_source* s, const rte_stop* stop, int image, int deriv,
+                                  const double* g, double* loss, double* g_mua, double* g_mus) {
+  if (!c || !s || !stop || !g || !g_mua || !g_mus) return fail(c, RTE_ERR_ARG, "null argument");
+  if (image != 0 && image != 1) return fail(c, RTE_ERR_ARG, "image must be 0 (transmission) or 1 (reflection)");
+  if (deriv != RTE_DERIV_EXACT && deriv != RTE_DERIV_REFERENCE) return fail(c, RTE_ERR_ARG, "bad derivative model");
+  if (c->kappa != 0.0 || s->modulation != 0.0) return unsupported_modulated(c, "the image gradient");
+  if (!c->medium_set) return fail(c, RTE_ERR_STATE, "medium not set");
+  if (stop->rule == RTE_STOP_REFERENCE && deriv == RTE_DERIV_EXACT)
+    return fail(c, RTE_ERR_UNSUPPORTED, "the exact derivative takes a fixed or relative-L2 stop rule");
+  int rc = deriv == RTE_DERIV_EXACT ? gradient_sources_ok(c, 1, s) : RTE_OK;
+  if (rc) return rc;
+  CUDA_TRY(c, cudaSetDevice(c->cfg.device));
+  rc = ensure_detector_buffers(c);
+  if (rc) return rc;
+  const size_t np = (size_t)c->nx * c->ny, NC = (size_t)c->N * c->C;
+  std::vector<double> ga(c->N, 0.0), gsum(c->N, 0.0), mut, mus;
+  if (deriv == RTE_DERIV_EXACT) {
+    rc = gradient_setup(c, mut, mus);
+    if (rc) return rc;
+  }
+  // forward solve: S in d_S, out = A S in d_out, the image with its ballistic term
+  const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
+  std::vector<double> J(npix);
+  int terms = 0;
+  if (s->kind == RTE_SRC_CPU) {  // several columns: the flux path takes single-column sources
+    c->has_point = false;
+    rc = launch_source(c, s, c->d_aux1, 0, nullptr, true, c->d_q);
+    if (!rc) rc = series_start(c, c->d_aux1, c->d_q, c->d_aux3, 1, c->d_Wf, c->cpad);
+    if (!rc) rc = neumann_real(c, c->d_aux3, c->d_aux1, c->d_out, 1, stop, -1, &terms, nullptr);
+    if (!rc) CUDA_TRY(c, cudaMemcpyAsync(c->d_S, c->d_sum, NC * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  } else {
+    rc = forward_with_flux(c, s, stop, J, &terms);
+  }
+  if (rc) return rc;
+  std::vector<rte_cplx> gbar(np);
+  rc = run_images(c, c->d_out, s, true, image == 0 ? gbar.data() : nullptr, image == 1 ? gbar.data() : nullptr);
+  if (rc) return rc;
+  // seed e = M^T rho on the image's voxel layer, rho_j = 2 (gbar_j - g_j), M the per-l image weights
+  ImgArgs wts;
+  rc = image_weights(c, s, wts);
+  if (rc) return rc;
+  const double* w = image == 0 ? wts.wt : wts.wr;
+  std::vector<double> rho(np), layer(np * c->C, 0.0);
+  double L2 = 0.0;
+  for (size_t j = 0; j < np; j++) {
+    const double e = gbar[j].re - g[j];
+    L2 += e * e;
+    rho[j] = 2.0 * e;
+    for (int l = 0; l <= c->L; l++) layer[j * c->C + l * l + l] = w[l] * rho[j];
+  }
+  const size_t layer_off = image == 0 ? (size_t)(c->nz - 1) * np : 0;
+  CUDA_TRY(c, cudaMemsetAsync(c->d_e, 0, NC * sizeof(double), c->st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_e + layer_off * c->C, layer.data(), layer.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, c->st));
+  if (deriv == RTE_DERIV_REFERENCE) {
+    // the reference's tangent sources -C dmu_a out and (-C + g^l) dmu_s out (C = 1, rte.h:15) paired
+    // with the adjoint field: d loss / d mu(r) = <lambda_r, source_r>
+    rc = adjoint_series(c, stop, terms);
+    if (rc) return rc;
+    double fa[RTE_MAX_L + 1], fs[RTE_MAX_L + 1];
+    for (int l = 0; l <= RTE_MAX_L; l++) {
+      fa[l] = -1.0;
+      fs[l] = -1.0 + pow(c->cfg.g, (double)l);
+    }
+    CUDA_TRY(c, (c->launches++, rte_launch_tangent_pair_dots(c->d_lam, c->d_out, fa, fs, c->N, c->L, c->d_gt, c->d_gs,
+                                                              c->st)));
+    CUDA_TRY(c, cudaMemcpyAsync(g_mua, c->d_gt, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+    CUDA_TRY(c, cudaMemcpyAsync(g_mus, c->d_gs, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->st));
+    CUDA_TRY(c, cudaStreamSynchronize(c->st));
+    rc = check_kernel_err(c);
+    if (rc) return rc;
+  } else {
+    std::vector<int> cols;
+    double scale;
+    source_columns(c, s, cols, scale);
+    // the ballistic beam reaches the transmission image at its column's pixel (dist.cu:137-145)
+    const double rho_b = (image == 0 && !cols.empty()) ? rho[(size_t)cols[0]] : 0.0;
+    rc = adjoint_source_terms(c, s, stop, terms, rho_b, true, mut, mus, ga, gsum);
+    if (!rc) rc = adjoint_finish(c, ga, gsum, g_mua, g_mus);
+    if (rc) return rc;
   }
   if (loss) *loss = L2;
   return RTE_OK;
@@ -2470,7 +2703,7 @@ static std::vector<uintptr_t> graph_signature(const rte_ctx* c, int nb) {
   return {u(std::min(W, Wn)), u(std::max(W, Wn)), u(nb == 1 ? c->d_sum : c->d_bsum),
           u(nb == 1 ? c->d_aux2 : c->d_bres), u(nb == 1 ? (const void*)c->d_Wf : (const void*)c->d_bWf),
           u(c->d_part), u(c->d_selfp), u(c->d_self_idx), u(c->d_self_lut), u(c->d_mom), (uintptr_t)c->K,
-          (uintptr_t)c->self_lut_ok, u(c->d_K), (uintptr_t)c->Kld, u(c->d_mut), u(c->d_mutf), u(c->d_mus),
+          (uintptr_t)c->self_lut_ok, u(c->d_K), u(c->d_K64), (uintptr_t)c->Kld, u(c->d_mut), u(c->d_mutf), u(c->d_mus),
           u(c->d_red), u(c->d_err), (uintptr_t)c->bcap, (uintptr_t)(fft_eligible(c) && !c->fft_graph_failed),
           rte_fft_signature(c->fft)};
 }
@@ -2824,6 +3057,7 @@ static int tangent_dA(rte_ctx* c, const double* d_in, double* d_outT, const std:
   PairArgs a = pair_args(c, d_in, nullptr, 1, S, split_chunk(c->N, S));
   a.nsplit = (c->N + a.chunk - 1) / a.chunk;
   a.Kmat = c->K_valid && c->d_K ? c->d_K : nullptr;
+  a.Kmat64 = c->K_valid && c->d_K64 ? c->d_K64 : nullptr;
   a.islot = c->d_islot;
   a.dmut = c->d_dmut;
   for (int q = 0; q < 3; q++) {
@@ -2879,6 +3113,8 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
                           int P, const double* dmua, const double* dmus, double* J, double* F) {
   if (!c || P < 1 || !dmua || !dmus || !F) return fail(c, RTE_ERR_ARG, "null argument");
   if (c->kappa != 0.0) return unsupported_modulated(c, "the Fisher information");
+  if (c->split)
+    return fail(c, RTE_ERR_UNSUPPORTED, "the Fisher information needs one tissue table (rte_set_medium_tissue_split)");
   int rc = check_detector(c, nsrc, srcs, stop, d);
   if (rc) return rc;
   for (int q = 0; q < nsrc; q++)

@@ -20,6 +20,7 @@ struct PairArgs {
   const double* Win;    // current term, real basis, N x Cfull, FP64
   const float* Winf;    // current term, FP32 copy in slot order, coefficient c times N_c (sh_eval_monic)
   float* Kmat;          // stored pair kernel [source slot][destination slot], row stride Kld
+  double* Kmat64;       // the same in FP64 (plain FP64 method with a stored kernel)
   size_t Kld;
   double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
   int chunk;            // source voxels per blockIdx.y
@@ -37,6 +38,10 @@ struct PairArgs {
   // intensity modulation: mu_t has the uniform imaginary part kappa, so every pair kernel gains the
   // phase exp(-i kappa |r - r'|); the right-hand sides are complex, (real, imaginary) pairs of rows
   double kappa;
+  // transposed operator of the table model: each pair's table direction is snapped from the reverse
+  // displacement (source minus destination).  Snapping does not commute with negation, so for the
+  // FisherInfo_IO table A^T != P A P; with exact SH the parity form is used instead.
+  int transpose;
 };
 
 struct EpiArgs {
@@ -132,6 +137,7 @@ struct BpArgs {
   const double* y;     // destination-side field [N][Cfull] (voxel order)
   const double* S;     // source-side field [N][Cfull] (voxel order)
   const float* Kmat;   // stored pair kernel (null: recompute the path integral)
+  const double* Kmat64;  // FP64 stored pair kernel (FP64 contexts in stored-kernel mode)
   size_t Kld;
   double* g;           // gradient w.r.t. mu_t, accumulated [N]
   int use_smem;        // per-CTA private accumulator of N entries in shared memory (set by the launcher)
@@ -163,6 +169,9 @@ cudaError_t rte_launch_face_flux(const FaceArgs& a, cudaStream_t st);
 cudaError_t rte_launch_adjoint_seed(const FaceArgs& a, cudaStream_t st);
 cudaError_t rte_launch_parity(double* x, int N, int L, int vstride, cudaStream_t st);
 cudaError_t rte_launch_axpy(double* y, const double* x, double alpha, size_t n, cudaStream_t st);
+// ga[r] = sum_c fa[l] lam[r][c] out[r][c], gs[r] likewise with fs (N voxels, rows of (L+1)^2)
+cudaError_t rte_launch_tangent_pair_dots(const double* lam, const double* out, const double* fa, const double* fs, int N,
+                                         int L, double* ga, double* gs, cudaStream_t st);
 cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, const double* mus, const double* scat,
                                int N, int L, int Cfull, cudaStream_t st);
 // Symmetric back-projection in two passes: pair weights of one source added into Q, then one walk
@@ -215,7 +224,8 @@ void rte_fft_destroy(FftState* s);
 ShTables make_sh_tables();
 void sh_real_host(const ShTables& t, int L, double x, double y, double z, double* R);
 cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table, int stored, cudaStream_t st);
-cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st);
+// fp64 = 1: FP64 path sums and exp into a.Kmat64; else FP32 into a.Kmat
+cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st, int fp64 = 0);
 cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm,
                                int cplx = 0);
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);

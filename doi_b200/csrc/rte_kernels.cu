@@ -295,12 +295,16 @@ __device__ __forceinline__ A path_sum(int i, int j, int k, int ip, int jp, int k
 // Plain FP64 method: every pair recomputed in FP64 (path integral, SH, projections).  CPLX: one
 // complex right-hand side stored as (real, imaginary) rows per voxel, and the pair kernel carries the
 // modulation phase exp(-i kappa |r - r'|) (complex mu_t = mu_t + i kappa, uniform imaginary part).
-template <int LA, bool TABLE, bool CPLX>
+// STORED: the pair kernel exp(-tau) dV/(cm r^2) is read from the FP64 matrix Kmat64[source slot]
+// [destination slot] instead of walking the path; sources are then visited in slot order, so the
+// warp's 32 destinations read one contiguous 256-byte run of K per source.
+template <int LA, bool TABLE, bool CPLX, bool STORED = false>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
   constexpr int NP = CPLX ? 2 : 1;        // rows per voxel
   constexpr int TS = RTE_PAIR_TS / NP;    // sources per shared-memory tile
   __shared__ double sW[TS * NP * C];
+  __shared__ int sxyz[STORED ? TS : 1][3];  // source coordinates (slot order)
   const int tid = threadIdx.x;
   const int slot = blockIdx.x * RTE_PAIR_THREADS + tid;
   const bool act = slot < a.N;
@@ -320,10 +324,66 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
     __syncthreads();
     for (int q = tid; q < ns * NP * C; q += RTE_PAIR_THREADS) {
       const int sv = q / (NP * C), e = q - sv * NP * C, p = e / C, c = e - p * C;
-      sW[q] = a.Win[(size_t)(s0 + sv) * vs + (size_t)p * a.Cfull + c];
+      const int src = STORED ? a.perm[s0 + sv] : s0 + sv;
+      sW[q] = a.Win[(size_t)src * vs + (size_t)p * a.Cfull + c];
+    }
+    if (STORED && tid < ns) {
+      const int v = a.perm[s0 + tid];
+      sxyz[tid][0] = v % a.nx;
+      sxyz[tid][1] = (v / a.nx) % a.ny;
+      sxyz[tid][2] = v / plane;
     }
     __syncthreads();
     if (!act) continue;
+    if constexpr (STORED) {
+      const double* Kcol = a.Kmat64 + (size_t)s0 * a.Kld + slot;
+      double knext = __ldg(Kcol);
+      for (int sv = 0; sv < ns; ++sv) {
+        const double kk = knext;
+        if (sv + 1 < ns) knext = __ldg(Kcol + (size_t)(sv + 1) * a.Kld);
+        if (kk == 0.0) continue;  // the diagonal and pairs beyond the coupling distance
+        const double ddx = (double)(k - sxyz[sv][0]) * a.dx, ddy = (double)(j - sxyz[sv][1]) * a.dy,
+                     ddz = (double)(i - sxyz[sv][2]) * a.dz;
+        const double dist = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+        double ux, uy, uz;
+        if (TABLE) {
+          // A^T: snap(source - destination), negated in integers so that a zero component stays +0.0 (the
+          // table's unwrapped phi index depends on atan2's sign of zero) -- the forward kernel's exact bits
+          const int sg = a.transpose ? -1 : 1;
+          table_direction((double)(sg * (k - sxyz[sv][0])) * a.dx, (double)(sg * (j - sxyz[sv][1])) * a.dy,
+                          (double)(sg * (i - sxyz[sv][2])) * a.dz, dist, ux, uy, uz);
+        } else {
+          const double inv = 1.0 / dist;
+          ux = ddx * inv;
+          uy = ddy * inv;
+          uz = ddz * inv;
+        }
+        double R[C];
+        sh_eval<LA, double>(ux, uy, uz, R);
+        double S[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          S[p] = 0.0;
+#pragma unroll
+          for (int c = 0; c < C; ++c) S[p] = fma(R[c], sW[(sv * NP + p) * C + c], S[p]);
+        }
+        if (CPLX) {
+          double sn, cs;
+          sincos(a.kappa * dist, &sn, &cs);
+          const double t0 = kk * (cs * S[0] + sn * S[NP - 1]), t1 = kk * (cs * S[NP - 1] - sn * S[0]);
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            acc[0][c] = fma(R[c], t0, acc[0][c]);
+            acc[NP - 1][c] = fma(R[c], t1, acc[NP - 1][c]);
+          }
+        } else {
+          const double t = kk * S[0];
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[0][c] = fma(R[c], t, acc[0][c]);
+        }
+      }
+      continue;
+    }
     int kp = s0 % a.nx, jp = (s0 / a.nx) % a.ny, ip = s0 / plane;
     for (int sv = 0; sv < ns; ++sv) {
       const int rp = s0 + sv;
@@ -334,7 +394,10 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_fp64(PairArgs a) {
         if (dist < a.prop_thresh) {
           double ux, uy, uz;
           if (TABLE) {
-            table_direction(ddx, ddy, ddz, dist, ux, uy, uz);
+            // A^T: snap(source - destination), negated in integers (a zero component stays +0.0)
+            const int sg = a.transpose ? -1 : 1;
+            table_direction((double)(sg * (k - kp)) * a.dx, (double)(sg * (j - jp)) * a.dy,
+                            (double)(sg * (i - ip)) * a.dz, dist, ux, uy, uz);
           } else {
             const double inv = 1.0 / dist;
             ux = ddx * inv;
@@ -457,7 +520,9 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
           if (dps != T(0)) {
             const T dtau = dps * dist / (T)Q;
             T kk;
-            if (a.Kmat) {
+            if (a.Kmat64) {
+              kk = (T)__ldg(a.Kmat64 + (size_t)a.islot[rp] * a.Kld + slot);
+            } else if (a.Kmat) {
               kk = (T)__ldg(a.Kmat + (size_t)a.islot[rp] * a.Kld + slot);
             } else {
               int Q2;
@@ -676,11 +741,13 @@ __device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
         if (live) {
           ShT R[C];
           if (TABLE) {
-            const double ex = (double)(k - (int)q.x) * a.dx, ey = (double)(j - (int)q.y) * a.dy,
-                         ez = (double)(i - (int)q.z) * a.dz;
+            // A^T: snap(source - destination), negated in integers (a zero component stays +0.0)
+            const int sg = a.transpose ? -1 : 1;
+            const double ex = (double)(sg * (k - (int)q.x)) * a.dx, ey = (double)(sg * (j - (int)q.y)) * a.dy,
+                         ez = (double)(sg * (i - (int)q.z)) * a.dz;
             double ux, uy, uz;
             table_direction(ex, ey, ez, sqrt(ex * ex + ey * ey + ez * ez), ux, uy, uz);
-            sh_eval_monic<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);
+            sh_eval_monic<LA, ShT>((ShT)ux, (ShT)uy, (ShT)uz, R);  // A^T: snap(source - destination)
           } else {
             const float inv = FLAT ? (d2 > 0.f ? rsqrtf(d2) : 0.f) : rsqrtf(d2);
             sh_eval_monic<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
@@ -774,12 +841,15 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS, 3) k_pair_mixed_3(PairArgs a
 }
 
 // Pair-kernel precompute K[s][d] = exp(-tau) dV/(cm |r_d - r_s|^2) over destination slots d and
-// source slots s (0 on the diagonal and beyond propThresh), path sums in FP32.  K is symmetric: one
-// CTA computes a 64x64 tile with source tile index <= destination tile index into shared memory
-// and writes it and its transpose with coalesced stores (a diagonal tile once).
+// source slots s (0 on the diagonal and beyond propThresh), path sums in FP32 (T = float, into Kmat)
+// or FP64 (T = double, into Kmat64, for the FP64 method).  K is symmetric: one CTA computes a 64x64
+// tile with source tile index <= destination tile index into shared memory and writes it and its
+// transpose with coalesced stores (a diagonal tile once).
 #define RTE_KT 64
+template <typename T>
 __global__ void __launch_bounds__(RTE_KT) k_store_kernel(PairArgs a) {
-  __shared__ float tile[RTE_KT][RTE_KT + 1];
+  constexpr bool F64 = std::is_same<T, double>::value;
+  __shared__ T tile[RTE_KT][RTE_KT + 1];
   __shared__ int sxyz[RTE_KT][3];
   const int ntile = (a.N + RTE_KT - 1) / RTE_KT;
   // linear CTA index -> (bs, bd) with bs <= bd, row-major over the upper triangle
@@ -804,35 +874,45 @@ __global__ void __launch_bounds__(RTE_KT) k_store_kernel(PairArgs a) {
   if (d < a.N) {
     const int r = a.perm[d];
     const int k = r % a.nx, j = (r / a.nx) % a.ny, i = r / plane;
-    const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
-    const float kscalef = (float)a.kscale, thr = (float)a.prop_thresh;
+    const T dxf = (T)a.dx, dyf = (T)a.dy, dzf = (T)a.dz;
+    const T kscalef = (T)a.kscale, thr = (T)a.prop_thresh;
     for (int q = 0; q < RTE_KT; ++q) {
-      float kk = 0.f;
+      T kk = T(0);
       if (s0 + q < a.N) {
         const int kp = sxyz[q][0], jp = sxyz[q][1], ip = sxyz[q][2];
-        const float ddx = (float)(k - kp) * dxf, ddy = (float)(j - jp) * dyf, ddz = (float)(i - ip) * dzf;
-        const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
-        const float dist = sqrtf(d2);
-        if (d2 > 0.f && dist < thr) {
+        const T ddx = (T)(k - kp) * dxf, ddy = (T)(j - jp) * dyf, ddz = (T)(i - ip) * dzf;
+        const T d2 = fma(ddx, ddx, fma(ddy, ddy, ddz * ddz));
+        const T dist = sqrt(d2);
+        if (d2 > T(0) && dist < thr) {
           int Q;
-          const float ps = path_sum<float, float>(i, j, k, ip, jp, kp, a.mutf, a.nx, plane, Q);
-          kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
+          if constexpr (F64) {
+            const double ps = path_sum<double, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q);
+            kk = exp(-ps * dist / (double)Q) * kscalef / d2;
+          } else {
+            const float ps = path_sum<float, float>(i, j, k, ip, jp, kp, a.mutf, a.nx, plane, Q);
+            kk = __expf(-ps * dist / (float)Q) * kscalef / d2;
+          }
         }
       }
       tile[tid][q] = kk;  // [destination][source]
     }
   }
   __syncthreads();
+  T* Km;
+  if constexpr (F64)
+    Km = a.Kmat64;
+  else
+    Km = a.Kmat;
   // K[s][d]: row = source slot, contiguous over destination slots
   for (int q = 0; q < RTE_KT; ++q) {
     const int sl = s0 + q;
-    if (sl < a.N && d0 + tid < a.N) a.Kmat[(size_t)sl * a.Kld + d0 + tid] = tile[tid][q];
+    if (sl < a.N && d0 + tid < a.N) Km[(size_t)sl * a.Kld + d0 + tid] = tile[tid][q];
   }
   if (bs != bd) {
     // K[d][s]: row = destination slot of this tile, now acting as the source
     for (int q = 0; q < RTE_KT; ++q) {
       const int dl = d0 + q;
-      if (dl < a.N && s0 + tid < a.N) a.Kmat[(size_t)dl * a.Kld + s0 + tid] = tile[q][tid];
+      if (dl < a.N && s0 + tid < a.N) Km[(size_t)dl * a.Kld + s0 + tid] = tile[q][tid];
     }
   }
 }
@@ -1251,6 +1331,26 @@ __global__ void k_masked_scale(const double* in, double* out, const uint8_t* mas
   out[t] = mask[r] ? fac.v[l] * in[t] : 0.0;
 }
 
+// Per voxel: ga[r] = sum_c fa[l(c)] lam[r][c] out[r][c], gs likewise with fs -- the reference's tangent
+// sources (-C out for mu_a, (-C + g^l) out for mu_s, compute_grad_rte.cu:296-299, 343-350) paired with
+// an adjoint field.
+__global__ void k_tangent_pair_dots(const double* lam, const double* out, ScatTab fa, ScatTab fs, int N, int L,
+                                    double* ga, double* gs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  const int C = (L + 1) * (L + 1);
+  const size_t b = (size_t)r * C;
+  double a = 0.0, s = 0.0;
+  for (int l = 0; l <= L; ++l)
+    for (int c = l * l; c < (l + 1) * (l + 1); ++c) {
+      const double p = lam[b + c] * out[b + c];
+      a = fma(fa.v[l], p, a);
+      s = fma(fs.v[l], p, s);
+    }
+  ga[r] = a;
+  gs[r] = s;
+}
+
 __global__ void k_axpy(double* y, const double* x, double alpha, size_t n) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) y[t] = fma(alpha, x[t], y[t]);
@@ -1369,7 +1469,9 @@ __global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
     T w = T(0);
     if (d2 > T(0) && dist < thr) {
       T kk;
-      if (a.Kmat) {
+      if (a.Kmat64) {
+        kk = (T)__ldg(a.Kmat64 + (size_t)sl * a.Kld + d);
+      } else if (a.Kmat) {
         kk = (T)__ldg(a.Kmat + (size_t)sl * a.Kld + d);
       } else {
         int Q0;
@@ -1652,7 +1754,7 @@ static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, i
   if (a.kappa != 0.0) {  // one complex right-hand side (exact SH only)
     if (table || nb != 2) return cudaErrorInvalidValue;
     if (precision == 0) {
-      void (*kern)(PairArgs) = k_pair_fp64<LA, false, true>;
+      void (*kern)(PairArgs) = stored ? k_pair_fp64<LA, false, true, true> : k_pair_fp64<LA, false, true>;
       if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, 0);
       dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
       kern<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
@@ -1661,7 +1763,8 @@ static cudaError_t launch_pair_LA(const PairArgs& a, int precision, int table, i
     return stored ? launch_mixed<LA, false, true, 2, true>(a, st, occ) : launch_mixed<LA, false, false, 2, true>(a, st, occ);
   }
   if (precision == 0) {
-    void (*kern)(PairArgs) = table ? k_pair_fp64<LA, true, false> : k_pair_fp64<LA, false, false>;
+    void (*kern)(PairArgs) = stored ? (table ? k_pair_fp64<LA, true, false, true> : k_pair_fp64<LA, false, false, true>)
+                                    : (table ? k_pair_fp64<LA, true, false> : k_pair_fp64<LA, false, false>);
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, 0);
     dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
     kern<<<grid, RTE_PAIR_THREADS, 0, st>>>(a);
@@ -1703,9 +1806,12 @@ cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int
   return pair_dispatch(dummy, LA, precision, table, stored, nb, nullptr, blocks_per_sm);
 }
 
-cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st) {
+cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st, int fp64) {
   const long long nt = (a.N + RTE_KT - 1) / RTE_KT;
-  k_store_kernel<<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, 0, st>>>(a);
+  if (fp64)
+    k_store_kernel<double><<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, 0, st>>>(a);
+  else
+    k_store_kernel<float><<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1875,6 +1981,17 @@ cudaError_t rte_launch_masked_scale(const double* in, double* out, const uint8_t
 cudaError_t rte_launch_parity(double* x, int N, int L, int vstride, cudaStream_t st) {
   const long long n = (long long)N * (L + 1) * (L + 1);
   k_parity<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, N, L, vstride);
+  return cudaGetLastError();
+}
+
+cudaError_t rte_launch_tangent_pair_dots(const double* lam, const double* out, const double* fa, const double* fs, int N,
+                                         int L, double* ga, double* gs, cudaStream_t st) {
+  ScatTab a, b;
+  for (int l = 0; l <= RTE_MAX_L; ++l) {
+    a.v[l] = l <= L ? fa[l] : 0.0;
+    b.v[l] = l <= L ? fs[l] : 0.0;
+  }
+  k_tangent_pair_dots<<<(N + 127) / 128, 128, 0, st>>>(lam, out, a, b, N, L, ga, gs);
   return cudaGetLastError();
 }
 

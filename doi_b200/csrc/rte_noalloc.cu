@@ -44,29 +44,6 @@ int set_err(int code, const char* msg) {
   return code;
 }
 
-ShTables sh_tables() {
-  // same normalised recurrence as the context path (rte_host.cpp)
-  ShTables t;
-  memset(&t, 0, sizeof t);
-  auto K = [](int l, int m) {
-    double f = 1.0;
-    for (int i = l - m + 1; i <= l + m; i++) f *= (double)i;
-    double k = sqrt((2.0 * l + 1.0) / (4.0 * M_PI) / f);
-    return m > 0 ? k * sqrt(2.0) : k;
-  };
-  for (int m = 0; m <= RTE_MAX_L; m++) {
-    double dfact = 1.0;
-    for (int i = 2 * m - 1; i > 0; i -= 2) dfact *= (double)i;
-    t.Q0[m] = K(m, m) * ((m & 1) ? -1.0 : 1.0) * dfact;
-    for (int l = m + 1; l <= RTE_MAX_L; l++) {
-      int id = l * (l + 1) / 2 + m;
-      t.A[id] = K(l, m) * (2.0 * l - 1.0) / ((double)(l - m) * K(l - 1, m));
-      t.B[id] = (l - 2 >= m) ? K(l, m) * (double)(l + m - 1) / ((double)(l - m) * K(l - 2, m)) : 0.0;
-    }
-  }
-  return t;
-}
-
 // once per device, with that device current: the scratch array's device address and the SH tables
 int setup(int dev, double** out) {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -75,7 +52,7 @@ int setup(int dev, double** out) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return set_err(RTE_ERR_DEVICE, cudaGetErrorString(e));
-    e = rte_upload_sh_tables(sh_tables());
+    e = rte_upload_sh_tables(make_sh_tables());  // the context path's tables (rte_host.cpp)
     if (e != cudaSuccess) return set_err(RTE_ERR_DEVICE, cudaGetErrorString(e));
     g_addr[dev] = (double*)p;
   }

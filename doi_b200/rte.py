@@ -24,6 +24,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 KERNEL_AUTO, KERNEL_STORE, KERNEL_RECOMPUTE = 0, 1, 2
 SRC_COLUMN, SRC_FIM, SRC_CPU, SRC_BEAM, SRC_POINT = 0, 1, 2, 3, 4
 STOP_REFERENCE, STOP_FIXED, STOP_REL_L2 = 0, 1, 2
+DERIV_EXACT, DERIV_REFERENCE = 0, 1
 
 # exported symbols of include/rte_b200.h (checked by the CPU tests)
 EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "rte_set_medium_tissue",
@@ -34,7 +35,8 @@ EXPORTS = ("rte_create", "rte_destroy", "rte_last_error", "rte_device_bytes", "r
            "rte_server_destroy", "rte_par_load", "rte_par_free", "rte_par_get_string", "rte_par_get_int",
            "rte_par_get_double", "rte_par_problem", "rte_problem_free", "rte_write_image", "rte_write_phase_image",
            "rte_read_image", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
-           "rte_cpu_face_outputs", "rte_set_modulation", "rte_downsample_image")
+           "rte_cpu_face_outputs", "rte_set_modulation", "rte_downsample_image", "rte_image_gradient",
+           "rte_set_medium_tissue_split", "rte_prop_abs_adjoint")
 
 
 class RteError(RuntimeError):
@@ -167,6 +169,7 @@ def load_library():
     L.rte_device_bytes.argtypes = [P]
     L.rte_device_bytes.restype = ctypes.c_size_t
     L.rte_set_medium_tissue.argtypes = [P, dp, ctypes.c_int, dp, dp]
+    L.rte_set_medium_tissue_split.argtypes = [P, dp, ctypes.c_int, dp, dp, dp, dp]
     L.rte_set_medium_voxel.argtypes = [P, dp, dp]
     L.rte_set_medium_device.argtypes = [P, dp, dp]
     L.rte_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
@@ -176,6 +179,7 @@ def load_library():
     L.rte_get_stats.argtypes = [P, ctypes.POINTER(_Stats)]
     L.rte_source_beam.argtypes = [P, ctypes.POINTER(_Source), dp]
     L.rte_prop_abs.argtypes = [P, dp, dp, ctypes.c_int, ctypes.c_int]
+    L.rte_prop_abs_adjoint.argtypes = [P, dp, dp, ctypes.c_int]
     L.rte_neumann.argtypes = [P, dp, dp, ctypes.c_int, ctypes.POINTER(_Stop), ctypes.POINTER(ctypes.c_int)]
     L.rte_images.argtypes = [P, dp, ctypes.POINTER(_Source), dp, dp]
     L.rte_forward.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
@@ -184,6 +188,8 @@ def load_library():
                                     ctypes.POINTER(_Detector), dp]
     L.rte_gradient.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop),
                                ctypes.POINTER(_Detector), dp, ctypes.POINTER(ctypes.c_double), dp, dp]
+    L.rte_image_gradient.argtypes = [P, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), ctypes.c_int, ctypes.c_int, dp,
+                                     ctypes.POINTER(ctypes.c_double), dp, dp]
     L.rte_forward_batch.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.POINTER(_Stop), dp, dp, dp,
                                     ctypes.POINTER(_Report)]
     L.rte_forward_graph.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Source), ctypes.c_int, dp, dp,
@@ -322,6 +328,18 @@ class Context:
         self._check(self.lib.rte_set_medium_tissue(self.h, _ptr(tiss), len(a), _ptr(a), _ptr(s)),
                     "rte_set_medium_tissue")
 
+    def set_medium_tissue_split(self, tiss, mua_tab, mus_tab, mua_kernel, mus_kernel):
+        """Tissue map with two tables: the self-voxel term, source and ballistic beam take (mua_tab, mus_tab),
+        the pair kernels and the scatter (mua_kernel, mus_kernel), as in the reference's SNR and
+        region-gradient mains (rte_set_medium_tissue_split)."""
+        tiss = np.ascontiguousarray(tiss, np.uint8).ravel()
+        tabs = [np.ascontiguousarray(t, np.float64) for t in (mua_tab, mus_tab, mua_kernel, mus_kernel)]
+        n = len(tabs[0])
+        if any(len(t) != n for t in tabs):
+            raise ValueError("the four tables must have the same length")
+        self._check(self.lib.rte_set_medium_tissue_split(self.h, _ptr(tiss), n, *[_ptr(t) for t in tabs]),
+                    "rte_set_medium_tissue_split", "rte_prop_abs_adjoint")
+
     def set_modulation(self, modulation):
         """Intensity modulation: mu_a -> mu_a + i*modulation/(c/n) (the reference's [Source] modulation);
         0 restores the steady state.  rte_forward solves at its source's own modulation."""
@@ -341,6 +359,13 @@ class Context:
         W = self._dist(W)
         out = np.zeros_like(W)
         self._check(self.lib.rte_prop_abs(self.h, _ptr(W), _ptr(out), flag, flag_scat), "rte_prop_abs")
+        return out
+
+    def prop_abs_adjoint(self, W, flag=1):
+        """A^H W: the adjoint of prop_abs without scatter (rte_prop_abs_adjoint)."""
+        W = self._dist(W)
+        out = np.zeros_like(W)
+        self._check(self.lib.rte_prop_abs_adjoint(self.h, _ptr(W), _ptr(out), flag), "rte_prop_abs_adjoint")
         return out
 
     def neumann(self, src, out, flag=1, stop=None):
@@ -383,6 +408,21 @@ class Context:
         st, d = stop.c(), det.c()
         self._check(self.lib.rte_gradient(self.h, B, arr, ctypes.byref(st), ctypes.byref(d), _ptr(target),
                                           ctypes.byref(loss), _ptr(ga), _ptr(gs)), "rte_gradient")
+        return loss.value, ga, gs
+
+    def image_gradient(self, src, stop, g, image=0, deriv=DERIV_EXACT):
+        """(loss, dL/dmu_a, dL/dmu_s) for the reference's image misfit loss = sum (gbar - g)^2 of one
+        source's transmission (image=0) or reflection (image=1) image, from one forward and one adjoint
+        series; deriv=DERIV_REFERENCE gives the reference's tangent model (rte_image_gradient)."""
+        g = np.ascontiguousarray(g, np.float64).ravel()
+        if g.size != self.nx * self.ny:
+            raise ValueError("g must hold nX*nY values")
+        ga = np.zeros(self.N)
+        gs = np.zeros(self.N)
+        loss = ctypes.c_double(0.0)
+        s, st = src.c(), stop.c()
+        self._check(self.lib.rte_image_gradient(self.h, ctypes.byref(s), ctypes.byref(st), int(image), int(deriv),
+                                                _ptr(g), ctypes.byref(loss), _ptr(ga), _ptr(gs)), "rte_image_gradient")
         return loss.value, ga, gs
 
     def forward_batch(self, srcs, stop=None, want_W=True, want_images=True):

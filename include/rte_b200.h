@@ -41,8 +41,10 @@ extern "C" {
 #define RTE_PREC_FP64 0  /* plain FP64 method: every pair recomputed in FP64 each term */
 #define RTE_PREC_MIXED 1 /* FP32 path integrals + SH projection, FP64 sums and norms */
 
-#define RTE_KERNEL_AUTO 0      /* store the voxel-pair kernel when it fits, else recompute */
-#define RTE_KERNEL_STORE 1     /* store exp(-tau)/r^2 per voxel pair in HBM (FP32) */
+#define RTE_KERNEL_AUTO 0      /* mixed precision: store the voxel-pair kernel when it fits, else recompute;
+                                  FP64: recompute (the plain method) */
+#define RTE_KERNEL_STORE 1     /* store exp(-tau)/r^2 per voxel pair in HBM (FP32 for mixed precision,
+                                  FP64 for the FP64 method: 8 N^2 bytes) */
 #define RTE_KERNEL_RECOMPUTE 2 /* recompute path integrals every term */
 
 #define RTE_SRC_COLUMN 0 /* collimated pencil on the z=0 face, column containing (pos_x,pos_y) */
@@ -119,6 +121,15 @@ size_t rte_device_bytes(const rte_ctx* ctx);    /* HBM held by this context */
  * mua[0] = mus[0] = 0 in the reference). */
 int rte_set_medium_tissue(rte_ctx* ctx, const uint8_t* tiss, int ntypes, const double* mua,
                           const double* mus);
+/* Two tissue tables on one tissue map (compat form of the FisherInfo_IO SNR and region-gradient mains,
+ * FisherInfo_IO/src/rte_snr.cu:239 and compute_grad_rte.cu:431: they change tissue values on the host but
+ * drop the result of populate_info_dev(), so the device's table keeps the .par values): the pair
+ * kernels' path integrals and the scatter D take mua_kernel / mus_kernel, the self-voxel term, the source
+ * and its ballistic beam take mua / mus.  Forward solves, Neumann, prop_abs, images and the region
+ * derivatives accept it; rte_gradient, rte_image_gradient (exact), rte_fisher and modulation return
+ * RTE_ERR_UNSUPPORTED.  Any other rte_set_medium_* call returns the context to one table. */
+int rte_set_medium_tissue_split(rte_ctx* ctx, const uint8_t* tiss, int ntypes, const double* mua,
+                                const double* mus, const double* mua_kernel, const double* mus_kernel);
 /* Per-voxel form (new): mua, mus of length nX*nY*nZ in cm^-1. */
 int rte_set_medium_voxel(rte_ctx* ctx, const double* mua, const double* mus);
 /* Same with DEVICE pointers (on the context's GPU), for callers whose media are already in HBM. */
@@ -142,6 +153,11 @@ int rte_source_beam(rte_ctx* ctx, const rte_source* src, rte_cplx* xi);
 /* One prop_abs pass (FisherInfo_IO/src/kernels.cu:704-808): out = [D] A in.  flag = 1 uses
  * all orders, flag = 0 only l = 0; flag_scat = 1 applies the scatter D. */
 int rte_prop_abs(rte_ctx* ctx, const rte_cplx* in, rte_cplx* out, int flag, int flag_scat);
+
+/* Adjoint of prop_abs without scatter (new): out = A^H in, so that sum conj(y) (A x) = sum conj(A^H y) x
+ * over all voxels and coefficients.  The adjoint of flag_scat = 1 is A^H D, D the real diagonal scatter.
+ * Not under intensity modulation. */
+int rte_prop_abs_adjoint(rte_ctx* ctx, const rte_cplx* in, rte_cplx* out, int flag);
 
 /* Neumann (FisherInfo_IO/src/neumann.cu:23-120).  flag = 1: W_0 = src, sum_0 = out (the
  * caller passes out = src as rte.cu:148-149 does), W_{k+1} = D A W_k, sum += W_{k+1} until
@@ -181,6 +197,28 @@ int rte_detector_flux(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_
 int rte_gradient(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop,
                  const rte_detector* det, const double* target, double* loss, double* g_mua,
                  double* g_mus);
+
+/* Gradient of the reference's image misfit, loss = sum_j (gbar_j - g_j)^2 over one exitance image of
+ * one source (image 0: the transmission image with its ballistic term, the gbar of
+ * FisherInfo_IO/src/compute_grad_rte.cu:257 and GPU package/src/inverse_rte.cu; 1: the reflection
+ * image), with respect to the per-voxel mu_a and mu_s (N each), from ONE forward and ONE adjoint
+ * Neumann series (new: the reference takes one tangent solve per tissue, or per voxel in the GPU
+ * package).  g: nX*nY target image.  deriv:
+ *   RTE_DERIV_EXACT      the exact derivative of the discrete model, as rte_gradient (collimated z = 0
+ *                        sources; fixed or relative-L2 stop rule);
+ *   RTE_DERIV_REFERENCE  the reference's tangent model: a change of mu in voxel r acts as the source
+ *                        -C dmu_a out(r) (mu_a) or (-C + g^l) dmu_s out(r) (mu_s), C = 1, of a tangent
+ *                        solve whose transmission (or reflection) image without ballistic term is dgbar
+ *                        (compute_grad_rte.cu:288-325, 343-377; per voxel in GPU package/src/
+ *                        inverse_rte.cu:293-433).  g_mua[r] = sum_j 2 (gbar_j - g_j) dgbar_j(r), so
+ *                        av * (sum of g_mua over tissue t) is the reference's grad2[t] (av = 0.01 for
+ *                        mu_a, 1 for mu_s) and g_mua[r] the GPU package's per-voxel grada[r].  The adjoint
+ *                        series takes the forward solve's term count (exact for RTE_STOP_FIXED).
+ * loss may be NULL. */
+#define RTE_DERIV_EXACT 0
+#define RTE_DERIV_REFERENCE 1
+int rte_image_gradient(rte_ctx* ctx, const rte_source* src, const rte_stop* stop, int image, int deriv,
+                       const double* g, double* loss, double* g_mua, double* g_mus);
 
 /* Region derivatives of the reference's inverse main (FisherInfo_IO/src/compute_grad_rte.cu:205-385),
  * one evaluation at the current medium: forward solve, gbar = transmission image; for every tissue

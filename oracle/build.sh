@@ -7,10 +7,14 @@
 #   oracle/_ref/fim_fisher     the same with the Fisher main (rte_fim.cu) as its "program"
 #   oracle/_ref/fim_snr        the same with the SNR main (rte_snr.cu) as its "program"
 #   oracle/_ref/fim_grad       the same with the region-gradient main (compute_grad_rte.cu)
+#   oracle/_ref/fim_shim       the forward main (rte.cu) as a program of its own, with the library's
+#                              Neumann() shim (doi_b200/shim/neumann_b200.cu) in place of neumann.cu:
+#                              the reference's host code around librte_b200 (needs doi_b200/lib built)
 # The reference sources are compiled where they lie; nothing is copied into the repo.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${RTE_REFERENCE_DIR:-/root/reference}"
+# the reference tree: $RTE_REFERENCE_DIR, else a "reference" directory beside the repository
+REF="${RTE_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 CXX="${RTE_CXX:-g++}"
 CC="${RTE_CC:-gcc}"
 
@@ -52,4 +56,17 @@ sed -n '1,418p' "$FIM/kernels.cu" | "$CXX" "${FLAGS[@]}" -c - -o "$OUT/fim/kerne
 "$CXX" -fopenmp -o "$OUT/fim_fisher" "$OUT"/fim/*.o "$OUT/main/rte_fim.o" -lpthread -lm
 "$CXX" -fopenmp -o "$OUT/fim_snr" "$OUT"/fim/*.o "$OUT/main/rte_snr.o" -lpthread -lm
 "$CXX" -fopenmp -o "$OUT/fim_grad" "$OUT"/fim/*.o "$OUT/main/compute_grad_rte.o" -lpthread -lm
-echo "oracle/build.sh: built liboracle.so, _ref/rte_cpu, _ref/fim_host, _ref/fim_fisher, _ref/fim_snr, _ref/fim_grad"
+built="liboracle.so, _ref/rte_cpu, _ref/fim_host, _ref/fim_fisher, _ref/fim_snr, _ref/fim_grad"
+LIB="$HERE/../doi_b200/lib"
+if [ -f "$LIB/librte_b200.so" ]; then
+  mkdir -p "$OUT/shim"
+  "$CXX" "${FLAGS[@]}" -I "$HERE/../include" -c "$HERE/../doi_b200/shim/neumann_b200.cu" -o "$OUT/shim/neumann_b200.o"
+  "$CXX" "${FLAGS[@]}" -c "$FIM/rte.cu" -o "$OUT/shim/rte_main.o"
+  "$CXX" -O2 -std=c++17 -w -D__CUDACC__ -include "$HERE/ref/fim_emu.h" -I "$HERE/ref/include" -I "$FIM" \
+    -c "$HERE/ref/fim_shim_support.cpp" -o "$OUT/shim/support.o"
+  "$CXX" -fopenmp -o "$OUT/fim_shim" "$OUT/shim/rte_main.o" "$OUT/shim/neumann_b200.o" "$OUT/shim/support.o" \
+    "$OUT"/fim/{dist,sph_harm,inits,iniparser,dictionary,kernels}.o -L "$LIB" -lrte_b200 \
+    -Wl,-rpath,'$ORIGIN/../../doi_b200/lib' -lpthread -lm
+  built="$built, _ref/fim_shim"
+fi
+echo "oracle/build.sh: built $built"

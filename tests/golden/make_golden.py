@@ -7,8 +7,8 @@ The reference ships no tests or golden outputs.  This script builds (oracle/buil
   * oracle/_ref/rte_cpu  -- the CPU package built from its own sources;
 on small inputs (.par files written below; tissue maps generated with a fixed seed, plus the two
 20^3 maps shipped in `GPU package/utility/`), and stores the outputs as .npz files.  It needs the
-reference tree (default /root/reference, or $RTE_REFERENCE_DIR); the fixtures it writes are
-committed so the tests run without it.
+reference tree: $RTE_REFERENCE_DIR, else a `reference` directory beside the repository; the
+fixtures it writes are committed so the tests run without it.
 
     python tests/golden/make_golden.py
 """
@@ -21,7 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("RTE_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("RTE_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 
 FIM_PAR = """[Runtime]
 TransFile = trans.out

@@ -59,9 +59,9 @@ def test_noalloc_rejects_bad_arguments_without_device(rte):
     assert b"scratch" in lib.rte_last_error(None)
 
 
-NULL_IS_ERROR = ["rte_set_medium_tissue", "rte_set_medium_voxel", "rte_set_medium_device", "rte_set_modulation",
-                 "rte_source_beam", "rte_prop_abs", "rte_neumann", "rte_images", "rte_forward",
-                 "rte_detector_flux", "rte_gradient", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
+NULL_IS_ERROR = ["rte_set_medium_tissue", "rte_set_medium_tissue_split", "rte_set_medium_voxel", "rte_set_medium_device", "rte_set_modulation",
+                 "rte_source_beam", "rte_prop_abs", "rte_prop_abs_adjoint", "rte_neumann", "rte_images", "rte_forward",
+                 "rte_detector_flux", "rte_gradient", "rte_image_gradient", "rte_region_gradient", "rte_fisher_regions", "rte_fisher",
                  "rte_forward_batch", "rte_forward_graph", "rte_server_submit", "rte_server_wait",
                  "rte_server_cancel", "rte_server_stats", "rte_set_profiling", "rte_get_stats", "rte_par_load",
                  "rte_par_problem", "rte_write_image", "rte_write_phase_image", "rte_read_image",

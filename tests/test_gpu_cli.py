@@ -22,12 +22,13 @@ def _exe(rte, name):
     return os.path.join(os.path.dirname(rte.rte.LIB_PATH), "..", "bin", name)
 
 
-def _par(g, d, extra=""):
+def _par(g, d, extra="", alg=""):
     text = str(g["par"])
     text = re.sub(r"(?im)^TissMapFile\s*=.*$", f"TissMapFile = {d}/tiss.bin", text)
     for k, f in (("TransFile", "trans.out"), ("ReflectFile", "ref.out"), ("PhaseFile", "phase.out")):
         text = re.sub(rf"(?im)^{k}\s*=.*$", f"{k} = {d}/{f}", text)
     text = text.replace("[Runtime]", "[Runtime]\n" + extra, 1)
+    text = text.replace("[Algorithm]", "[Algorithm]\n" + alg, 1)
     g["tiss"].astype(np.uint8).tofile(os.path.join(d, "tiss.bin"))
     p = os.path.join(d, "case.par")
     open(p, "w").write(text)
@@ -55,6 +56,26 @@ def test_rte_gpu_matches_reference_outputs(rte, tmp_path, case):
     ny, nx = struct.unpack("2i", b[:8])
     ph = np.frombuffer(b[8:], np.float64).reshape(ny, nx)
     assert np.all(np.isfinite(ph)) and ph.shape == tr.shape
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_reference_main_with_library_neumann(rte, tmp_path, case):
+    """The reference's own forward main (FisherInfo_IO/src/rte.cu, unchanged: its parameter reading, source,
+    images and files) linked with the library's Neumann() shim (doi_b200/shim/neumann_b200.cu) in place of
+    neumann.cu, as a maintainer would build it (oracle/build.sh makes oracle/_ref/fim_shim): its TransFile /
+    ReflectFile equal the images of the reference main run as shipped (the golden fixtures, pinned to that
+    main's own files by test_fim_forward_main_files) to 1e-6."""
+    exe = os.path.join(os.path.dirname(GOLD), "..", "oracle", "_ref", "fim_shim")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/fim_shim is built by oracle/build.sh where the reference tree is present")
+    g = np.load(os.path.join(GOLD, case + ".npz"))
+    d = str(tmp_path)
+    r = subprocess.run([exe, _par(g, d)], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:]
+    tr, rf = _read_img(os.path.join(d, "trans.out")), _read_img(os.path.join(d, "ref.out"))
+    assert rel(tr, g["trans"].reshape(tr.shape)) < 1e-6, rel(tr, g["trans"].reshape(tr.shape))
+    assert rel(rf, g["ref"].reshape(rf.shape)) < 1e-6, rel(rf, g["ref"].reshape(rf.shape))
 
 
 def _oracle_setup(oracle, g, mua_t, mus_t, tiss):
@@ -110,7 +131,7 @@ def test_rte_inv_matches_oracle(rte, oracle, tmp_path):
     with open(os.path.join(d, "g.out"), "wb") as f:
         f.write(struct.pack("2i", ny, nx))
         f.write(meas.tobytes())
-    par = _par(g, d, extra=f"gFile = {d}/g.out\nnumIterations = 1\n")
+    par = _par(g, d, extra=f"gFile = {d}/g.out\nnumIterations = 1\n", alg="ReferenceQuirks = 0\n")
     r = subprocess.run([_exe(rte, "rte_inv"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     assert r.returncode == 0, r.stdout
     got = [tuple(float(x) for x in m) for m in re.findall(r"mua grad1 = (\S+) musgrad1 = (\S+)", r.stdout)]
@@ -184,7 +205,7 @@ def test_rte_snr_matches_oracle(rte, oracle, tmp_path):
     nx, ny, nz = (int(g[k]) for k in ("nx", "ny", "nz"))
     with open(os.path.join(d, "g.out"), "wb") as f:  # the program insists on a measured image
         f.write(struct.pack("2i", ny, nx) + np.zeros(nx * ny).tobytes())
-    par = _par(g, d, extra=f"gFile = {d}/g.out\n")
+    par = _par(g, d, extra=f"gFile = {d}/g.out\n", alg="ReferenceQuirks = 0\n")
     r = subprocess.run([_exe(rte, "rte_snr"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     assert r.returncode == 0, r.stdout
     snr = np.fromfile(os.path.join(d, "snr_terms.dat"), np.float64)
@@ -208,3 +229,54 @@ def test_rte_snr_matches_oracle(rte, oracle, tmp_path):
             imgs.append(oracle.images(p, mua, mus, out, 1, mag=float(g["mag"]))[1].real.ravel())
         ref = float(np.sum((imgs[0] - imgs[1]) ** 2 / imgs[1]))
         assert abs(snr[lz - 2] - ref) <= 1e-5 * abs(ref), (lz, snr[lz - 2], ref)
+
+
+def test_rte_inv_reproduces_reference_main(rte, tmp_path):
+    """rte_inv with its defaults (ReferenceQuirks = 1: kernels on the .par tissue table, the rest on the swept
+    values, as the reference's main leaves its device table) prints the values the reference's own
+    region-gradient main (compute_grad_rte.cu, run unchanged on the CPU for the fixture) printed for the same
+    .par file and measured image, and writes the same Residual.out.  grad2 to 1e-5, grad1 (which divides by
+    per-pixel residuals, amplifying the 1e-7 path-integral difference of the table model) to 1e-3."""
+    run = np.load(os.path.join(GOLD, "fim_grad_main_10x10x20_L2.npz"))
+    g = np.load(os.path.join(GOLD, str(run["base"]) + ".npz"))
+    d = str(tmp_path)
+    nx, ny = int(g["nx"]), int(g["ny"])
+    meas = (g["trans"].real.reshape(ny, nx) * float(run["measured_scale"])).astype(np.float64)
+    with open(os.path.join(d, "g.out"), "wb") as f:
+        f.write(struct.pack("2i", ny, nx) + meas.tobytes())
+    par = _par(g, d, extra=f"gFile = {d}/g.out\nnumIterations = 1\n")
+    r = subprocess.run([_exe(rte, "rte_inv"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+    pat1, pat2 = r"mua grad1 = (\S+) musgrad1 = (\S+)", r"mua grad2 = (\S+) musgrad2 = (\S+)"
+    got1 = [tuple(float(x) for x in m) for m in re.findall(pat1, r.stdout)]
+    got2 = [tuple(float(x) for x in m) for m in re.findall(pat2, r.stdout)]
+    ref1 = [tuple(float(x) for x in m) for m in re.findall(pat1, str(run["stdout"]))]
+    ref2 = [tuple(float(x) for x in m) for m in re.findall(pat2, str(run["stdout"]))]
+    assert len(got1) == len(ref1) > 0 and len(got2) == len(ref2)
+    for a, b in zip(got2, ref2):
+        for x, y in zip(a, b):
+            assert abs(x - y) <= 1e-5 * abs(y), (x, y)
+    for a, b in zip(got1, ref1):
+        for x, y in zip(a, b):
+            assert abs(x - y) <= 1e-3 * abs(y), (x, y)
+    res = np.fromfile(os.path.join(d, "Residual.out"), np.float64)
+    assert abs(res[0] - run["Residual_out"][0]) <= 1e-6 * abs(run["Residual_out"][0])
+
+
+def test_rte_snr_reproduces_reference_main(rte, tmp_path):
+    """rte_snr with its defaults (ReferenceQuirks = 1: kernels on the .par tissue table, and z coordinates from
+    index nX on read as 0, as in the reference's run) gives at the first lesion depth the SNR^2 the
+    reference's own SNR main printed (the only depth it reaches: its loop step never advances) to 1e-5."""
+    run = np.load(os.path.join(GOLD, "fim_snr_main_10x10x20_L2.npz"))
+    g = np.load(os.path.join(GOLD, str(run["base"]) + ".npz"))
+    m = re.match(r"(\S+) is snr_sq for (\d+) as z index", str(run["first_line"]))
+    snr_ref, lz = float(m.group(1)), int(m.group(2))
+    d = str(tmp_path)
+    nx, ny = int(g["nx"]), int(g["ny"])
+    with open(os.path.join(d, "g.out"), "wb") as f:
+        f.write(struct.pack("2i", ny, nx) + np.zeros(nx * ny).tobytes())
+    par = _par(g, d, extra=f"gFile = {d}/g.out\n")
+    r = subprocess.run([_exe(rte, "rte_snr"), par], cwd=d, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+    snr = np.fromfile(os.path.join(d, "snr_terms.dat"), np.float64)
+    assert abs(snr[lz - 2] - snr_ref) <= 1e-5 * abs(snr_ref), (snr[lz - 2], snr_ref)

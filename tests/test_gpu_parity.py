@@ -33,8 +33,8 @@ def _ctx(rte, O, nx, ny, nz, L, model, prec, g=0.8, kernel_mode=0, n=1.0, prop=N
 @pytest.mark.parametrize("prec,tol", [(0, 1e-11), (1, 1e-5)])
 @pytest.mark.parametrize("kernel_mode", [1, 2])
 def test_prop_abs_exact_hetero(rte, oracle, prec, tol, kernel_mode):
-    if prec == 0 and kernel_mode == 1:
-        pytest.skip("the FP64 method always recomputes")
+    """kernel_mode 1 stores the pair kernel (FP32 for mixed precision, FP64 for the FP64 method), 2
+    recomputes every path integral."""
     rng = np.random.default_rng(1)
     nx, ny, nz, L = 7, 6, 5, 3
     N, C = nx * ny * nz, (L + 1) ** 2
@@ -64,13 +64,15 @@ def test_prop_abs_general_complex_input(rte, oracle):
     ctx.close()
 
 
-def test_prop_abs_fim_model(rte, oracle):
+@pytest.mark.parametrize("kernel_mode", [0, 1])
+def test_prop_abs_fim_model(rte, oracle, kernel_mode):
     """FisherInfo_IO discretisation: SH table with the un-wrapped phi index, tissue-0 self term 0,
-    g truncated to int in the scatter."""
+    g truncated to int in the scatter; FP64 method with the path integrals recomputed (0) or the FP64
+    pair kernel stored (1)."""
     rng = np.random.default_rng(3)
     nx, ny, nz, L = 10, 10, 10, 2
     N, C = nx * ny * nz, (L + 1) ** 2
-    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_FIM, 0, g=0.8)
+    ctx, p = _ctx(rte, oracle, nx, ny, nz, L, rte.MODEL_FIM, 0, g=0.8, kernel_mode=kernel_mode)
     tiss = rng.integers(0, 3, N).astype(np.uint8)
     mua_t = np.array([0.0, 0.01, 0.05])
     mus_t = np.array([0.0, 1.0, 1.5])
@@ -188,3 +190,26 @@ def test_uniform_medium_convolution_path(rte, oracle, prec, tol):
     pair.set_medium_voxel(mua, mus)
     assert rel(pair.forward(srcs[0], stop)["W"], res["W"]) < max(tol, 1e-12)
     pair.close()
+
+
+@pytest.mark.parametrize("model", [0, 1, 2])
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-6)])
+def test_prop_abs_adjoint_is_the_transpose(rte, model, prec, tol):
+    """rte_prop_abs_adjoint against the inner-product identity <y, A x> = <A^H y, x> on random complex
+    inputs, for the exact, table (FisherInfo_IO: transposed pair kernels, since snapping directions to its
+    table does not commute with negation) and CPU-package models.  The grid is even, so displacements with
+    zero components (where the table's unwrapped phi depends on the sign of zero) are present."""
+    rng = np.random.default_rng(12)
+    n, L = 6, 2
+    N, C = n ** 3, (L + 1) ** 2
+    ctx = rte.Context(n, n, n, dx=0.1, nL=L, g=0.8, model=model, precision=prec,
+                      kernel_mode=rte.KERNEL_STORE if prec else rte.KERNEL_RECOMPUTE)
+    mua, mus = _medium(rng, N)
+    ctx.set_medium_voxel(mua, mus)
+    for _ in range(3):
+        x = rng.standard_normal((N, C)) + 1j * rng.standard_normal((N, C))
+        y = rng.standard_normal((N, C)) + 1j * rng.standard_normal((N, C))
+        lhs = np.vdot(y, ctx.prop_abs(x, 1, 0))
+        rhs = np.vdot(ctx.prop_abs_adjoint(y, 1), x)
+        assert abs(lhs - rhs) <= tol * abs(lhs), (model, prec, lhs, rhs)
+    ctx.close()
