@@ -556,8 +556,8 @@ def run_ours(args):
     src = R.Source(pos_x=0.0, pos_y=0.0, kind=R.SRC_COLUMN)
     stop = R.Stop(R.STOP_FIXED, TERMS)
     # batched form: B of the four collimated z=0 sources at (+-0.825, +-0.825) cm of the adjoint
-    # configuration, solved together on each phantom (B = 2 by default: the best throughput of the
-    # kernel instantiations; B = 4 runs out of registers)
+    # configuration, solved together on each phantom (each pair's direction, spherical harmonics and
+    # kernel value serve all B sources)
     B = args.batch
     srcs = [R.Source(pos_x=x, pos_y=y, kind=R.SRC_COLUMN) for x, y in
             ((-0.825, -0.825), (0.825, -0.825), (-0.825, 0.825), (0.825, 0.825))][:B] if B > 1 else [src]

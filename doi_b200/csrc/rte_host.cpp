@@ -877,7 +877,8 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
   const bool f64 = c->precision == RTE_PREC_FP64;
   if (c->kernel_mode == RTE_KERNEL_RECOMPUTE || (f64 && c->kernel_mode != RTE_KERNEL_STORE)) return RTE_OK;
   const size_t ld = ((size_t)c->N + 31) / 32 * 32;  // 128-byte rows
-  const size_t need = (size_t)c->N * ld * (f64 ? sizeof(double) : sizeof(float));
+  const size_t need = f64 ? (size_t)c->N * ld * sizeof(double)
+                          : ((size_t)c->N + RTE_KBLK - 1) / RTE_KBLK * RTE_KBLK * ld * sizeof(float);
   if (f64 ? !c->d_K64 : !c->d_K) {
     size_t fr = 0, tot = 0;
     CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
@@ -888,8 +889,8 @@ static int ensure_pair_kernel(rte_ctx* c, bool* stored) {
     }
     if (f64)
       CUDA_TRY(c, dalloc(c, &c->d_K64, (size_t)c->N * ld));
-    else
-      CUDA_TRY(c, dalloc(c, &c->d_K, (size_t)c->N * ld));
+    else  // whole 128-destination blocks of ld source rows (kmat_index)
+      CUDA_TRY(c, dalloc(c, &c->d_K, ((size_t)c->N + RTE_KBLK - 1) / RTE_KBLK * RTE_KBLK * ld));
     c->Kld = ld;
   }
   if (!c->K_valid || c->capture_store) {
@@ -1024,6 +1025,18 @@ static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<
   return check_kernel_err(c);
 }
 
+// The tile-staged stored-kernel launch (mixed precision, exact directions, real right-hand sides: see
+// k_pair_mixed_tk) keeps each CTA's FP32 sums in registers over its whole source chunk; chunks of at most
+// kTkChunk sources keep those sums short (the epilogue adds the chunks in FP64): 33^3 L=5 error against
+// FP64 3.9e-6 with chunks of ~4,500 sources, see the bench line's fp64_rel_err for the capped chunks.
+static const int kTkChunk = 1024;
+static bool tk_kernel(const rte_ctx* c, int stored, int cplx) {
+  return c->precision == RTE_PREC_MIXED && stored && c->model != RTE_MODEL_FIM && !cplx;
+}
+
+template <class T>
+static int grow(rte_ctx* c, T** p, size_t& cap, size_t n);
+
 static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
   const int cplx = c->kappa != 0.0 ? 1 : 0;
   const int key = (((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0)) * 2 + cplx;
@@ -1041,10 +1054,17 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
   CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
   const long long slots = (long long)std::max(occ, 1) * sms;
   const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
-  int bestS = 1;
+  const bool tk = tk_kernel(c, stored, cplx);
+  const int Smin = tk ? (c->N + kTkChunk - 1) / kTkChunk : 1;
+  const int Smax = tk ? Smin + c->max_split : c->max_split;
+  if (tk) {  // partial sums of Smax chunks (before any capture: plan_split runs ahead of graph recording)
+    int rc = grow(c, &c->d_part, c->part_cap, (size_t)c->N * c->C * nb * Smax);
+    if (rc) return rc;
+  }
+  int bestS = Smin;
   double best = -1.0;
   std::vector<std::pair<double, int>> fills;  // (wave fill, S) of the realisable splits
-  for (int S = 1; S <= c->max_split; S++) {
+  for (int S = Smin; S <= Smax; S++) {
     const int Sreal = (c->N + split_chunk(c->N, S) - 1) / split_chunk(c->N, S);
     if (Sreal != S) continue;
     const double waves = (double)tiles * S / (double)slots;
@@ -1061,14 +1081,14 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
   const bool tune = !forced && !(at && at[0] == '0') && !c->capturing && c->precision == RTE_PREC_MIXED &&
                     c->N >= 4096;
   if (forced) {
-    bestS = std::max(1, std::min(c->max_split, atoi(forced)));
+    bestS = std::max(1, std::min(Smax, atoi(forced)));
   } else if (tune) {
     const TuneKey tk{c->cfg.device, c->N, LA, stored, nb, c->precision, table + 2 * cplx};
     bool have = false;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
       auto it = g_tuned.find(tk);
-      if (it != g_tuned.end() && it->second <= c->max_split) {
+      if (it != g_tuned.end() && it->second <= Smax && it->second >= Smin) {
         bestS = it->second;
         have = true;
       }

@@ -9,6 +9,14 @@
 #define RTE_PAIR_TS 64        // source voxels staged in shared memory per step
 #define RTE_MAX_MOM 48        // self-term power-series terms
 
+// Stored FP32 pair kernel layout: blocks of 128 destination slots, each block [source slot][128
+// destinations] with ld (>= N) source rows.  The kernel values of a run of consecutive sources for one
+// pair-kernel CTA's 128 destinations are then one contiguous block (a single bulk copy).
+#define RTE_KBLK 128
+__host__ __device__ inline size_t kmat_index(size_t s, size_t d, size_t ld) {
+  return ((d / RTE_KBLK) * ld + s) * RTE_KBLK + (d % RTE_KBLK);
+}
+
 struct PairArgs {
   int N, nx, ny, nz, Cfull;
   double dx, dy, dz;
@@ -19,8 +27,8 @@ struct PairArgs {
   const float* mutf;    // mu_t per voxel, FP32
   const double* Win;    // current term, real basis, N x Cfull, FP64
   const float* Winf;    // current term, FP32 copy in slot order, coefficient c times N_c (sh_eval_monic)
-  float* Kmat;          // stored pair kernel [source slot][destination slot], row stride Kld
-  double* Kmat64;       // the same in FP64 (plain FP64 method with a stored kernel)
+  float* Kmat;          // stored pair kernel K(source slot, destination slot), blocked (kmat_index, ld = Kld)
+  double* Kmat64;       // FP64 stored kernel (FP64 method), row-major [source slot][destination slot], stride Kld
   size_t Kld;
   double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
   int chunk;            // source voxels per blockIdx.y

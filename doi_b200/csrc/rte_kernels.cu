@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
             if (a.Kmat64) {
               kk = (T)__ldg(a.Kmat64 + (size_t)a.islot[rp] * a.Kld + slot);
             } else if (a.Kmat) {
-              kk = (T)__ldg(a.Kmat + (size_t)a.islot[rp] * a.Kld + slot);
+              kk = (T)__ldg(a.Kmat + kmat_index(a.islot[rp], slot, a.Kld));
             } else {
               int Q2;
               const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q2);
@@ -709,11 +709,11 @@ __device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
       for (int b = 0; b < NB; ++b)
 #pragma unroll
         for (int c = 0; c < C2; ++c) acc[b][c] = 0ull;
-      const float* Kcol = STORED ? a.Kmat + (size_t)s0 * a.Kld + slot : nullptr;
+      const float* Kcol = STORED ? a.Kmat + kmat_index(s0, slot, a.Kld) : nullptr;  // next source: +RTE_KBLK
       float k0 = 0.f, k1 = 0.f;
       if (STORED) {
         k0 = __ldg(Kcol);
-        if (ns > 1) k1 = __ldg(Kcol + a.Kld);
+        if (ns > 1) k1 = __ldg(Kcol + RTE_KBLK);
       }
       // stored kernel with exact SH: no per-pair branch (the diagonal and pairs beyond the coupling
       // distance carry k = 0), so two sources' SH recurrences can interleave
@@ -725,7 +725,7 @@ __device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
         if (STORED) {
           kk = k0;
           k0 = k1;
-          if (sv + 2 < ns) k1 = __ldg(Kcol + (size_t)(sv + 2) * a.Kld);
+          if (sv + 2 < ns) k1 = __ldg(Kcol + (size_t)(sv + 2) * RTE_KBLK);
         }
         const float4 q = P[sv];
         const float ddx = (me.x - q.x) * dxf, ddy = (me.y - q.y) * dyf, ddz = (me.z - q.z) * dzf;
@@ -828,6 +828,132 @@ __device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
   }
 }
 
+// Stored pair kernel with exact directions (the benchmark's form): the kernel values of each 32-source
+// tile for the CTA's 128 destinations are one contiguous block of the blocked K layout (kmat_index) and
+// arrive by bulk copy on the same mbarrier as the tile's FP32 rows and coordinates, so the pair loop
+// reads K from shared memory instead of waiting on a global load per source.  The FP32 accumulators stay
+// in registers across the chunk's tiles (the chunks are summed in FP64 by the epilogue), which frees the
+// shared-memory accumulator and leaves room for the K tiles.
+#define RTE_TK_TS 32
+struct TkLayout {
+  size_t off_w, off_k, off_bar, bytes;
+  __host__ __device__ explicit TkLayout(int cpad) {
+    off_w = sizeof(float4) * 2 * RTE_TK_TS;
+    off_k = off_w + sizeof(float) * 2 * RTE_TK_TS * (size_t)cpad;  // cpad is a multiple of 4: 16-byte aligned
+    off_bar = off_k + sizeof(float) * 2 * RTE_TK_TS * RTE_KBLK;
+    bytes = off_bar + 2 * sizeof(uint64_t);
+  }
+};
+
+template <int LA, int NB>
+__global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) {
+  static_assert(RTE_PAIR_THREADS == RTE_KBLK, "one K block per CTA");
+  constexpr int C = (LA + 1) * (LA + 1), TS = RTE_TK_TS, T = RTE_PAIR_THREADS;
+  typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
+  const int CP = a.cpad;
+  const TkLayout Sh(CP);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sP = reinterpret_cast<float4*>(smem_raw);
+  float* sW = reinterpret_cast<float*>(smem_raw + Sh.off_w);
+  float* sK = reinterpret_cast<float*>(smem_raw + Sh.off_k);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Sh.off_bar);
+  const int tid = threadIdx.x;
+  const int slot = blockIdx.x * T + tid;
+  const bool act = slot < a.N;
+  const float4 me = a.slot_xyz[act ? slot : 0];
+  const int r = __float_as_int(me.w);
+  const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  const int ntile = (se - sb + TS - 1) / TS;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const float* Kblk = a.Kmat + kmat_index(0, (size_t)blockIdx.x * T, a.Kld);  // this CTA's destination block
+  auto issue = [&](int t) {  // tile t -> buffer t & 1 (one thread)
+    const int s0 = sb + t * TS;
+    const int ns = min(TS, se - s0);
+    const int b = t & 1;
+    const uint32_t bw = (uint32_t)(ns * CP * sizeof(float)), bp = (uint32_t)(ns * sizeof(float4)),
+                   bk = (uint32_t)(ns * RTE_KBLK * sizeof(float));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[b], bw + bp + bk);
+    bulk_g2s(sW + b * TS * CP, a.Winf + (size_t)s0 * CP, bw, &bar[b]);
+    bulk_g2s(sP + b * TS, a.slot_xyz + s0, bp, &bar[b]);
+    bulk_g2s(sK + b * TS * RTE_KBLK, Kblk + (size_t)s0 * RTE_KBLK, bk, &bar[b]);
+  };
+  if (tid == 0 && ntile > 0) issue(0);
+  constexpr int C2 = (C + 1) / 2;  // coefficient pairs (packed f32x2 arithmetic)
+  const int CS = a.cstride;        // FP32 row stride of one right-hand side (even)
+  f2_t acc[NB][C2];
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+#pragma unroll
+    for (int c = 0; c < C2; ++c) acc[b][c] = 0ull;
+  for (int t = 0; t < ntile; ++t) {
+    if (tid == 0 && t + 1 < ntile) issue(t + 1);
+    const bool ok = mbar_wait(&bar[t & 1], (uint32_t)((t >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(a.err, 1);
+      return;
+    }
+    const int ns = min(TS, se - (sb + t * TS));
+    const float4* P = sP + (t & 1) * TS;
+    const float* Wt = sW + (t & 1) * TS * CP;
+    const float* Kt = sK + (t & 1) * TS * RTE_KBLK + tid;
+    if (act) {
+      // no per-pair branch: the diagonal and pairs beyond the coupling distance carry K = 0
+#pragma unroll 3
+      for (int sv = 0; sv < ns; ++sv) {
+        const float kk = Kt[sv * RTE_KBLK];
+        const float4 q = P[sv];
+        const float ddx = (me.x - q.x) * dxf, ddy = (me.y - q.y) * dyf, ddz = (me.z - q.z) * dzf;
+        const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+        const float inv = d2 > 0.f ? rsqrtf(d2) : 0.f;
+        ShT R[C];
+        sh_eval_monic<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+        f2_t R2[C2];
+#pragma unroll
+        for (int c = 0; c < C2; ++c) R2[c] = f2_pack((float)R[2 * c], 2 * c + 1 < C ? (float)R[2 * c + 1] : 0.f);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+          f2_t Sa = 0ull, Sb = 0ull;
+#pragma unroll
+          for (int c = 0; c < C2; c += 2) {
+            Sa = f2_fma(R2[c], w[c], Sa);
+            if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+          }
+          float a0, a1, b0, b1;
+          f2_unpack(Sa, a0, a1);
+          f2_unpack(Sb, b0, b1);
+          const float tb = kk * ((a0 + a1) + (b0 + b1));
+          const f2_t T2 = f2_pack(tb, tb);
+#pragma unroll
+          for (int c = 0; c < C2; ++c) acc[b][c] = f2_fma(R2[c], T2, acc[b][c]);
+        }
+      }
+    }
+    __syncthreads();  // buffer t & 1 is free for tile t + 2
+  }
+  if (act) {
+    const int vstride = NB * a.Cfull;
+    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * vstride;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int c = 0; c < C2; ++c) {
+        float lo, hi;
+        f2_unpack(acc[b][c], lo, hi);
+        o[b * a.Cfull + 2 * c] = (double)lo * kMonic.N[2 * c];
+        if (2 * c + 1 < C) o[b * a.Cfull + 2 * c + 1] = (double)hi * kMonic.N[2 * c + 1];
+      }
+  }
+}
+
 // Launch wrappers.  k_pair_mixed_3 carries a 3-CTA register bound and is used for L = 7 with one
 // right-hand side only; an explicit minimum-block count on the others makes ptxas take more registers
 // (L = 5, 2 RHS: 218 instead of 164, two CTAs per SM instead of three, 13.2 -> 17.0 ms per launch).
@@ -898,21 +1024,23 @@ __global__ void __launch_bounds__(RTE_KT) k_store_kernel(PairArgs a) {
     }
   }
   __syncthreads();
-  T* Km;
-  if constexpr (F64)
-    Km = a.Kmat64;
-  else
-    Km = a.Kmat;
-  // K[s][d]: row = source slot, contiguous over destination slots
+  // K(s, d): FP64 row-major [source slot][destination slot]; FP32 in 128-destination blocks
+  // (kmat_index).  Either way the 64 destinations of a tile row are contiguous (d0 is a multiple of 64).
+  auto at = [&](size_t sl, size_t d) -> T& {
+    if constexpr (F64)
+      return a.Kmat64[sl * a.Kld + d];
+    else
+      return a.Kmat[kmat_index(sl, d, a.Kld)];
+  };
   for (int q = 0; q < RTE_KT; ++q) {
     const int sl = s0 + q;
-    if (sl < a.N && d0 + tid < a.N) Km[(size_t)sl * a.Kld + d0 + tid] = tile[tid][q];
+    if (sl < a.N && d0 + tid < a.N) at(sl, d0 + tid) = tile[tid][q];
   }
   if (bs != bd) {
-    // K[d][s]: row = destination slot of this tile, now acting as the source
+    // K(d, s): the destination slots of this tile acting as sources
     for (int q = 0; q < RTE_KT; ++q) {
       const int dl = d0 + q;
-      if (dl < a.N && s0 + tid < a.N) Km[(size_t)dl * a.Kld + s0 + tid] = tile[q][tid];
+      if (dl < a.N && s0 + tid < a.N) at(dl, s0 + tid) = tile[q][tid];
     }
   }
 }
@@ -1472,7 +1600,7 @@ __global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
       if (a.Kmat64) {
         kk = (T)__ldg(a.Kmat64 + (size_t)sl * a.Kld + d);
       } else if (a.Kmat) {
-        kk = (T)__ldg(a.Kmat + (size_t)sl * a.Kld + d);
+        kk = (T)__ldg(a.Kmat + kmat_index(sl, d, a.Kld));
       } else {
         int Q0;
         const T ps = path_sum<T, double>(i, j, k, ip, jp, kp, a.mut, a.nx, plane, Q0);
@@ -1727,6 +1855,16 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
+  if constexpr (STORED && !TABLE && !CPLX) {  // K tiles staged with the source rows
+    const size_t smem = TkLayout(a.cpad).bytes;
+    void (*kern)(PairArgs) = k_pair_mixed_tk<LA, NB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
+    dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
+    kern<<<grid, RTE_PAIR_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   const size_t smem = MixedLayout(a.cpad, NB * (LA + 1) * (LA + 1), NB * (LA + 1) * (LA + 1) >= 128 ? 32 : RTE_PAIR_TS).bytes;
   void (*kern)(PairArgs);
   if constexpr (LA == 7 && NB == 1)

@@ -69,7 +69,10 @@ size_t estimate_bytes(const ShapeKey& k, int nsrc) {
   const size_t N = (size_t)k.n * k.n * k.n, C = (size_t)(k.L + 1) * (k.L + 1);
   const size_t nb = nsrc == 1 ? 1 : (nsrc <= 2 ? 2 : 4);
   size_t b = 8 * N * C * (24 + 14 * nb) + (64ull << 20);
-  if (k.prec == RTE_PREC_MIXED) b += 4 * N * ((N + 31) / 32 * 32);
+  if (k.prec == RTE_PREC_MIXED) {
+    b += 4 * ((N + 127) / 128 * 128) * ((N + 31) / 32 * 32);  // stored pair kernel (128-destination blocks)
+    b += 8 * N * C * nb * ((N + 1023) / 1024 + 8);            // partial sums of 1024-source chunks
+  }
   return b;
 }
 
