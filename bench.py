@@ -659,10 +659,12 @@ def run_ours(args):
         apply_flop = counts["pairs"] * (3 * counts["C"] + 4 * counts["C"] * B + 10)
         achieved = apply_flop / (avg_pair_ms * 1e-3) / 1e12
         peak = peak32 if prec == R.PREC_MIXED else peak64
+        # DRAM bytes of one pair launch from the ncu capture in profiles/ (per pair, scaled to this grid)
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tp):
-            traffic = json.load(open(tp)).get("pair_apply_bytes_per_launch")
+        if os.path.exists(tp) and prec == R.PREC_MIXED:
+            bpp = json.load(open(tp)).get("bytes_per_pair", {}).get(str(nbk))
+            traffic = bpp * counts["pairs"] if bpp else None
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -679,8 +681,8 @@ def run_ours(args):
                        "parallelism": f"replicas x{ws}"},
             "roofline": {"bound": "fp32-cuda-core" if prec == R.PREC_MIXED else "fp64-cuda-core",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": "k_pair_mixed<5,stored>" if prec == R.PREC_MIXED
-                         else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
+                         "traffic": traffic, "kernel": f"k_pair_mixed_tk<5,{nbk}> (stored FP32 kernel staged by bulk copy)"
+                         if prec == R.PREC_MIXED else "k_pair_fp64<5>", "avg_launch_ms": avg_pair_ms,
                          "flop_per_launch": apply_flop, "rhs_per_launch": nbk,
                          "peak_source": ("measured in this run by rte_measure_fma_peak (8 independent FMA chains "
                                          "per thread on every SM), of measured; theoretical FP32 148 SMs x 128 "
@@ -728,7 +730,8 @@ def run_profile(args):
     """Small single-purpose runs for ncu captures (no timing line): --profile-grad N runs one mixed-
     precision gradient of the config-4 problem at N^3 (4 sources, 8x8 bins, 20 terms); --profile-fisher N
     one mixed-precision Fisher information at N^3, L=5 (1 face beam, 8 parameters, 16x16 bins, path
-    integrals recomputed)."""
+    integrals recomputed); --profile-uniform N three forward solves of a uniform N^3, L=5 medium through
+    the FFT convolution path."""
     import doi_b200 as R
     if args.profile_grad:
         ctx, srcs, stop, det, target = grad_problem(0, n=args.profile_grad)
@@ -738,6 +741,13 @@ def run_profile(args):
     if args.profile_fisher:
         F = run_fisher_case(0, args.profile_fisher, 5, 16, TERMS, nsrc=1, P=8, kernel_mode=R.KERNEL_RECOMPUTE)[0]
         print(json.dumps({"profile": "fisher", "n": args.profile_fisher, "F_trace": float(np.trace(F))}))
+    if args.profile_uniform:
+        n = args.profile_uniform
+        with R.Context(n, n, n, dx=DX, nL=L, g=0.8, precision=R.PREC_MIXED, kernel_mode=R.KERNEL_AUTO) as ctx:
+            ctx.set_medium_voxel(np.full(n ** 3, 0.01), np.full(n ** 3, 1.0))
+            for _ in range(3):  # the first solve builds the table spectra and the transform plans
+                r = ctx.forward(R.Source(kind=R.SRC_COLUMN), R.Stop(R.STOP_FIXED, TERMS), want_W=False)
+        print(json.dumps({"profile": "uniform", "n": n, "ms_device": r["ms_device"]}))
     return 0
 
 
@@ -752,7 +762,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64-check", action="store_true")
     ap.add_argument("--n", type=int, default=33, help="grid side (33 = the benchmark; smaller for profiling)")
-    ap.add_argument("--batch", type=int, default=2, choices=[1, 2, 3, 4],
+    ap.add_argument("--batch", type=int, default=4, choices=[1, 2, 3, 4],
                     help="sources per phantom solved together (1 = one source per solve)")
     ap.add_argument("--skip-extras", action="store_true", help="skip the config-1, gradient and Fisher measurements")
     ap.add_argument("--fisher-full", action="store_true",
@@ -761,6 +771,8 @@ def main():
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
     ap.add_argument("--profile-grad", type=int, default=0, help="one config-4 gradient at this grid side, then exit")
     ap.add_argument("--profile-fisher", type=int, default=0, help="one Fisher information at this grid side, then exit")
+    ap.add_argument("--profile-uniform", type=int, default=0,
+                    help="three uniform-medium solves (FFT convolution path) at this grid side, then exit")
     ap.add_argument("--serve-requests-33", type=int, default=32,
                     help="requests in the single-shape 33^3 L=5 serving stream (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=0.0,
@@ -773,7 +785,7 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
-    if args.profile_grad or args.profile_fisher:
+    if args.profile_grad or args.profile_fisher or args.profile_uniform:
         return run_profile(args)
     return run_ours(args)
 

@@ -324,7 +324,7 @@ struct rte_ctx {
   double* d_img = nullptr;  // trans, ref (complex)
   bool medium_set = false;
   int max_split = 8;
-  std::vector<std::array<int, 3>> splits;  // (kernel key, S, chunk)
+  std::vector<std::array<int, 4>> splits;  // (kernel key, S, chunk, tile) of each planned launch shape
   size_t Kld = 0;
   double* d_selfp = nullptr;    // self-voxel term [N][nb][C]
   int* d_self_idx = nullptr;    // voxel -> distinct mu_t
@@ -336,7 +336,7 @@ struct rte_ctx {
   float4* d_slot_xyz = nullptr; // slot -> (x, y, z, voxel)
   int* d_err = nullptr;         // bounded-wait failure flag of the pair kernels
   int cpad = 0;                 // FP32 source row length (nb = 1)
-  int cstride = 0;              // FP32 stride of one right-hand side within a row (even)
+  int cstride = 0;              // FP32 stride of one right-hand side within a row (multiple of 4: 16-byte loads)
   // batched solves (several sources on one medium): buffers for up to bcap right-hand sides
   int bcap = 0;
   double *d_bW = nullptr, *d_bWn = nullptr, *d_bsum = nullptr, *d_bres = nullptr, *d_bball = nullptr;
@@ -598,7 +598,7 @@ int rte_create(const rte_config* cfg, rte_ctx** out) {
   c->part_cap = NC * c->max_split;
   c->selfp_cap = NC;
   if (rc == RTE_OK) cu(dalloc(c, &c->d_self_idx, c->N), "alloc");
-  c->cstride = (c->C + 1) / 2 * 2;
+  c->cstride = (c->C + 3) / 4 * 4;
   c->cpad = (c->cstride + 3) / 4 * 4;
   if (rc == RTE_OK) cu(dalloc(c, &c->d_Wf, (size_t)c->N * c->cpad), "alloc");
   if (rc == RTE_OK) cu(cudaMemset(c->d_Wf, 0, sizeof(float) * (size_t)c->N * c->cpad), "memset");
@@ -963,7 +963,7 @@ static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in3
   a.nsplit = S;
   a.nb = nb;
   a.slot_xyz = c->d_slot_xyz;
-  a.cstride = (c->C + 1) / 2 * 2;
+  a.cstride = (c->C + 3) / 4 * 4;
   a.cpad = (nb * a.cstride + 3) / 4 * 4;
   a.err = c->d_err;
   a.kappa = c->kappa;
@@ -985,11 +985,17 @@ static inline int split_chunk(int N, int S) {
 namespace {
 using TuneKey = std::tuple<int, int, int, int, int, int, int>;  // device, N, LA, stored, nb, precision, table
 std::mutex g_tune_mu;
-std::map<TuneKey, int> g_tuned;
+std::map<TuneKey, std::pair<int, int>> g_tuned;  // (S, tile)
+struct Plan {
+  double fill;  // wave fill of the occupancy model
+  int S, tile;
+};
 }  // namespace
 
-static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<std::pair<double, int>>& cands,
-                      int* S_best) {
+// Launch-plan autotuner: each candidate (split S, source tile) is launched on the context's own buffers
+// and timed with CUDA events (best of two); the fastest is kept for the process.
+static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<Plan>& cands, int* S_best,
+                      int* tile_best) {
   const int table = c->model == RTE_MODEL_FIM ? 1 : 0;
   const double* in64 = nb == 1 ? c->d_W : c->d_bW;
   const float* in32 = nb == 1 ? c->d_Wf : c->d_bWf;
@@ -1000,8 +1006,8 @@ static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<
   double best = 1e30;
   cudaError_t err = cudaSuccess;
   for (const auto& cand : cands) {
-    const int S = cand.second;
-    const PairArgs a = pair_args(c, in64, in32, nb, S, split_chunk(c->N, S));
+    PairArgs a = pair_args(c, in64, in32, nb, cand.S, split_chunk(c->N, cand.S));
+    a.tile = cand.tile;
     float t = 1e30f;
     for (int rep = 0; rep < 2 && err == cudaSuccess; rep++) {
       cudaEventRecord(e0, c->st);
@@ -1016,12 +1022,13 @@ static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<
     if (err != cudaSuccess) break;
     if (t < best) {
       best = t;
-      *S_best = S;
+      *S_best = cand.S;
+      *tile_best = cand.tile;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (err != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "split autotuner: %s", cudaGetErrorString(err));
+  if (err != cudaSuccess) return fail(c, RTE_ERR_DEVICE, "launch autotuner: %s", cudaGetErrorString(err));
   return check_kernel_err(c);
 }
 
@@ -1037,22 +1044,20 @@ static bool tk_kernel(const rte_ctx* c, int stored, int cplx) {
 template <class T>
 static int grow(rte_ctx* c, T** p, size_t& cap, size_t n);
 
-static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out) {
+static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* chunk_out, int* tile_out = nullptr) {
   const int cplx = c->kappa != 0.0 ? 1 : 0;
   const int key = (((LA * 2 + stored) * 8 + nb) * 2 + (c->precision == RTE_PREC_MIXED ? 1 : 0)) * 2 + cplx;
   for (auto& e : c->splits)
     if (e[0] == key) {
       *S_out = e[1];
       *chunk_out = e[2];
+      if (tile_out) *tile_out = e[3];
       return RTE_OK;
     }
   const int table = c->model == RTE_MODEL_FIM ? 1 : 0;
-  int occ = 0;
-  const int cpad = (nb * ((c->C + 1) / 2 * 2) + 3) / 4 * 4;
-  CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, table, stored, nb, cpad, &occ, cplx));
+  const int cpad = (nb * ((c->C + 3) / 4 * 4) + 3) / 4 * 4;
   int sms = 0;
   CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
-  const long long slots = (long long)std::max(occ, 1) * sms;
   const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
   const bool tk = tk_kernel(c, stored, cplx);
   const int Smin = tk ? (c->N + kTkChunk - 1) / kTkChunk : 1;
@@ -1061,57 +1066,76 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
     int rc = grow(c, &c->d_part, c->part_cap, (size_t)c->N * c->C * nb * Smax);
     if (rc) return rc;
   }
-  int bestS = Smin;
-  double best = -1.0;
-  std::vector<std::pair<double, int>> fills;  // (wave fill, S) of the realisable splits
-  for (int S = Smin; S <= Smax; S++) {
-    const int Sreal = (c->N + split_chunk(c->N, S) - 1) / split_chunk(c->N, S);
-    if (Sreal != S) continue;
-    const double waves = (double)tiles * S / (double)slots;
-    const double eff = waves / ceil(waves);
-    fills.push_back({eff, S});
-    // prefer the smallest S within 3% of the best fill, and at least one full wave when possible
-    if (eff > best + 0.03 || (best < 0.97 && eff > best)) {
-      best = eff;
-      bestS = S;
+  // occupancy-model candidates: (wave fill, S, tile) for each source tile the kernel offers
+  std::vector<Plan> fills;
+  Plan model{-1.0, Smin, 0};
+  for (int tile = 0; tile < (tk ? 2 : 1); tile++) {
+    int occ = 0;
+    CUDA_TRY(c, rte_pair_occupancy(LA, c->precision, table, stored, nb, cpad, &occ, cplx, tile));
+    const long long slots = (long long)std::max(occ, 1) * sms;
+    double best = -1.0;
+    int bestS = Smin;
+    for (int S = Smin; S <= Smax; S++) {
+      const int Sreal = (c->N + split_chunk(c->N, S) - 1) / split_chunk(c->N, S);
+      if (Sreal != S) continue;
+      const double waves = (double)tiles * S / (double)slots;
+      const double eff = waves / ceil(waves);
+      fills.push_back({eff, S, tile});
+      // prefer the smallest S within 3% of the best fill, and at least one full wave when possible
+      if (eff > best + 0.03 || (best < 0.97 && eff > best)) {
+        best = eff;
+        bestS = S;
+      }
     }
+    if (tile == 0) model = {best, bestS, 0};
   }
+  int bestS = model.S, bestTile = 0;
   const char* forced = getenv("RTE_NSPLIT");
   const char* at = getenv("RTE_AUTOTUNE");
   const bool tune = !forced && !(at && at[0] == '0') && !c->capturing && c->precision == RTE_PREC_MIXED &&
                     c->N >= 4096;
   if (forced) {
-    bestS = std::max(1, std::min(Smax, atoi(forced)));
+    bestS = std::max(Smin, std::min(Smax, atoi(forced)));
   } else if (tune) {
-    const TuneKey tk{c->cfg.device, c->N, LA, stored, nb, c->precision, table + 2 * cplx};
+    const TuneKey tk_key{c->cfg.device, c->N, LA, stored, nb, c->precision, table + 2 * cplx};
     bool have = false;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
-      auto it = g_tuned.find(tk);
-      if (it != g_tuned.end() && it->second <= Smax && it->second >= Smin) {
-        bestS = it->second;
+      auto it = g_tuned.find(tk_key);
+      if (it != g_tuned.end() && it->second.first <= Smax && it->second.first >= Smin) {
+        bestS = it->second.first;
+        bestTile = it->second.second;
         have = true;
       }
     }
     if (!have) {
-      std::vector<std::pair<double, int>> cands;
-      for (auto& f : fills)
-        if (f.first >= 0.75 * best) cands.push_back(f);
-      std::sort(cands.begin(), cands.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
-        return x.first > y.first || (x.first == y.first && x.second < y.second);
-      });
-      if (cands.size() > 5) cands.resize(5);
-      int rc = tune_split(c, LA, stored, nb, cands, &bestS);
+      // per tile: the splits whose wave fill is within 25% of that tile's best, the four best of them
+      std::vector<Plan> cands;
+      for (int tile = 0; tile < (tk ? 2 : 1); tile++) {
+        double best = 0.0;
+        for (auto& f : fills)
+          if (f.tile == tile) best = std::max(best, f.fill);
+        std::vector<Plan> mine;
+        for (auto& f : fills)
+          if (f.tile == tile && f.fill >= 0.75 * best) mine.push_back(f);
+        std::sort(mine.begin(), mine.end(), [](const Plan& x, const Plan& y) {
+          return x.fill > y.fill || (x.fill == y.fill && x.S < y.S);
+        });
+        if (mine.size() > 4) mine.resize(4);
+        cands.insert(cands.end(), mine.begin(), mine.end());
+      }
+      int rc = tune_split(c, LA, stored, nb, cands, &bestS, &bestTile);
       if (rc) return rc;
       std::lock_guard<std::mutex> lk(g_tune_mu);
-      g_tuned[tk] = bestS;
+      g_tuned[tk_key] = {bestS, bestTile};
     }
   }
   const int chunk = split_chunk(c->N, bestS);
   const int S = (c->N + chunk - 1) / chunk;
-  c->splits.push_back({key, S, chunk});
+  c->splits.push_back({key, S, chunk, bestTile});
   *S_out = S;
   *chunk_out = chunk;
+  if (tile_out) *tile_out = bestTile;
   return RTE_OK;
 }
 
@@ -1164,9 +1188,11 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
     bool stored = false;
     rc = ensure_pair_kernel(c, &stored);
     if (rc) return rc;
-    rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk);
+    int tile = 0;
+    rc = plan_split(c, LA, stored ? 1 : 0, nb, &S, &chunk, &tile);
     if (rc) return rc;
-    const PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
+    PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
+    a.tile = tile;
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
   }
@@ -1210,7 +1236,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   e.Wout = out;
   e.Woutf = out32;
   e.islot = c->d_islot;
-  e.cstride = (c->C + 1) / 2 * 2;
+  e.cstride = (c->C + 3) / 4 * 4;
   e.cpad = (nb * e.cstride + 3) / 4 * 4;
   e.sum = sum;
   e.red = c->d_red;

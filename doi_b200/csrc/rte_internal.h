@@ -36,7 +36,7 @@ struct PairArgs {
   int nb;               // right-hand sides sharing the medium (mixed kernels), layout [N][nb][Cfull]
   const float4* slot_xyz;  // per slot: (x, y, z) voxel coordinates as exact floats, w = voxel index
   int cpad;             // FP32 source row length in floats: nb*cstride rounded up to a multiple of 4
-  int cstride;          // FP32 row stride of one right-hand side: Cfull rounded up to even
+  int cstride;          // FP32 row stride of one right-hand side: Cfull rounded up to a multiple of 4
   int* err;             // set to 1 when a bounded wait runs out (kernel result invalid)
   // tangent pass (k_pair_tangent): derivative of mu_t along a parameter direction, and the voxel
   // bounding box of its support (pairs whose segment misses the box have no path derivative)
@@ -50,6 +50,7 @@ struct PairArgs {
   // displacement (source minus destination).  Snapping does not commute with negation, so for the
   // FisherInfo_IO table A^T != P A P; with exact SH the parity form is used instead.
   int transpose;
+  int tile;  // staged stored-kernel launch: 0 = 32-source tiles, 1 = 64-source tiles (autotuned)
 };
 
 struct EpiArgs {
@@ -235,7 +236,7 @@ cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table,
 // fp64 = 1: FP64 path sums and exp into a.Kmat64; else FP32 into a.Kmat
 cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st, int fp64 = 0);
 cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm,
-                               int cplx = 0);
+                               int cplx = 0, int tile = 0);
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st);
 cudaError_t rte_launch_images(const ImgArgs& a, cudaStream_t st);
 cudaError_t rte_launch_self(const SelfArgs& a, cudaStream_t st);

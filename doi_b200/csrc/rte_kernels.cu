@@ -834,24 +834,27 @@ __device__ __forceinline__ void pair_mixed_body(const PairArgs& a) {
 // reads K from shared memory instead of waiting on a global load per source.  The FP32 accumulators stay
 // in registers across the chunk's tiles (the chunks are summed in FP64 by the epilogue), which frees the
 // shared-memory accumulator and leaves room for the K tiles.
-#define RTE_TK_TS 32
+// The source tile size TS (32 or 64) is chosen per shape by the autotuner (PairArgs::tile).
 struct TkLayout {
   size_t off_w, off_k, off_bar, bytes;
-  __host__ __device__ explicit TkLayout(int cpad) {
-    off_w = sizeof(float4) * 2 * RTE_TK_TS;
-    off_k = off_w + sizeof(float) * 2 * RTE_TK_TS * (size_t)cpad;  // cpad is a multiple of 4: 16-byte aligned
-    off_bar = off_k + sizeof(float) * 2 * RTE_TK_TS * RTE_KBLK;
+  __host__ __device__ TkLayout(int cpad, int ts) {
+    off_w = sizeof(float4) * 2 * ts;
+    off_k = off_w + sizeof(float) * 2 * ts * (size_t)cpad;  // cpad is a multiple of 4: 16-byte aligned
+    off_bar = off_k + sizeof(float) * 2 * ts * RTE_KBLK;
     bytes = off_bar + 2 * sizeof(uint64_t);
   }
 };
 
-template <int LA, int NB>
+template <int LA, int NB, int TS>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) {
   static_assert(RTE_PAIR_THREADS == RTE_KBLK, "one K block per CTA");
-  constexpr int C = (LA + 1) * (LA + 1), TS = RTE_TK_TS, T = RTE_PAIR_THREADS;
+  constexpr int C = (LA + 1) * (LA + 1), T = RTE_PAIR_THREADS;
   typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
+  // 16-byte source-row loads, except for wide L = 7 rows where the extra registers cost more than the
+  // loads save (33^3 L=7, 2 RHS: 30.1 -> 33.8 ms per launch with them)
+  constexpr bool V4 = LA < 7 || NB == 1;
   const int CP = a.cpad;
-  const TkLayout Sh(CP);
+  const TkLayout Sh(CP, TS);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* sP = reinterpret_cast<float4*>(smem_raw);
   float* sW = reinterpret_cast<float*>(smem_raw + Sh.off_w);
@@ -887,7 +890,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) 
   };
   if (tid == 0 && ntile > 0) issue(0);
   constexpr int C2 = (C + 1) / 2;  // coefficient pairs (packed f32x2 arithmetic)
-  const int CS = a.cstride;        // FP32 row stride of one right-hand side (even)
+  const int CS = a.cstride;        // FP32 row stride of one right-hand side (a multiple of 4)
   f2_t acc[NB][C2];
 #pragma unroll
   for (int b = 0; b < NB; ++b)
@@ -920,12 +923,24 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) 
         for (int c = 0; c < C2; ++c) R2[c] = f2_pack((float)R[2 * c], 2 * c + 1 < C ? (float)R[2 * c + 1] : 0.f);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-          const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+          // broadcast loads of the source row (CS and CP are multiples of 4 floats; the padding beyond C
+          // is zero)
           f2_t Sa = 0ull, Sb = 0ull;
+          if constexpr (V4) {
+            const float4* w4 = reinterpret_cast<const float4*>(Wt + sv * CP + b * CS);
 #pragma unroll
-          for (int c = 0; c < C2; c += 2) {
-            Sa = f2_fma(R2[c], w[c], Sa);
-            if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+            for (int c = 0; c < C2; c += 2) {
+              const float4 v = w4[c / 2];
+              Sa = f2_fma(R2[c], f2_pack(v.x, v.y), Sa);
+              if (c + 1 < C2) Sb = f2_fma(R2[c + 1], f2_pack(v.z, v.w), Sb);
+            }
+          } else {
+            const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+#pragma unroll
+            for (int c = 0; c < C2; c += 2) {
+              Sa = f2_fma(R2[c], w[c], Sa);
+              if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+            }
           }
           float a0, a1, b0, b1;
           f2_unpack(Sa, a0, a1);
@@ -1855,9 +1870,10 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
-  if constexpr (STORED && !TABLE && !CPLX) {  // K tiles staged with the source rows
-    const size_t smem = TkLayout(a.cpad).bytes;
-    void (*kern)(PairArgs) = k_pair_mixed_tk<LA, NB>;
+  if constexpr (STORED && !TABLE && !CPLX) {  // K tiles staged with the source rows, 32 or 64 sources a tile
+    const int ts = a.tile ? 64 : 32;
+    const size_t smem = TkLayout(a.cpad, ts).bytes;
+    void (*kern)(PairArgs) = a.tile ? k_pair_mixed_tk<LA, NB, 64> : k_pair_mixed_tk<LA, NB, 32>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
@@ -1936,11 +1952,12 @@ cudaError_t rte_launch_pair(const PairArgs& a, int LA, int precision, int table,
 }
 
 cudaError_t rte_pair_occupancy(int LA, int precision, int table, int stored, int nb, int cpad, int* blocks_per_sm,
-                               int cplx) {
+                               int cplx, int tile) {
   PairArgs dummy;
   memset(&dummy, 0, sizeof dummy);
   dummy.cpad = cpad;
   dummy.kappa = cplx ? 1.0 : 0.0;
+  dummy.tile = tile;
   return pair_dispatch(dummy, LA, precision, table, stored, nb, nullptr, blocks_per_sm);
 }
 
