@@ -959,6 +959,7 @@ static PairArgs pair_args(const rte_ctx* c, const double* in64, const float* in3
   a.Kmat64 = c->d_K64;
   a.Kld = c->Kld;
   a.part = c->d_part;
+  a.partf = reinterpret_cast<float*>(c->d_part);
   a.chunk = chunk;
   a.nsplit = S;
   a.nb = nb;
@@ -1178,6 +1179,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
                       int flag, int flag_scat, int nb = 1) {
   const int LA = flag ? c->L : 0;
   int S = 1, chunk = c->N;
+  bool f32part = false;  // the tile-staged kernel leaves FP32 chunk sums
   int rc;
   if (fft_active(c)) {
     rc = ensure_fft(c);
@@ -1193,6 +1195,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
     if (rc) return rc;
     PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
     a.tile = tile;
+    f32part = tk_kernel(c, stored ? 1 : 0, c->kappa != 0.0 ? 1 : 0);
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
   }
@@ -1229,6 +1232,7 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
   e.S = S;
   e.nb = nb;
   e.part = c->d_part;
+  e.partf = f32part ? reinterpret_cast<const float*>(c->d_part) : nullptr;
   e.selfp = c->d_selfp;
   e.mus = c->d_mus;
   e.flag_scat = flag_scat;

@@ -31,6 +31,7 @@ struct PairArgs {
   double* Kmat64;       // FP64 stored kernel (FP64 method), row-major [source slot][destination slot], stride Kld
   size_t Kld;
   double* part;         // split-K partial sums, [S][N][Cfull], indexed by voxel
+  float* partf;         // FP32 partial sums in the same layout (tile-staged kernel: raw chunk sums, no N_c)
   int chunk;            // source voxels per blockIdx.y
   int nsplit;           // S
   int nb;               // right-hand sides sharing the medium (mixed kernels), layout [N][nb][Cfull]
@@ -56,6 +57,7 @@ struct PairArgs {
 struct EpiArgs {
   int N, nx, ny, nz, Cfull, S, nb;  // nb right-hand sides, layout [N][nb][Cfull]
   const double* part;   // [S][N][nb][Cfull]
+  const float* partf;   // or FP32 chunk sums of the tile-staged kernel, times N_c here (then part is unused)
   const double* selfp;  // self-voxel term [N][nb][Cfull] (may be null)
   const double* mus;
   int flag_scat;

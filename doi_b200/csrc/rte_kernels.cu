@@ -954,17 +954,17 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) 
     }
     __syncthreads();  // buffer t & 1 is free for tile t + 2
   }
-  if (act) {
+  if (act) {  // the chunk's FP32 sums as they are (the epilogue applies N_c after adding the chunks in FP64)
     const int vstride = NB * a.Cfull;
-    double* o = a.part + ((size_t)blockIdx.y * a.N + r) * vstride;
+    float* o = a.partf + ((size_t)blockIdx.y * a.N + r) * vstride;
 #pragma unroll
     for (int b = 0; b < NB; ++b)
 #pragma unroll
       for (int c = 0; c < C2; ++c) {
         float lo, hi;
         f2_unpack(acc[b][c], lo, hi);
-        o[b * a.Cfull + 2 * c] = (double)lo * kMonic.N[2 * c];
-        if (2 * c + 1 < C) o[b * a.Cfull + 2 * c + 1] = (double)hi * kMonic.N[2 * c + 1];
+        o[b * a.Cfull + 2 * c] = lo;
+        if (2 * c + 1 < C) o[b * a.Cfull + 2 * c + 1] = hi;
       }
   }
 }
@@ -1074,56 +1074,51 @@ __device__ __forceinline__ double stop_weight(int c, bool imag) {
 
 // ---------------------------------------------------------------------------------------------
 // Epilogue: add split-K partials, self-voxel term, scatter; write the next term (FP64 and FP32),
-// accumulate the running sum and the norms used by the stop rules.
-// Self term: Dself(mu) = sum_k mu^k M_k (Horner), see the moment construction in rte_host.cpp.
-template <int LA>
-__global__ void __launch_bounds__(128) k_epilogue(EpiArgs a) {
-  constexpr int C = (LA + 1) * (LA + 1);
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double w2 = 0.0, s2 = 0.0, lw = 0.0, ls = 0.0;
+// accumulate the running sum and the norms used by the stop rules.  One thread per (voxel, right-hand
+// side, coefficient) element, grid-stride, so every stream (partials, self term, outputs, running sum)
+// is read and written coalesced; the four norms are reduced per block and added atomically.
+// Self term: computed by k_self into selfp.  Coefficients above (LA+1)^2 are written as 0.
+__global__ void __launch_bounds__(256) k_epilogue(EpiArgs a, int Cact) {
   const int nb = a.nb > 0 ? a.nb : 1;
   const int vstride = nb * a.Cfull;
-  if (r < a.N) {
-    const bool stop_layer = (r / (a.nx * a.ny)) == a.nz - 1;
-    for (int b = 0; b < nb; ++b) {
-      const size_t base = (size_t)r * vstride + (size_t)b * a.Cfull;
-      double v[C];
-#pragma unroll
-      for (int c = 0; c < C; ++c) v[c] = a.selfp ? a.selfp[base + c] : 0.0;
-      for (int s = 0; s < a.S; ++s) {
-        const double* p = a.part + (size_t)s * a.N * vstride + base;
-#pragma unroll
-        for (int c = 0; c < C; ++c) v[c] += p[c];
+  const size_t total = (size_t)a.N * vstride, NV = (size_t)a.N * vstride;
+  const int plane = a.nx * a.ny;
+  double w2 = 0.0, s2 = 0.0, lw = 0.0, ls = 0.0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t / vstride), e = (int)(t - (size_t)r * vstride);
+    const int b = e / a.Cfull, c = e - b * a.Cfull;
+    int l = 0;
+    while ((l + 1) * (l + 1) <= c) ++l;
+    double x = 0.0;
+    if (c < Cact) {
+      x = a.selfp ? a.selfp[t] : 0.0;
+      if (a.partf) {  // FP32 chunk sums of the tile-staged kernel: FP64 sum over the chunks, then N_c
+        double u = 0.0;
+        for (int q = 0; q < a.S; ++q) u += (double)a.partf[(size_t)q * NV + t];
+        x = fma(u, kMonic.N[c], x);
+      } else {
+        for (int q = 0; q < a.S; ++q) x += a.part[(size_t)q * NV + t];
       }
-      if (a.flag_scat) {
-        const double ms = a.mus[r];
-#pragma unroll
-        for (int l = 0; l <= LA; ++l)
-#pragma unroll
-          for (int m = -l; m <= l; ++m) v[l * l + l + m] *= a.scat[l] * ms;
-      }
-      for (int c = 0; c < a.Cfull; ++c) {
-        const double x = c < C ? v[c] : 0.0;
-        a.Wout[base + c] = x;
-        // the mixed pair kernels read N_c W_c (monic SH, sh_eval_monic)
-        if (a.Woutf) a.Woutf[(size_t)a.islot[r] * a.cpad + (size_t)b * a.cstride + c] = (float)(x * kMonic.N[c]);
-        w2 += x * x;
-        double sv = 0.0;
-        if (a.sum) {
-          sv = a.sum[base + c] + x;
-          a.sum[base + c] = sv;
-          s2 += sv * sv;
-        }
-        if (stop_layer) {
-          const double wgt = stop_weight(c, a.cplx && (b & 1));
-          lw += wgt * x;
-          ls += wgt * sv;
-        }
-      }
+      if (a.flag_scat) x *= a.scat[l] * a.mus[r];
+    }
+    a.Wout[t] = x;
+    // the mixed pair kernels read N_c W_c (monic SH, sh_eval_monic)
+    if (a.Woutf) a.Woutf[(size_t)a.islot[r] * a.cpad + (size_t)b * a.cstride + c] = (float)(x * kMonic.N[c]);
+    w2 += x * x;
+    double sv = 0.0;
+    if (a.sum) {
+      sv = a.sum[t] + x;
+      a.sum[t] = sv;
+      s2 += sv * sv;
+    }
+    if (r / plane == a.nz - 1) {  // the reference stop rule's layer
+      const double wgt = stop_weight(c, a.cplx && (b & 1));
+      lw += wgt * x;
+      ls += wgt * sv;
     }
   }
   // block reduction of the four norms
-  __shared__ double red[4][32];
+  __shared__ double red[4][8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double vals[4] = {w2, s2, lw, ls};
 #pragma unroll
@@ -1971,18 +1966,10 @@ cudaError_t rte_launch_store_kernel(const PairArgs& a, cudaStream_t st, int fp64
 }
 
 cudaError_t rte_launch_epilogue(const EpiArgs& a, int LA, cudaStream_t st) {
-  const int blocks = (a.N + 127) / 128;
-  switch (LA) {
-    case 0: k_epilogue<0><<<blocks, 128, 0, st>>>(a); break;
-    case 1: k_epilogue<1><<<blocks, 128, 0, st>>>(a); break;
-    case 2: k_epilogue<2><<<blocks, 128, 0, st>>>(a); break;
-    case 3: k_epilogue<3><<<blocks, 128, 0, st>>>(a); break;
-    case 4: k_epilogue<4><<<blocks, 128, 0, st>>>(a); break;
-    case 5: k_epilogue<5><<<blocks, 128, 0, st>>>(a); break;
-    case 6: k_epilogue<6><<<blocks, 128, 0, st>>>(a); break;
-    case 7: k_epilogue<7><<<blocks, 128, 0, st>>>(a); break;
-    default: return cudaErrorInvalidValue;
-  }
+  if (LA < 0 || LA > RTE_MAX_L) return cudaErrorInvalidValue;
+  const size_t total = (size_t)a.N * (a.nb > 0 ? a.nb : 1) * a.Cfull;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+  k_epilogue<<<blocks, 256, 0, st>>>(a, (LA + 1) * (LA + 1));
   return cudaGetLastError();
 }
 
