@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) 
     const float* Kt = sK + (t & 1) * TS * RTE_KBLK + tid;
     if (act) {
       // no per-pair branch: the diagonal and pairs beyond the coupling distance carry K = 0
-#pragma unroll 3
+#pragma unroll 4
       for (int sv = 0; sv < ns; ++sv) {
         const float kk = Kt[sv * RTE_KBLK];
         const float4 q = P[sv];
