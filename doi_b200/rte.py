@@ -425,14 +425,31 @@ class Context:
                                                 _ptr(g), ctypes.byref(loss), _ptr(ga), _ptr(gs)), "rte_image_gradient")
         return loss.value, ga, gs
 
-    def forward_batch(self, srcs, stop=None, want_W=True, want_images=True):
+    def _outputs(self, out, shapes):
+        """Result arrays: those given in out (C-contiguous complex128 of the right shape, e.g. views of
+        pinned host memory, written in place), else fresh zeros."""
+        res = []
+        for key, shape in shapes:
+            if shape is None:
+                res.append(None)
+                continue
+            a = (out or {}).get(key)
+            if a is None:
+                a = np.zeros(shape, np.complex128)
+            elif (not isinstance(a, np.ndarray) or a.dtype != np.complex128 or a.shape != shape
+                  or not a.flags.c_contiguous):
+                raise RteError(f"out[{key!r}] must be a C-contiguous complex128 array of shape {shape}")
+            res.append(a)
+        return res
+
+    def forward_batch(self, srcs, stop=None, want_W=True, want_images=True, out=None):
         """Several sources on the current medium in one batched solve; returns the per-source results
-        stacked along a leading axis."""
+        stacked along a leading axis.  out may hold preallocated arrays "W", "trans", "ref" to write."""
         stop = stop or Stop()
         B = len(srcs)
-        W = np.zeros((B, self.N, self.C), np.complex128) if want_W else None
-        tr = np.zeros((B, self.ny, self.nx), np.complex128) if want_images else None
-        rf = np.zeros((B, self.ny, self.nx), np.complex128) if want_images else None
+        W, tr, rf = self._outputs(out, (("W", (B, self.N, self.C) if want_W else None),
+                                        ("trans", (B, self.ny, self.nx) if want_images else None),
+                                        ("ref", (B, self.ny, self.nx) if want_images else None)))
         arr = (_Source * B)(*[s.c() for s in srcs])
         rep = _Report()
         st = stop.c()
@@ -496,11 +513,11 @@ class Context:
                     "rte_forward_graph")
         return tr, rf, rep.ms_device
 
-    def forward(self, src, stop=None, want_W=True, want_images=True):
+    def forward(self, src, stop=None, want_W=True, want_images=True, out=None):
         stop = stop or Stop()
-        W = np.zeros((self.N, self.C), np.complex128) if want_W else None
-        tr = np.zeros(self.nx * self.ny, np.complex128) if want_images else None
-        rf = np.zeros(self.nx * self.ny, np.complex128) if want_images else None
+        W, tr, rf = self._outputs(out, (("W", (self.N, self.C) if want_W else None),
+                                        ("trans", (self.nx * self.ny,) if want_images else None),
+                                        ("ref", (self.nx * self.ny,) if want_images else None)))
         rep = _Report()
         s, st = src.c(), stop.c()
         self._check(self.lib.rte_forward(self.h, ctypes.byref(s), ctypes.byref(st), _ptr(W), _ptr(tr), _ptr(rf),

@@ -106,3 +106,17 @@ def test_server_errors_carry_messages(rte):
             rte.Server(device=0, workers=2)
         msg = str(e.value).split("):", 1)[1].strip()
         assert msg
+
+
+def test_preallocated_outputs_are_checked(rte):
+    """forward / forward_batch out= arrays: used as given when complex128, C-contiguous and of the
+    result's shape; anything else is refused before the library is called."""
+    import numpy as np
+    shapes = (("W", (2, 8, 4)), ("trans", None), ("ref", (2, 3, 3)))
+    w = np.zeros((2, 8, 4), np.complex128)
+    got = rte.Context._outputs(None, {"W": w}, shapes)
+    assert got[0] is w and got[1] is None and got[2].shape == (2, 3, 3)
+    for bad in (np.zeros((2, 8, 4)), np.zeros((2, 8, 5), np.complex128),
+                np.zeros((2, 4, 8), np.complex128).transpose(0, 2, 1)):
+        with pytest.raises(rte.RteError):
+            rte.Context._outputs(None, {"W": bad}, shapes)

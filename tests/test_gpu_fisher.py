@@ -61,11 +61,16 @@ def test_sensitivity_matches_finite_differences(rte):
 
 
 def test_fisher_mixed_vs_fp64(rte):
+    """Mixed precision (stored FP32 kernel) against the FP64 method: J and F within 1e-5 (measured 1.6e-7
+    and 2.3e-7 here).  F weights bins by 1/flux, so on detectors with near-zero-flux bins its relative
+    error can exceed J's."""
     stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-12)
     det = rte.Detector(nbins=3, faces=63)
     out = []
     for prec in (rte.PREC_FP64, rte.PREC_MIXED):
         ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, prec)
-        out.append(ctx.fisher(srcs, stop, det, dmua, dmus))
+        out.append(ctx.fisher(srcs, stop, det, dmua, dmus, want_J=True))
         ctx.close()
-    assert rel(out[1], out[0]) < 1e-4, rel(out[1], out[0])
+    (F64, J64), (F32, J32) = out
+    assert rel(J32, J64) < 1e-5, rel(J32, J64)
+    assert rel(F32, F64) < 1e-5, rel(F32, F64)

@@ -161,6 +161,12 @@ def test_forward_batch_matches_single(rte, oracle, n, L):
                              max_terms=12, pos_x=s.pos_x, pos_y=s.pos_y)
         assert rel(rb4["W"][b], ref["out"]) < 1e-5
         assert rel(rb4["trans"][b], ref["trans"]) < 1e-5
+    # preallocated result arrays (as pinned host buffers are passed) are written in place
+    out = {"W": np.full_like(rb4["W"], np.nan), "trans": np.full_like(rb4["trans"], np.nan),
+           "ref": np.full_like(rb4["ref"], np.nan)}
+    rb = ctx.forward_batch(srcs, stop, out=out)
+    assert rb["W"] is out["W"] and rb["trans"] is out["trans"]
+    assert rel(out["W"], rb4["W"]) < 1e-12 and rel(out["ref"], rb4["ref"]) < 1e-12
     ctx.close()
 
 
