@@ -3174,7 +3174,9 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   const size_t npix = 2 * (np + (size_t)c->nz * c->nx + (size_t)c->nz * c->ny);
   const int nb = d->nbins;
   const size_t NB2 = (size_t)6 * nb * nb;
-  const int nbt = c->precision == RTE_PREC_MIXED ? 2 : 1;  // tangent series run together
+  // tangent series run together: four at L <= 5 (the widest pair-kernel batch whose accumulators fit in
+  // registers), two above; the pair walk and the SH recurrence of every pair serve the whole group
+  const int nbt = c->precision == RTE_PREC_MIXED ? (c->L <= 5 ? 4 : 2) : 1;
   if (nbt > 1) {
     rc = ensure_batch(c, nbt);
     if (rc) return rc;
@@ -3182,7 +3184,7 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   if (!c->d_dmut) {
     CUDA_TRY(c, dalloc(c, &c->d_dmut, (size_t)c->N));
     CUDA_TRY(c, dalloc(c, &c->d_dmus, (size_t)c->N));
-    CUDA_TRY(c, dalloc(c, &c->d_T, 2 * NC));
+    CUDA_TRY(c, dalloc(c, &c->d_T, (size_t)std::max(2, nbt) * NC));  // nbt is fixed for a context (L, precision)
     CUDA_TRY(c, dalloc(c, &c->d_cidx, (size_t)std::max(c->nx, std::max(c->ny, c->nz))));
     CUDA_TRY(c, dalloc(c, &c->d_cval, (size_t)std::max(c->nx, std::max(c->ny, c->nz)) * c->C));
   }

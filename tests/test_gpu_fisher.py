@@ -13,10 +13,11 @@ pytestmark = pytest.mark.gpu
 N_SIDE, L = 9, 2
 
 
-def _problem(rte, prec):
+def _problem(rte, prec, kernel_mode=None, Lq=L):
     sph = rte.random_spheres(N_SIDE, 2, seed=3, rmin=0.15, rmax=0.25)
-    ctx = rte.Context(N_SIDE, N_SIDE, N_SIDE, dx=0.1, nL=L, g=0.9, precision=prec,
-                      kernel_mode=rte.KERNEL_STORE if prec == rte.PREC_MIXED else rte.KERNEL_RECOMPUTE)
+    if kernel_mode is None:
+        kernel_mode = rte.KERNEL_STORE if prec == rte.PREC_MIXED else rte.KERNEL_RECOMPUTE
+    ctx = rte.Context(N_SIDE, N_SIDE, N_SIDE, dx=0.1, nL=Lq, g=0.9, precision=prec, kernel_mode=kernel_mode)
     mua, mus, dmua, dmus = rte.smooth_sphere_phantom(N_SIDE, sph, mua_bg=0.02, mus_bg=2.0)
     ctx.set_medium_voxel(mua, mus)
     c = 0.45 - 0.45  # face centres of the 0.9 cm box (x, y centred on 0, z from 0.05 to 0.85)
@@ -60,15 +61,18 @@ def test_sensitivity_matches_finite_differences(rte):
     ctx.close()
 
 
-def test_fisher_mixed_vs_fp64(rte):
-    """Mixed precision (stored FP32 kernel) against the FP64 method: J and F within 1e-5 (measured 1.6e-7
-    and 2.3e-7 here).  F weights bins by 1/flux, so on detectors with near-zero-flux bins its relative
-    error can exceed J's."""
+@pytest.mark.parametrize("Lq,stored", [(2, True), (2, False), (5, False)])
+def test_fisher_mixed_vs_fp64(rte, Lq, stored):
+    """Mixed precision against the FP64 method, with the stored FP32 kernel or with the path integrals
+    recomputed in every term (the Fisher benchmark's form): J and F within 1e-5 (measured 1.6e-7 and
+    2.3e-7 at L = 2, stored).  The 8 parameters run as two groups of four tangent series.  F weights bins
+    by 1/flux, so on detectors with near-zero-flux bins its relative error can exceed J's."""
     stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-12)
     det = rte.Detector(nbins=3, faces=63)
     out = []
     for prec in (rte.PREC_FP64, rte.PREC_MIXED):
-        ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, prec)
+        mode = None if prec == rte.PREC_FP64 else (rte.KERNEL_STORE if stored else rte.KERNEL_RECOMPUTE)
+        ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, prec, mode, Lq)
         out.append(ctx.fisher(srcs, stop, det, dmua, dmus, want_J=True))
         ctx.close()
     (F64, J64), (F32, J32) = out
