@@ -568,6 +568,8 @@ def run_ours(args):
                torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")) for a, b in media]
     peak32 = R.rte.measure_fma_peak(False, dev)
     peak64 = R.rte.measure_fma_peak(True, dev)
+    streams = {k: R.rte.measure_fma_peak(device=dev, stream=k)
+               for k in ("fp32_scalar", "fp32_packed", "fp32_packed_fresh")}
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{dev}")
     counts = algorithmic_counts(N_SIDE, L)
 
@@ -715,7 +717,9 @@ def run_ours(args):
             "kernel_ms_per_step": {"pair": st["ms_pair"] / args.steps, "store": st["ms_store"] / args.steps,
                                    "epilogue": st["ms_epi"] / args.steps},
             "solve_tflops_canonical": B * counts["solve_flop"] / (ms / args.steps / 1e3) / 1e12,
-            "peaks_tflops": {"fp32": peak32, "fp64": peak64},
+            "peaks_tflops": {"fp32": peak32, "fp64": peak64, **streams,
+                             "streams": "fp32_* time one FP32 stream alone: scalar FMA, packed f32x2 FMA with "
+                                        "reused operands, packed with three distinct operand registers"},
         }
         if ws == 1 and not args.skip_cpu:
             line["cpu_baseline"] = cpu_baseline(args.ref_seconds)

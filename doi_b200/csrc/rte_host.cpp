@@ -1966,7 +1966,7 @@ extern "C" int rte_forward(rte_ctx* c, const rte_source* s, const rte_stop* stop
 }
 
 extern "C" int rte_measure_fma_peak(int device, int fp64, double* tflops) {
-  if (!tflops) return RTE_ERR_ARG;
+  if (!tflops || fp64 < 0 || fp64 > 4) return RTE_ERR_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return RTE_ERR_DEVICE;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1975,11 +1975,16 @@ extern "C" int rte_measure_fma_peak(int device, int fp64, double* tflops) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int blocks = sms * 8, iters = fp64 ? 20000 : 40000;
+  const int blocks = sms * 8, iters = fp64 == 1 ? 20000 : 40000;
   double best = 0;
-  // FP32: the faster of scalar and packed (f32x2) FMA streams
-  const int variants[2] = {fp64 ? 1 : 0, fp64 ? 1 : 2};
-  for (int v = 0; v < (fp64 ? 1 : 2); v++)
+  // mode 0: the faster of the scalar and packed (f32x2) FP32 streams; 1: FP64; 2: scalar FP32 only;
+  // 3: packed FP32 only; 4: packed FP32 with three distinct operands per instruction
+  int variants[2] = {0, 2}, nv = 2;
+  if (fp64 == 1) variants[0] = 1, nv = 1;
+  if (fp64 == 2) nv = 1;
+  if (fp64 == 3) variants[0] = 2, nv = 1;
+  if (fp64 == 4) variants[0] = 3, nv = 1;
+  for (int v = 0; v < nv; v++)
     for (int rep = 0; rep < 4; rep++) {
       cudaEventRecord(e0, 0);
       rte_launch_fma_peak(variants[v], iters, sink, 0, blocks);
@@ -1987,7 +1992,8 @@ extern "C" int rte_measure_fma_peak(int device, int fp64, double* tflops) {
       cudaEventSynchronize(e1);
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
-      const double flops = 2.0 * 8.0 * (double)iters * blocks * 256.0 * (variants[v] == 2 ? 2.0 : 1.0);
+      const double per_iter = variants[v] == 3 ? 24.0 : (variants[v] == 2 ? 16.0 : 8.0);  // FMAs per thread
+      const double flops = 2.0 * per_iter * (double)iters * blocks * 256.0;
       if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
     }
   cudaError_t e = cudaGetLastError();

@@ -1378,6 +1378,30 @@ __global__ void k_fma2_peak(int iters, float* sink) {
   if (s == -1.2345f) sink[blockIdx.x] = s;
 }
 
+// k_fma2_fresh_peak: packed FMAs whose three operands are all distinct registers (none shared with the
+// neighbouring instructions), the operand pattern of the pair kernels' source-row dot products.
+__global__ void k_fma2_fresh_peak(int iters, float* sink) {
+  f2_t a[12], x[12], y[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    a[q] = f2_pack((float)(threadIdx.x + q) * 1e-3f, (float)(threadIdx.x + 2 * q) * 1e-3f);
+    x[q] = f2_pack(0.9999f + (float)q * 1e-7f, 0.9998f + (float)q * 1e-7f);
+    y[q] = f2_pack(1e-7f * (float)(q + 1) + (float)threadIdx.x * 1e-9f, 2e-7f * (float)(q + 1));
+  }
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 12; ++q) a[q] = f2_fma(x[q], a[q], y[q]);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    float lo, hi;
+    f2_unpack(a[q], lo, hi);
+    s += lo + hi;
+  }
+  if (s == -1.2345f) sink[blockIdx.x] = s;
+}
+
 template <typename T>
 __global__ void k_fma_peak(int iters, float* sink) {
   T a[8];
@@ -2024,7 +2048,9 @@ cudaError_t rte_launch_medium(const double* mua, const double* mus, double* mut,
 }
 
 cudaError_t rte_launch_fma_peak(int fp64, int iters, float* sink, cudaStream_t st, int blocks) {
-  if (fp64 == 2)
+  if (fp64 == 3)
+    k_fma2_fresh_peak<<<blocks, 256, 0, st>>>(iters, sink);
+  else if (fp64 == 2)
     k_fma2_peak<<<blocks, 256, 0, st>>>(iters, sink);
   else if (fp64)
     k_fma_peak<double><<<blocks, 256, 0, st>>>(iters, sink);

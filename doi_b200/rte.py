@@ -234,11 +234,16 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
 
-def measure_fma_peak(fp64=False, device=0):
-    """Measured FMA throughput (TFLOP/s) of the device's CUDA cores."""
+FMA_STREAMS = {"fp32": 0, "fp64": 1, "fp32_scalar": 2, "fp32_packed": 3, "fp32_packed_fresh": 4}
+
+
+def measure_fma_peak(fp64=False, device=0, stream=None):
+    """Measured FMA throughput (TFLOP/s) of the device's CUDA cores: FP32 (the faster of the scalar and
+    packed streams) or FP64, or one named stream of FMA_STREAMS."""
     lib = load_library()
     v = ctypes.c_double(0.0)
-    rc = lib.rte_measure_fma_peak(device, int(bool(fp64)), ctypes.byref(v))
+    mode = FMA_STREAMS[stream] if stream is not None else int(bool(fp64))
+    rc = lib.rte_measure_fma_peak(device, mode, ctypes.byref(v))
     if rc != 0:
         raise RteError(f"rte_measure_fma_peak failed ({rc})")
     return v.value

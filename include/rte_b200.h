@@ -426,7 +426,9 @@ int rte_set_profiling(rte_ctx* ctx, int on);
 int rte_get_stats(rte_ctx* ctx, rte_stats* out);
 
 /* FP32 (fp64 = 0) or FP64 (fp64 = 1) FMA throughput of the device in TFLOP/s, measured with an
- * 8-chain FMA loop: the denominator of the roofline of the CUDA-core-bound kernels. */
+ * 8-chain FMA loop: the denominator of the roofline of the CUDA-core-bound kernels.  FP32 takes the
+ * faster of a scalar and a packed (f32x2) stream; fp64 = 2, 3 and 4 time one FP32 stream alone: scalar,
+ * packed, and packed with three distinct operand registers per instruction.  Other values: RTE_ERR_ARG. */
 int rte_measure_fma_peak(int device, int fp64, double* tflops);
 
 #ifdef __cplusplus

@@ -120,3 +120,11 @@ def test_preallocated_outputs_are_checked(rte):
                 np.zeros((2, 4, 8), np.complex128).transpose(0, 2, 1)):
         with pytest.raises(rte.RteError):
             rte.Context._outputs(None, {"W": bad}, shapes)
+
+
+def test_fma_peak_rejects_unknown_stream(rte):
+    """rte_measure_fma_peak takes modes 0-4 only; others are refused before any device call."""
+    lib = rte.load_library()
+    v = ctypes.c_double(0.0)
+    for mode in (-1, 5):
+        assert lib.rte_measure_fma_peak(0, mode, ctypes.byref(v)) == 1  # RTE_ERR_ARG
