@@ -459,25 +459,25 @@ def run_fisher_case(dev, n, Lq, nbins, terms, nsrc=6, P=32, kernel_mode=None, pr
 def run_fisher(dev, full_matrix_at_49=False):
     """Fisher information of 8 seeded inclusions x (x, y, z, mu_a contrast) = 32 parameters (BASELINE config
     5), Poisson noise, path integrals recomputed along every pair in every term (no stored pair kernel):
-    (1) the full configuration, 49^3, L=7, 16x16 bins, on a bounded leg of 1 source x 2 parameters (one
-    two-right-hand-side tangent series), extrapolated to 6 sources x 32 parameters; (2) the whole 32 x 32
+    (1) the full configuration, 49^3, L=7, 16x16 bins, on a bounded leg of 1 source x 4 parameters (one
+    four-right-hand-side tangent series), extrapolated to 6 sources x 32 parameters; (2) the whole 32 x 32
     matrix at 25^3, L=5; (3) its FP64 error on 1 source x 4 parameters against the FP64 method."""
     import doi_b200 as R
     out = {"workload": "8 inclusions x 4 = 32 parameters, 6 face-centre beams, 16x16 bins x 6 faces, 20 terms, "
                        "mixed precision, path integrals recomputed (no stored pair kernel)"}
     # (1) the full configuration, bounded
-    run_fisher_case(dev, 49, 7, 16, 2, nsrc=1, P=2)  # warm-up: split autotuning, buffers
+    run_fisher_case(dev, 49, 7, 16, 2, nsrc=1, P=4)  # warm-up: split autotuning, buffers
     if full_matrix_at_49:
         F, _, sec, t_fwd, st = run_fisher_case(dev, 49, 7, 16, TERMS)
         out["full_49_L7"] = {"seconds": sec, "measured": "6 sources x 32 parameters", "pair_kernel_ms": st["ms_pair"]}
     else:
-        F, _, sec, t_fwd, st = run_fisher_case(dev, 49, 7, 16, TERMS, nsrc=1, P=2)
+        F, _, sec, t_fwd, st = run_fisher_case(dev, 49, 7, 16, TERMS, nsrc=1, P=4)
         t_tan = max(sec - t_fwd, 0.0)
         out["full_49_L7"] = {
-            "measured": "1 source x 2 parameters (the forward solve and one two-right-hand-side tangent series)",
-            "seconds": sec, "forward_s_1src": t_fwd, "tangent_s_2params": t_tan,
-            "extrapolated_s_6src_32params": 6 * t_fwd + 6 * 16 * t_tan,
-            "extrapolation": "6 forward solves + 6 x 16 two-parameter tangent series at the measured rates",
+            "measured": "1 source x 4 parameters (the forward solve and one four-right-hand-side tangent series)",
+            "seconds": sec, "forward_s_1src": t_fwd, "tangent_s_4params": t_tan,
+            "extrapolated_s_6src_32params": 6 * t_fwd + 6 * 8 * t_tan,
+            "extrapolation": "6 forward solves + 6 x 8 four-parameter tangent series at the measured rates",
             "pair_kernel_ms": st["ms_pair"], "launches": st["launches"]}
     # (2) the whole matrix at 25^3, L=5
     F, _, sec, t_fwd, st = run_fisher_case(dev, 25, 5, 16, TERMS)

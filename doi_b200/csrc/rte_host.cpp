@@ -1041,6 +1041,11 @@ static const int kTkChunk = 1024;
 static bool tk_kernel(const rte_ctx* c, int stored, int cplx) {
   return c->precision == RTE_PREC_MIXED && stored && c->model != RTE_MODEL_FIM && !cplx;
 }
+// The recomputed four-right-hand-side kernel at L >= 6 (k_pair_mixed_grp: two thread groups sharing the
+// path walks) leaves FP32 chunk sums as well.
+static bool grp_kernel(const rte_ctx* c, int stored, int cplx, int nb, int LA) {
+  return c->precision == RTE_PREC_MIXED && !stored && c->model != RTE_MODEL_FIM && !cplx && nb == 4 && LA >= 6;
+}
 
 template <class T>
 static int grow(rte_ctx* c, T** p, size_t& cap, size_t n);
@@ -1061,9 +1066,10 @@ static int plan_split(rte_ctx* c, int LA, int stored, int nb, int* S_out, int* c
   CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
   const int tiles = (c->N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS;
   const bool tk = tk_kernel(c, stored, cplx);
-  const int Smin = tk ? (c->N + kTkChunk - 1) / kTkChunk : 1;
-  const int Smax = tk ? Smin + c->max_split : c->max_split;
-  if (tk) {  // partial sums of Smax chunks (before any capture: plan_split runs ahead of graph recording)
+  const bool chunked = tk || grp_kernel(c, stored, cplx, nb, LA);  // FP32 chunk sums, chunks capped
+  const int Smin = chunked ? (c->N + kTkChunk - 1) / kTkChunk : 1;
+  const int Smax = chunked ? Smin + c->max_split : c->max_split;
+  if (chunked) {  // partial sums of Smax chunks (before any capture: plan_split runs ahead of graph recording)
     int rc = grow(c, &c->d_part, c->part_cap, (size_t)c->N * c->C * nb * Smax);
     if (rc) return rc;
   }
@@ -1195,7 +1201,8 @@ static int apply_term(rte_ctx* c, const double* in64, const float* in32, double*
     if (rc) return rc;
     PairArgs a = pair_args(c, in64, in32, nb, S, chunk);
     a.tile = tile;
-    f32part = tk_kernel(c, stored ? 1 : 0, c->kappa != 0.0 ? 1 : 0);
+    f32part = tk_kernel(c, stored ? 1 : 0, c->kappa != 0.0 ? 1 : 0) ||
+              grp_kernel(c, stored ? 1 : 0, c->kappa != 0.0 ? 1 : 0, nb, LA);
     ProfScope ps(c, 0);
     CUDA_TRY(c, rte_launch_pair(a, LA, c->precision, c->model == RTE_MODEL_FIM ? 1 : 0, stored ? 1 : 0, c->st));
   }
@@ -3181,8 +3188,11 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   const int nb = d->nbins;
   const size_t NB2 = (size_t)6 * nb * nb;
   // tangent series run together: four at L <= 5 (the widest pair-kernel batch whose accumulators fit in
-  // registers), two above; the pair walk and the SH recurrence of every pair serve the whole group
-  const int nbt = c->precision == RTE_PREC_MIXED ? (c->L <= 5 ? 4 : 2) : 1;
+  // registers) and, with the path integrals recomputed, at L >= 6 (k_pair_mixed_grp: two thread groups
+  // of two sharing each pair's walk); two otherwise.  The pair walk (and at L <= 5 the SH recurrence) of
+  // every pair serves the whole group.
+  const bool recompute = c->kernel_mode == RTE_KERNEL_RECOMPUTE && c->model != RTE_MODEL_FIM;
+  const int nbt = c->precision == RTE_PREC_MIXED ? (c->L <= 5 || recompute ? 4 : 2) : 1;
   if (nbt > 1) {
     rc = ensure_batch(c, nbt);
     if (rc) return rc;

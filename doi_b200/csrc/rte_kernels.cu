@@ -996,6 +996,180 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_mixed_tk(PairArgs a) 
   }
 }
 
+// Recomputed pair kernel for four right-hand sides at L >= 6 (exact directions, real rows), where four
+// right-hand sides' FP32 sums no longer fit one thread's registers: 256 threads per CTA, the 128
+// destinations of a K block twice over, thread group g = tid / 128 holding right-hand sides 2g and
+// 2g + 1.  The path walks are shared: the kernel values of the CTA's 128 destinations x a 32-source tile
+// go to shared memory, each group walking half of the tile's sources, so every pair is walked once for
+// the four right-hand sides instead of once per pair of them.  The walks for tile t + 1 are interleaved
+// with the projections of tile t (one walk after every second source), so each thread's instruction
+// stream mixes the integer walk with the FMA work as the one-group kernels do.  FP32 sums stay in
+// registers over the source chunk (FP32 chunk partials, as k_pair_mixed_tk).
+struct GrpLayout {
+  size_t off_w, off_k, off_bar, bytes;
+  __host__ __device__ GrpLayout(int cpad, int ts) {
+    off_w = sizeof(float4) * 2 * ts;
+    off_k = off_w + sizeof(float) * 2 * ts * (size_t)cpad;  // cpad is a multiple of 4: 16-byte aligned
+    off_bar = off_k + sizeof(float) * 2 * ts * RTE_KBLK;
+    bytes = off_bar + 2 * sizeof(uint64_t);
+  }
+};
+#define RTE_GRP_THREADS (2 * RTE_KBLK)
+#define RTE_GRP_TS 32
+
+template <int LA>
+__global__ void __launch_bounds__(RTE_GRP_THREADS, 1) k_pair_mixed_grp(PairArgs a) {
+  constexpr int C = (LA + 1) * (LA + 1), C2 = (C + 1) / 2, TS = RTE_GRP_TS, NBG = 2, HALF = TS / 2;
+  typedef typename std::conditional<(LA >= 7), double, float>::type ShT;
+  constexpr bool V4 = LA < 7;  // 16-byte row loads (the one-group rule for two right-hand sides)
+  const int CP = a.cpad;
+  const GrpLayout Sh(CP, TS);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sP = reinterpret_cast<float4*>(smem_raw);
+  float* sW = reinterpret_cast<float*>(smem_raw + Sh.off_w);
+  float* sK = reinterpret_cast<float*>(smem_raw + Sh.off_k);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + Sh.off_bar);
+  const int tid = threadIdx.x;
+  const int d = tid & (RTE_KBLK - 1), g = tid / RTE_KBLK;
+  const int slot = blockIdx.x * RTE_KBLK + d;
+  const bool act = slot < a.N;
+  const float4 me = a.slot_xyz[act ? slot : 0];
+  const int r = __float_as_int(me.w);
+  const int plane = a.nx * a.ny;
+  const int i = (int)me.z, j = (int)me.y, k = (int)me.x;
+  const float dxf = (float)a.dx, dyf = (float)a.dy, dzf = (float)a.dz;
+  const float kscalef = (float)a.kscale, thr = (float)a.prop_thresh;
+  const int sb = blockIdx.y * a.chunk;
+  const int se = min(a.N, sb + a.chunk);
+  const int ntile = (se - sb + TS - 1) / TS;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int t) {  // source rows and coordinates of tile t -> buffer t & 1 (one thread)
+    const int s0 = sb + t * TS;
+    const int ns = min(TS, se - s0);
+    const int b = t & 1;
+    const uint32_t bw = (uint32_t)(ns * CP * sizeof(float)), bp = (uint32_t)(ns * sizeof(float4));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[b], bw + bp);
+    bulk_g2s(sW + b * TS * CP, a.Winf + (size_t)s0 * CP, bw, &bar[b]);
+    bulk_g2s(sP + b * TS, a.slot_xyz + s0, bp, &bar[b]);
+  };
+  // the pair kernel exp(-tau) dV/(cm r^2) of this destination and source q, as the one-group kernels
+  // recompute it (0 on the diagonal and beyond the coupling distance)
+  auto kval = [&](const float4 q) -> float {
+    const float ddx = (me.x - q.x) * dxf, ddy = (me.y - q.y) * dyf, ddz = (me.z - q.z) * dzf;
+    const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+    const float dist = sqrtf(d2);
+    if (!(d2 > 0.f && dist < thr)) return 0.f;
+    int Q;
+    const float ps = path_sum<float, float>(i, j, k, (int)q.z, (int)q.y, (int)q.x, a.mutf, a.nx, plane, Q);
+    return __expf(-ps * dist / (float)Q) * kscalef / d2;
+  };
+  f2_t acc[NBG][C2];
+#pragma unroll
+  for (int b = 0; b < NBG; ++b)
+#pragma unroll
+    for (int c = 0; c < C2; ++c) acc[b][c] = 0ull;
+  if (ntile > 0) {
+    if (tid == 0) issue(0);
+    const bool ok = mbar_wait(&bar[0], 0u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(a.err, 1);
+      return;
+    }
+    if (tid == 0 && ntile > 1) issue(1);
+    const int ns0 = min(TS, se - sb);
+    if (act)
+      for (int h = 0; h < HALF; ++h) {
+        const int sv = g * HALF + h;
+        if (sv < ns0) sK[sv * RTE_KBLK + d] = kval(sP[sv]);
+      }
+    __syncthreads();
+  }
+  const int CS = a.cstride;  // FP32 row stride of one right-hand side (a multiple of 4)
+  for (int t = 0; t < ntile; ++t) {
+    const bool has_next = t + 1 < ntile;
+    bool ok = true;
+    if (has_next) ok = mbar_wait(&bar[(t + 1) & 1], (uint32_t)(((t + 1) >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(a.err, 1);
+      return;
+    }
+    const int ns = min(TS, se - (sb + t * TS));
+    const int nsn = has_next ? min(TS, se - (sb + (t + 1) * TS)) : 0;
+    const float4* P = sP + (t & 1) * TS;
+    const float* Wt = sW + (t & 1) * TS * CP + 2 * g * CS;  // this group's two right-hand sides
+    const float* Kt = sK + (t & 1) * TS * RTE_KBLK + d;
+    const float4* Pn = sP + ((t + 1) & 1) * TS;
+    float* Kn = sK + ((t + 1) & 1) * TS * RTE_KBLK + d;
+    if (act) {
+      for (int sv = 0; sv < ns; ++sv) {
+        const float kk = Kt[sv * RTE_KBLK];
+        const float4 q = P[sv];
+        const float ddx = (me.x - q.x) * dxf, ddy = (me.y - q.y) * dyf, ddz = (me.z - q.z) * dzf;
+        const float d2 = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz));
+        const float inv = d2 > 0.f ? rsqrtf(d2) : 0.f;
+        ShT R[C];
+        sh_eval_monic<LA, ShT>((ShT)(ddx * inv), (ShT)(ddy * inv), (ShT)(ddz * inv), R);
+        f2_t R2[C2];
+#pragma unroll
+        for (int c = 0; c < C2; ++c) R2[c] = f2_pack((float)R[2 * c], 2 * c + 1 < C ? (float)R[2 * c + 1] : 0.f);
+#pragma unroll
+        for (int b = 0; b < NBG; ++b) {
+          f2_t Sa = 0ull, Sb = 0ull;
+          if constexpr (V4) {
+            const float4* w4 = reinterpret_cast<const float4*>(Wt + sv * CP + b * CS);
+#pragma unroll
+            for (int c = 0; c < C2; c += 2) {
+              const float4 v = w4[c / 2];
+              Sa = f2_fma(R2[c], f2_pack(v.x, v.y), Sa);
+              if (c + 1 < C2) Sb = f2_fma(R2[c + 1], f2_pack(v.z, v.w), Sb);
+            }
+          } else {
+            const f2_t* w = reinterpret_cast<const f2_t*>(Wt + sv * CP + b * CS);
+#pragma unroll
+            for (int c = 0; c < C2; c += 2) {
+              Sa = f2_fma(R2[c], w[c], Sa);
+              if (c + 1 < C2) Sb = f2_fma(R2[c + 1], w[c + 1], Sb);
+            }
+          }
+          float a0, a1, b0, b1;
+          f2_unpack(Sa, a0, a1);
+          f2_unpack(Sb, b0, b1);
+          const float tb = kk * ((a0 + a1) + (b0 + b1));
+          const f2_t T2 = f2_pack(tb, tb);
+#pragma unroll
+          for (int c = 0; c < C2; ++c) acc[b][c] = f2_fma(R2[c], T2, acc[b][c]);
+        }
+        if ((sv & 1) == 0) {  // one walk of the next tile after every second source
+          const int svn = g * HALF + (sv >> 1);
+          if (svn < nsn) Kn[svn * RTE_KBLK] = kval(Pn[svn]);
+        }
+      }
+      // a short last tile leaves walks of the next tile undone only when there is no next tile
+    }
+    __syncthreads();  // tile t's buffers are free, tile t + 1's kernel values complete
+    if (tid == 0 && t + 2 < ntile) issue(t + 2);
+  }
+  if (act) {  // the chunk's FP32 sums (the epilogue applies N_c after adding the chunks in FP64)
+    const int vstride = 2 * NBG * a.Cfull;
+    float* o = a.partf + ((size_t)blockIdx.y * a.N + r) * vstride + (size_t)(NBG * g) * a.Cfull;
+#pragma unroll
+    for (int b = 0; b < NBG; ++b)
+#pragma unroll
+      for (int c = 0; c < C2; ++c) {
+        float lo, hi;
+        f2_unpack(acc[b][c], lo, hi);
+        o[b * a.Cfull + 2 * c] = lo;
+        if (2 * c + 1 < C) o[b * a.Cfull + 2 * c + 1] = hi;
+      }
+  }
+}
+
 // Launch wrappers.  k_pair_mixed_3 carries a 3-CTA register bound and is used for L = 7 with one
 // right-hand side only; an explicit minimum-block count on the others makes ptxas take more registers
 // (L = 5, 2 RHS: 218 instead of 164, two CTAs per SM instead of three, 13.2 -> 17.0 ms per launch).
@@ -1916,6 +2090,16 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 // launchers
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
+  if constexpr (!STORED && !TABLE && !CPLX && NB == 4 && LA >= 6) {  // shared walks, two groups of two
+    const size_t smem = GrpLayout(a.cpad, RTE_GRP_TS).bytes;
+    void (*kern)(PairArgs) = k_pair_mixed_grp<LA>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_GRP_THREADS, smem);
+    dim3 grid((a.N + RTE_KBLK - 1) / RTE_KBLK, a.nsplit);
+    kern<<<grid, RTE_GRP_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   if constexpr (STORED && !TABLE && !CPLX) {  // K tiles staged with the source rows, 32 or 64 sources a tile
     const int ts = a.tile ? 64 : 32;
     const size_t smem = TkLayout(a.cpad, ts).bytes;

@@ -61,12 +61,13 @@ def test_sensitivity_matches_finite_differences(rte):
     ctx.close()
 
 
-@pytest.mark.parametrize("Lq,stored", [(2, True), (2, False), (5, False)])
+@pytest.mark.parametrize("Lq,stored", [(2, True), (2, False), (5, False), (7, False)])
 def test_fisher_mixed_vs_fp64(rte, Lq, stored):
     """Mixed precision against the FP64 method, with the stored FP32 kernel or with the path integrals
     recomputed in every term (the Fisher benchmark's form): J and F within 1e-5 (measured 1.6e-7 and
-    2.3e-7 at L = 2, stored).  The 8 parameters run as two groups of four tangent series.  F weights bins
-    by 1/flux, so on detectors with near-zero-flux bins its relative error can exceed J's."""
+    2.3e-7 at L = 2, stored).  The 8 parameters run as two groups of four tangent series (at L = 7 with
+    the kernel whose two thread groups share each pair's walk).  F weights bins by 1/flux, so on detectors
+    with near-zero-flux bins its relative error can exceed J's."""
     stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-12)
     det = rte.Detector(nbins=3, faces=63)
     out = []

@@ -170,6 +170,27 @@ def test_forward_batch_matches_single(rte, oracle, n, L):
     ctx.close()
 
 
+@pytest.mark.parametrize("n,L", [(7, 6), (7, 7), (11, 6)])
+def test_forward_batch_recomputed_high_order(rte, oracle, n, L):
+    """Four sources, path integrals recomputed, L >= 6: the kernel whose two thread groups share each
+    pair's walk (k_pair_mixed_grp) against four single solves (1e-6) and the FP64 oracle (1e-5); 11^3
+    has 1331 voxels, more than one 1024-source chunk, so the FP32 chunk sums meet in the epilogue."""
+    mua, mus, _ = rte.sphere_phantom(n, nspheres=2, seed=5, rmin=0.15, rmax=0.25)
+    srcs = [rte.Source(pos_x=x, pos_y=y) for x, y in ((-0.2, -0.2), (0.2, -0.2), (-0.2, 0.2), (0.0, 0.0))]
+    stop = rte.Stop(rte.STOP_FIXED, 8)
+    ctx, p = _ctx(rte, oracle, n, n, n, L, rte.MODEL_EXACT, rte.PREC_MIXED, kernel_mode=rte.KERNEL_RECOMPUTE)
+    ctx.set_medium_voxel(mua, mus)
+    rb = ctx.forward_batch(srcs, stop)
+    for b, s in enumerate(srcs):
+        single = ctx.forward(s, stop)
+        assert rel(rb["W"][b], single["W"]) < 1e-6, (b, rel(rb["W"][b], single["W"]))
+        ref = oracle.forward(p, mua, mus, src_kind=oracle.SRC_COLUMN, img_mode=0, stop_rule=oracle.STOP_FIXED,
+                             max_terms=8, pos_x=s.pos_x, pos_y=s.pos_y)
+        assert rel(rb["W"][b], ref["out"]) < 1e-5, (b, rel(rb["W"][b], ref["out"]))
+        assert rel(rb["trans"][b], ref["trans"]) < 1e-5
+    ctx.close()
+
+
 @pytest.mark.parametrize("prec,tol", [(0, 1e-11), (1, 1e-9)])
 def test_uniform_medium_convolution_path(rte, oracle, prec, tol):
     """A uniform medium in automatic kernel mode runs the operator as an FFT convolution: the same
