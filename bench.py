@@ -748,7 +748,7 @@ def run_profile(args):
     """Small single-purpose runs for ncu captures (no timing line): --profile-grad N runs one mixed-
     precision gradient of the config-4 problem at N^3 (4 sources, 8x8 bins, 20 terms); --profile-fisher N
     one mixed-precision Fisher information at N^3, L=5 (1 face beam, 8 parameters, 16x16 bins, path
-    integrals recomputed); --profile-uniform N three forward solves of a uniform N^3, L=5 medium through
+    integrals recomputed; --profile-order 7: L=7 and 4 parameters); --profile-uniform N three forward solves of a uniform N^3, L=5 medium through
     the FFT convolution path."""
     import doi_b200 as R
     if args.profile_grad:
@@ -757,8 +757,10 @@ def run_profile(args):
         ctx.close()
         print(json.dumps({"profile": "gradient", "n": args.profile_grad, "loss": loss}))
     if args.profile_fisher:
-        F = run_fisher_case(0, args.profile_fisher, 5, 16, TERMS, nsrc=1, P=8, kernel_mode=R.KERNEL_RECOMPUTE)[0]
-        print(json.dumps({"profile": "fisher", "n": args.profile_fisher, "F_trace": float(np.trace(F))}))
+        Lq = args.profile_order
+        F = run_fisher_case(0, args.profile_fisher, Lq, 16, TERMS, nsrc=1, P=8 if Lq <= 5 else 4,
+                            kernel_mode=R.KERNEL_RECOMPUTE)[0]
+        print(json.dumps({"profile": "fisher", "n": args.profile_fisher, "L": Lq, "F_trace": float(np.trace(F))}))
     if args.profile_uniform:
         n = args.profile_uniform
         with R.Context(n, n, n, dx=DX, nL=L, g=0.8, precision=R.PREC_MIXED, kernel_mode=R.KERNEL_AUTO) as ctx:
@@ -789,6 +791,8 @@ def main():
                     help="requests in the serving stream (0 = skip; 2000 = the full stream)")
     ap.add_argument("--profile-grad", type=int, default=0, help="one config-4 gradient at this grid side, then exit")
     ap.add_argument("--profile-fisher", type=int, default=0, help="one Fisher information at this grid side, then exit")
+    ap.add_argument("--profile-order", type=int, default=5, choices=[5, 7],
+                    help="SH order of --profile-fisher (5: 8 parameters; 7: 4 parameters, one four-RHS series)")
     ap.add_argument("--profile-uniform", type=int, default=0,
                     help="three uniform-medium solves (FFT convolution path) at this grid side, then exit")
     ap.add_argument("--serve-requests-33", type=int, default=32,

@@ -256,67 +256,7 @@ __device__ __forceinline__ void table_direction(double ddx, double ddy, double d
   uz = ct;
 }
 
-// Radiological path sum_v mu_t(v) len(v) between the centres of voxels (i,j,k) and (ip,jp,kp).
-// Axis crossings are compared as integers: with m_a = max(D_a, 1) and Q = 2 m_x m_y m_z, the
-// n-th crossing on axis a is at alpha*Q = (2n+1) * Q / (2 m_a).  Ties step z, then y, then x
-// (as mu_int); a tie leaves a zero-length segment, so the order does not change the sum.
-template <typename A, typename MU>
-__device__ __forceinline__ A path_sum(int i, int j, int k, int ip, int jp, int kp, const MU* __restrict__ mu,
-                                      int nx, int plane, int& Q) {
-  const int Dz = abs(ip - i), Dy = abs(jp - j), Dx = abs(kp - k);
-  const int mz = max(Dz, 1), my = max(Dy, 1), mx = max(Dx, 1);
-  Q = 2 * mx * my * mz;
-  if constexpr (std::is_same<A, float>::value) {
-    // FP32 sums: the crossing parameters are integers below 2^24 and so exact in FP32, which gives the
-    // same segments and the same sum without an integer-to-float conversion per step
-    if (Q < (1 << 24)) {
-      const float incz = (float)(2 * mx * my), incy = (float)(2 * mx * mz), incx = (float)(2 * my * mz);
-      float Az = Dz ? (float)(mx * my) : 3.0e38f, Ay = Dy ? (float)(mx * mz) : 3.0e38f,
-            Ax = Dx ? (float)(my * mz) : 3.0e38f;
-      const int stz = ip > i ? plane : -plane, sty = jp > j ? nx : -nx, stx = kp > k ? 1 : -1;
-      int v = i * plane + j * nx + k;
-      float prev = 0.f, acc = 0.f;
-      const int steps = Dx + Dy + Dz;
-      for (int s = 0; s < steps; ++s) {
-        const float m = fminf(Az, fminf(Ay, Ax));
-        acc = fmaf((float)__ldg(mu + v), m - prev, acc);
-        prev = m;
-        const bool bz = Az == m;
-        const bool by = !bz && (Ay == m);
-        const bool bx = !bz && !by;
-        v += bz ? stz : (by ? sty : stx);
-        Az += bz ? incz : 0.f;
-        Ay += by ? incy : 0.f;
-        Ax += bx ? incx : 0.f;
-      }
-      acc = fmaf((float)__ldg(mu + v), (float)Q - prev, acc);
-      return acc;
-    }
-  }
-  const int BIG = 0x3fffffff;
-  const int incz = 2 * mx * my, incy = 2 * mx * mz, incx = 2 * my * mz;
-  int Az = Dz ? mx * my : BIG, Ay = Dy ? mx * mz : BIG, Ax = Dx ? my * mz : BIG;
-  const int stz = ip > i ? plane : -plane, sty = jp > j ? nx : -nx, stx = kp > k ? 1 : -1;
-  int v = i * plane + j * nx + k;
-  int prev = 0;
-  A acc = A(0);
-  const int steps = Dx + Dy + Dz;
-  for (int s = 0; s < steps; ++s) {
-    const int m = min(Az, min(Ay, Ax));
-    const A muv = (A)__ldg(mu + v);
-    acc = fma(muv, (A)(m - prev), acc);
-    prev = m;
-    const bool bz = Az == m;
-    const bool by = !bz && (Ay == m);
-    const bool bx = !bz && !by;
-    v += bz ? stz : (by ? sty : stx);
-    Az += bz ? incz : 0;
-    Ay += by ? incy : 0;
-    Ax += bx ? incx : 0;
-  }
-  acc = fma((A)__ldg(mu + v), (A)(Q - prev), acc);
-  return acc;
-}
+#include "rte_walk.cuh"
 
 // ---------------------------------------------------------------------------------------------
 // Plain FP64 method: every pair recomputed in FP64 (path integral, SH, projections).  CPLX: one
@@ -543,7 +483,7 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
         const T dist = sqrt(d2);
         if (dist < thr) {
           int Q;
-          const T dps = path_sum<T, double>(i, j, k, ip, jp, kp, a.dmut, a.nx, plane, Q);
+          const T dps = path_sum_box<T, double>(i, j, k, ip, jp, kp, a.dmut, a.nx, plane, a.box_lo, a.box_hi, Q);
           if (dps != T(0)) {
             const T dtau = dps * dist / (T)Q;
             T kk;
