@@ -449,6 +449,59 @@ __device__ __forceinline__ bool segment_hits_box(float ax, float ay, float az, f
   return true;
 }
 
+// Real SH of a direction for the FP32 (or FP64) pair arithmetic of type T: at L >= 7 the recurrence runs
+// in FP64 (the monic form of the mixed pair kernels, normalised as each value is rounded to T).
+template <int LA, typename T>
+__device__ __forceinline__ void sh_eval_prec(T x, T y, T z, T* R) {
+  if constexpr (LA < 7 || std::is_same<T, double>::value) {
+    sh_eval<LA, T>(x, y, z, R);
+  } else {  // the recurrence of sh_eval_monic in FP64, each value normalised and rounded as it is made
+    const double xd = x, yd = y, zd = z;
+    double cmv = 1.0, smv = 0.0;
+#pragma unroll
+    for (int m = 0; m <= LA; ++m) {
+      if (m == 1) {
+        cmv = xd;
+        smv = yd;
+      } else if (m > 1) {
+        const double c2 = cmv * xd - smv * yd;
+        const double s2 = cmv * yd + smv * xd;
+        cmv = c2;
+        smv = s2;
+      }
+      double c1 = cmv, s1 = smv, c0 = 0.0, s0 = 0.0;
+      if (m == 0) {
+        R[0] = (T)kMonic.N[0];
+      } else {
+        R[m * m + 2 * m] = (T)(cmv * kMonic.N[m * m + 2 * m]);
+        R[m * m] = (T)(smv * kMonic.N[m * m]);
+      }
+#pragma unroll
+      for (int l = m + 1; l <= LA; ++l) {
+        double cn, sn = 0.0;
+        if (l == m + 1) {
+          cn = m == 0 ? zd : zd * c1;
+          if (m > 0) sn = zd * s1;
+        } else {
+          const double b = kMonic.beta[l * (l + 1) / 2 + m];
+          cn = fma(zd, c1, -b * c0);
+          if (m > 0) sn = fma(zd, s1, -b * s0);
+        }
+        c0 = c1;
+        c1 = cn;
+        s0 = s1;
+        s1 = sn;
+        if (m == 0) {
+          R[l * l + l] = (T)(cn * kMonic.N[l * l + l]);
+        } else {
+          R[l * l + l + m] = (T)(cn * kMonic.N[l * l + l + m]);
+          R[l * l + l - m] = (T)(sn * kMonic.N[l * l + l - m]);
+        }
+      }
+    }
+  }
+}
+
 template <int LA, bool TABLE, typename T>
 __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
   constexpr int C = (LA + 1) * (LA + 1);
@@ -500,10 +553,10 @@ __global__ void __launch_bounds__(RTE_PAIR_THREADS) k_pair_tangent(PairArgs a) {
             if (TABLE) {
               double ux, uy, uz;
               table_direction((double)ddx, (double)ddy, (double)ddz, (double)dist, ux, uy, uz);
-              sh_eval<LA, T>((T)ux, (T)uy, (T)uz, R);
+              sh_eval_prec<LA, T>((T)ux, (T)uy, (T)uz, R);
             } else {
               const T inv = T(1) / dist;
-              sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
+              sh_eval_prec<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
             }
             T S = T(0);
 #pragma unroll
@@ -1727,6 +1780,11 @@ __global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
   T* ys = reinterpret_cast<T*>(smem_raw);             // [64][C] y of the tile's sources
   T* Ss = ys + RTE_KT * C;                             // [64][C] S of the tile's sources
   int* sx = reinterpret_cast<int*>(Ss + RTE_KT * C);   // [64][3] source coordinates
+  // FP32 sums at L >= 6: the destination's own y and S rows live in shared memory ([2][C][64], one
+  // column per thread) instead of 2C registers, which leaves room for the FP64 SH recurrence at L >= 7
+  // (the FP64 kernel keeps them in registers: in shared memory they would halve its CTAs per SM)
+  constexpr bool DST_SMEM = C >= 49 && sizeof(T) == 4;
+  T* sD = reinterpret_cast<T*>(sx + RTE_KT * 3);
   const int ntile = (a.N + RTE_KT - 1) / RTE_KT;
   int bd, bs;
   tri_tile(blockIdx.x, bd, bs);
@@ -1753,11 +1811,17 @@ __global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
   if (d >= a.N) return;
   const int r = a.perm[d];
   const int k = r % a.nx, j = (r / a.nx) % a.ny, i = r / plane;
-  T yd[C], Sd[C];
+  T yd[DST_SMEM ? 1 : C], Sd[DST_SMEM ? 1 : C];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
-    yd[c] = (T)a.y[(size_t)r * a.Cfull + c];
-    Sd[c] = (T)a.S[(size_t)r * a.Cfull + c];
+    const T yv = (T)a.y[(size_t)r * a.Cfull + c], Sv = (T)a.S[(size_t)r * a.Cfull + c];
+    if constexpr (DST_SMEM) {
+      sD[c * RTE_KT + tid] = yv;
+      sD[(C + c) * RTE_KT + tid] = Sv;
+    } else {
+      yd[c] = yv;
+      Sd[c] = Sv;
+    }
   }
   const T dxf = (T)a.dx, dyf = (T)a.dy, dzf = (T)a.dz, thr = (T)a.prop_thresh, ks = (T)a.kscale;
   T* Qp = reinterpret_cast<T*>(a.Q);
@@ -1783,17 +1847,19 @@ __global__ void __launch_bounds__(RTE_KT) k_bp_weights(BpArgs a) {
       }
       const T inv = T(1) / dist;
       T R[C];
-      sh_eval<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
+      sh_eval_prec<LA, T>(ddx * inv, ddy * inv, ddz * inv, R);
       const T* yq = ys + q * C;
       const T* Sq = Ss + q * C;
       T a1 = T(0), b1 = T(0), a2 = T(0), b2 = T(0);
 #pragma unroll
       for (int c = 0; c < C; ++c) {
         const T Rp = (l_of_c(c) & 1) ? -R[c] : R[c];
-        a1 = fma(yd[c], R[c], a1);
+        const T ydc = DST_SMEM ? sD[c * RTE_KT + tid] : yd[DST_SMEM ? 0 : c];
+        const T Sdc = DST_SMEM ? sD[(C + c) * RTE_KT + tid] : Sd[DST_SMEM ? 0 : c];
+        a1 = fma(ydc, R[c], a1);
         b1 = fma(R[c], Sq[c], b1);
         a2 = fma(yq[c], Rp, a2);
-        b2 = fma(Rp, Sd[c], b2);
+        b2 = fma(Rp, Sdc, b2);
       }
       w = kk * (a1 * b1 + a2 * b2);
     }
@@ -2331,7 +2397,7 @@ cudaError_t rte_launch_y_field(double* y, const double* e, const double* lam, co
 template <int LA, typename T>
 static cudaError_t launch_bpw(const BpArgs& a, cudaStream_t st) {
   constexpr int C = (LA + 1) * (LA + 1);
-  const size_t smem = (size_t)RTE_KT * C * 2 * sizeof(T) + RTE_KT * 3 * sizeof(int);
+  const size_t smem = (size_t)RTE_KT * C * 2 * sizeof(T) * (C >= 49 && sizeof(T) == 4 ? 2 : 1) + RTE_KT * 3 * sizeof(int);
   cudaError_t e = cudaFuncSetAttribute(k_bp_weights<LA, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long nt = (a.N + RTE_KT - 1) / RTE_KT;

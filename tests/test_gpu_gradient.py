@@ -54,11 +54,14 @@ def test_gradient_matches_finite_differences(rte):
     ctx.close()
 
 
-def test_gradient_mixed_vs_fp64(rte):
-    c64, mua, mus, srcs, stop, det, target = _setup(rte, rte.PREC_FP64)
+@pytest.mark.parametrize("L", [2, 7])
+def test_gradient_mixed_vs_fp64(rte, L):
+    """At L = 7 the back-projection keeps the destination rows in shared memory and runs the SH
+    recurrence in FP64."""
+    c64, mua, mus, srcs, stop, det, target = _setup(rte, rte.PREC_FP64, L=L)
     _, ga64, gs64 = c64.gradient(srcs, stop, det, target)
     c64.close()
-    c32, *_ = _setup(rte, rte.PREC_MIXED)
+    c32, *_ = _setup(rte, rte.PREC_MIXED, L=L)
     _, ga32, gs32 = c32.gradient(srcs, stop, det, target)
     c32.close()
     assert rel(ga32, ga64) < 1e-5 and rel(gs32, gs64) < 1e-5, (rel(ga32, ga64), rel(gs32, gs64))
