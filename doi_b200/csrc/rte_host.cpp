@@ -1006,6 +1006,9 @@ static int tune_split(rte_ctx* c, int LA, int stored, int nb, const std::vector<
   CUDA_TRY(c, cudaEventCreate(&e1));
   double best = 1e30;
   cudaError_t err = cudaSuccess;
+  // each launch is checked with cudaGetLastError: clear what an earlier call of this thread left there
+  // (a failure handled where it happened, or one inside a library), so it is not read as a launch's
+  (void)cudaGetLastError();
   for (const auto& cand : cands) {
     PairArgs a = pair_args(c, in64, in32, nb, cand.S, split_chunk(c->N, cand.S));
     a.tile = cand.tile;
@@ -2131,8 +2134,11 @@ extern "C" int rte_forward_batch(rte_ctx* c, int nsrc, const rte_source* srcs, c
   if (stop->rule == RTE_STOP_REFERENCE)
     return fail(c, RTE_ERR_UNSUPPORTED, "batched solves take a fixed or relative-L2 stop rule");
   const size_t NC = (size_t)c->N * c->C, np = (size_t)c->nx * c->ny;
-  if (c->L >= 6 && nsrc > 2 && c->precision == RTE_PREC_MIXED) {
-    // four right-hand sides of 49-64 coefficients exceed the registers (spills): two batches of two
+  // four right-hand sides of 49-64 coefficients exceed one thread's registers: at L >= 6 the recomputed
+  // path integrals take k_pair_mixed_grp (two thread groups of two sharing the walks), the other forms
+  // run two batches of two
+  const bool grp = c->kernel_mode == RTE_KERNEL_RECOMPUTE && c->model != RTE_MODEL_FIM && c->kappa == 0.0;
+  if (c->L >= 6 && nsrc > 2 && c->precision == RTE_PREC_MIXED && !grp) {
     rte_report r1, r2;
     int rc = rte_forward_batch(c, 2, srcs, stop, W_out, trans, ref, &r1);
     if (!rc)
@@ -3218,7 +3224,16 @@ extern "C" int rte_fisher(rte_ctx* c, int nsrc, const rte_source* srcs, const rt
   for (int si = 0; si < nsrc; si++) {
     const rte_source* s = &srcs[si];
     int terms = 0;
-    rc = forward_with_flux(c, s, stop, Jpix, &terms);  // S -> d_S, out -> d_out
+    // the forward solve (S -> d_S, out -> d_out, flux -> Jpix) by the FP64 method, path integrals
+    // recomputed: F weights every bin by 1 / flux, and in the mixed series the flux of dim bins
+    // (1e-6..1e-4 of the brightest) carries up to ~1e-4 relative error, which F inherits (25^3 L=5, 6
+    // beams: F 5.4e-5 from FP64 with mixed forward solves, 1.9e-6 with FP64 ones; J 2.5e-6 either way)
+    const int prec = c->precision, mode = c->kernel_mode;
+    c->precision = RTE_PREC_FP64;
+    if (prec != RTE_PREC_FP64) c->kernel_mode = RTE_KERNEL_RECOMPUTE;
+    rc = forward_with_flux(c, s, stop, Jpix, &terms);
+    c->precision = prec;
+    c->kernel_mode = mode;
     if (rc) return rc;
     bin_faces(c, d, Jpix, ybar.data());
     std::vector<int> cols;

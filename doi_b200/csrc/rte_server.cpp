@@ -194,6 +194,7 @@ static void worker_main(rte_server* s) {
       rte_report rep;
       r->trans.assign((size_t)r->rq.nsrc * r->rq.n * r->rq.n, rte_cplx{0, 0});
       r->ref.assign(r->trans.size(), rte_cplx{0, 0});
+      (void)cudaGetLastError();  // a handled failure of an earlier request on this thread is not this one's
       rc = rte_forward_graph(sl->ctx, r->rq.nsrc, r->rq.src, r->rq.terms, r->trans.data(), r->ref.data(), &rep);
       r->device_ms = rep.ms_device;
     }

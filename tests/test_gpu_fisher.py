@@ -79,3 +79,40 @@ def test_fisher_mixed_vs_fp64(rte, Lq, stored):
     (F64, J64), (F32, J32) = out
     assert rel(J32, J64) < 1e-5, rel(J32, J64)
     assert rel(F32, F64) < 1e-5, rel(F32, F64)
+
+
+def test_fisher_adds_over_sources(rte):
+    """F is a sum over sources: two sources in one call against the sum of two one-source calls, mixed
+    precision, path integrals recomputed, L = 5 (four-parameter tangent groups)."""
+    stop = rte.Stop(rte.STOP_REL_L2, 600, 1e-12)
+    det = rte.Detector(nbins=3, faces=63)
+    ctx, sph, srcs, mua, mus, dmua, dmus = _problem(rte, rte.PREC_MIXED, rte.KERNEL_RECOMPUTE, 5)
+    F2, J2 = ctx.fisher(srcs, stop, det, dmua, dmus, want_J=True)
+    F0, J0 = ctx.fisher(srcs[:1], stop, det, dmua, dmus, want_J=True)
+    F1, J1 = ctx.fisher(srcs[1:], stop, det, dmua, dmus, want_J=True)
+    ctx.close()
+    assert rel(J2[0], J0[0]) < 1e-6 and rel(J2[1], J1[0]) < 1e-6, (rel(J2[0], J0[0]), rel(J2[1], J1[0]))
+    assert rel(F2, F0 + F1) < 1e-6, rel(F2, F0 + F1)
+
+
+def test_fisher_six_beams_mixed_vs_fp64(rte):
+    """Six face-centre beams on a strongly scattering medium (mu_s 2, g 0.9), 16x16 bins on every face:
+    the detector has dim bins, whose 1/flux weights amplify flux errors in F.  Mixed precision (FP64
+    forward solves, mixed tangent series) against the FP64 method: F and J within 1e-5."""
+    n, Lq = 17, 3
+    stop = rte.Stop(rte.STOP_FIXED, 20)
+    det = rte.Detector(nbins=16, faces=63)
+    sph = rte.random_spheres(n, 2, seed=7, rmin=0.2, rmax=0.3)
+    mua, mus, dmua, dmus = rte.smooth_sphere_phantom(n, sph, mua_bg=0.02, mus_bg=2.0)
+    h = n * 0.1 / 2
+    srcs = [rte.Source(kind=rte.SRC_BEAM, face=0), rte.Source(kind=rte.SRC_BEAM, face=1, pos_z=n * 0.1)] + \
+           [rte.Source(kind=rte.SRC_BEAM, face=f, pos_z=h) for f in (2, 3, 4, 5)]
+    out = {}
+    for prec in (rte.PREC_FP64, rte.PREC_MIXED):
+        ctx = rte.Context(n, n, n, dx=0.1, nL=Lq, g=0.9, precision=prec, kernel_mode=rte.KERNEL_RECOMPUTE)
+        ctx.set_medium_voxel(mua, mus)
+        out[prec] = ctx.fisher(srcs, stop, det, dmua, dmus, want_J=True)
+        ctx.close()
+    (F64, J64), (F32, J32) = out[rte.PREC_FP64], out[rte.PREC_MIXED]
+    assert rel(J32, J64) < 1e-5, rel(J32, J64)
+    assert rel(F32, F64) < 1e-5, rel(F32, F64)
