@@ -2094,12 +2094,28 @@ __global__ void k_f64_to_f32(const double* a, float* b, size_t n) {
 
 // ---------------------------------------------------------------------------------------------
 // launchers
+
+// Dynamic shared memory above 48 KB for a kernel: the attribute is set to the device's opt-in maximum,
+// the same value from every host thread, not to one launch's size.  The size a launch needs can depend
+// on the context (the lower-order passes of a pair kernel size their source rows by the context's own
+// order), and the server launches the same instantiation from several worker threads; per-launch values
+// let one thread lower the limit between another thread's set and launch, which fails that launch with
+// an invalid-argument error.  Each launch still asks for its own size.
+static cudaError_t allow_smem(const void* kern, size_t smem) {
+  int dev = 0, cap = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (smem > (size_t)cap) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
 template <int LA, bool TABLE, bool STORED, int NB, bool CPLX = false>
 static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
   if constexpr (!STORED && !TABLE && !CPLX && NB == 4 && LA >= 6) {  // shared walks, two groups of two
     const size_t smem = GrpLayout(a.cpad, RTE_GRP_TS).bytes;
     void (*kern)(PairArgs) = k_pair_mixed_grp<LA>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_smem((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_GRP_THREADS, smem);
     dim3 grid((a.N + RTE_KBLK - 1) / RTE_KBLK, a.nsplit);
@@ -2110,7 +2126,7 @@ static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
     const int ts = a.tile ? 64 : 32;
     const size_t smem = TkLayout(a.cpad, ts).bytes;
     void (*kern)(PairArgs) = a.tile ? k_pair_mixed_tk<LA, NB, 64> : k_pair_mixed_tk<LA, NB, 32>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_smem((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
     dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
@@ -2123,7 +2139,7 @@ static cudaError_t launch_mixed(const PairArgs& a, cudaStream_t st, int* occ) {
     kern = k_pair_mixed_3<LA, TABLE, STORED, NB, CPLX>;
   else
     kern = k_pair_mixed<LA, TABLE, STORED, NB, CPLX>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)kern, smem);
   if (e != cudaSuccess) return e;
   if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, RTE_PAIR_THREADS, smem);
   dim3 grid((a.N + RTE_PAIR_THREADS - 1) / RTE_PAIR_THREADS, a.nsplit);
@@ -2398,7 +2414,7 @@ template <int LA, typename T>
 static cudaError_t launch_bpw(const BpArgs& a, cudaStream_t st) {
   constexpr int C = (LA + 1) * (LA + 1);
   const size_t smem = (size_t)RTE_KT * C * 2 * sizeof(T) * (C >= 49 && sizeof(T) == 4 ? 2 : 1) + RTE_KT * 3 * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_bp_weights<LA, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_bp_weights<LA, T>, smem);
   if (e != cudaSuccess) return e;
   const long long nt = (a.N + RTE_KT - 1) / RTE_KT;
   k_bp_weights<LA, T><<<(unsigned)(nt * (nt + 1) / 2), RTE_KT, smem, st>>>(a);
@@ -2433,7 +2449,7 @@ static cudaError_t launch_walk(BpArgs a, cudaStream_t st) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   a.use_smem = base + (size_t)a.N * sizeof(T) <= (size_t)maxsm ? 1 : 0;
   const size_t smem = base + (a.use_smem ? (size_t)a.N * sizeof(T) : 0);
-  cudaError_t e = cudaFuncSetAttribute(k_bp_walk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = allow_smem((const void*)k_bp_walk<T>, smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bp_walk<T>, RTE_BPW_THREADS, smem);
