@@ -83,3 +83,19 @@ def test_budget_and_cancel(rte):
         st = srv.stats()
     assert st["failed"] == 1 and st["cancelled"] == sum(cancelled)
     assert st["completed"] == 4 - sum(cancelled)
+
+
+def test_orders_run_concurrently(rte):
+    """Requests of orders 3, 5 and 7 on 17^3 grids (large enough for the launch autotuner) from four
+    workers at once: the lower-order passes of a pair kernel size their shared memory by the context's
+    order, so contexts of different orders configure the same kernels concurrently.  Every request
+    completes and equals the same request alone (1e-6, mixed precision)."""
+    rng = np.random.default_rng(11)
+    n, terms = 17, 4
+    reqs = [(Lq,) + _request(rte, rng, n, Lq, 1) for Lq in (3, 5, 7, 3, 5, 7, 5, 3)]
+    with rte.Server(workers=4) as srv:
+        tickets = [srv.submit(mua, mus, srcs, n, dx=DX, nL=Lq, terms=terms) for Lq, mua, mus, srcs in reqs]
+        outs = [srv.wait(t, timeout=600) for t in tickets]
+    for (Lq, mua, mus, srcs), (tr, rf, info) in zip(reqs, outs):
+        tr0, rf0 = _alone(rte, n, Lq, rte.PREC_MIXED, mua, mus, srcs, terms)
+        assert rel(tr, tr0) < 1e-6 and rel(rf, rf0) < 1e-6, (Lq, rel(tr, tr0), rel(rf, rf0))
