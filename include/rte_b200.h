@@ -248,7 +248,9 @@ int rte_fisher_regions(rte_ctx* ctx, const rte_source* src, const rte_stop* stop
  * attenuation operator recomputes the path integral of the parameter direction along every voxel
  * pair), giving J = d(binned exitant flux)/d(parameter) on the detector of rte_detector_flux; with
  * Poisson counts F = sum over sources and bins with flux > 0 of J_b,p J_b,q / flux_b.  Exact for the
- * discrete model when the series converge (RTE_STOP_REL_L2 with a small tolerance).  J (may be NULL):
+ * discrete model when the series converge (RTE_STOP_REL_L2 with a small tolerance).  In a
+ * mixed-precision context the forward solves (whose fluxes weight every bin) run by the FP64 method
+ * with the path integrals recomputed, and the tangent solves in mixed precision.  J (may be NULL):
  * nsrc * 6 * nbins^2 rows of P.  F: P x P.  Sources: RTE_SRC_COLUMN, RTE_SRC_FIM, RTE_SRC_BEAM. */
 int rte_fisher(rte_ctx* ctx, int nsrc, const rte_source* srcs, const rte_stop* stop, const rte_detector* det,
                int P, const double* dmua, const double* dmus, double* J, double* F);
