@@ -188,8 +188,10 @@ constexpr MonicTab make_monic() {
 }
 __device__ constexpr MonicTab kMonic = make_monic();
 
-template <int L, typename T>
-__device__ __forceinline__ void sh_eval_monic(T x, T y, T z, T* U) {
+// The monic recurrence, each coefficient handed to emit(index, value) as it is made (the index is a
+// compile-time constant once the loops unroll).
+template <int L, typename T, typename Emit>
+__device__ __forceinline__ void sh_monic_recurrence(T x, T y, T z, Emit emit) {
   T cmv = T(1), smv = T(0);
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
@@ -204,10 +206,10 @@ __device__ __forceinline__ void sh_eval_monic(T x, T y, T z, T* U) {
     }
     T c1 = cmv, s1 = smv, c0 = T(0), s0 = T(0);
     if (m == 0) {
-      U[0] = T(1);
+      emit(0, T(1));
     } else {
-      U[m * m + 2 * m] = cmv;
-      U[m * m] = smv;
+      emit(m * m + 2 * m, cmv);
+      emit(m * m, smv);
     }
 #pragma unroll
     for (int l = m + 1; l <= L; ++l) {
@@ -225,13 +227,18 @@ __device__ __forceinline__ void sh_eval_monic(T x, T y, T z, T* U) {
       s0 = s1;
       s1 = sn;
       if (m == 0) {
-        U[l * l + l] = cn;
+        emit(l * l + l, cn);
       } else {
-        U[l * l + l + m] = cn;
-        U[l * l + l - m] = sn;
+        emit(l * l + l + m, cn);
+        emit(l * l + l - m, sn);
       }
     }
   }
+}
+
+template <int L, typename T>
+__device__ __forceinline__ void sh_eval_monic(T x, T y, T z, T* U) {
+  sh_monic_recurrence<L, T>(x, y, z, [&](int c, T v) { U[c] = v; });
 }
 
 // Direction snapped to the reference's 100x100 SH table cell (FisherInfo_IO/src/defines.h:53-56
@@ -455,50 +462,9 @@ template <int LA, typename T>
 __device__ __forceinline__ void sh_eval_prec(T x, T y, T z, T* R) {
   if constexpr (LA < 7 || std::is_same<T, double>::value) {
     sh_eval<LA, T>(x, y, z, R);
-  } else {  // the recurrence of sh_eval_monic in FP64, each value normalised and rounded as it is made
-    const double xd = x, yd = y, zd = z;
-    double cmv = 1.0, smv = 0.0;
-#pragma unroll
-    for (int m = 0; m <= LA; ++m) {
-      if (m == 1) {
-        cmv = xd;
-        smv = yd;
-      } else if (m > 1) {
-        const double c2 = cmv * xd - smv * yd;
-        const double s2 = cmv * yd + smv * xd;
-        cmv = c2;
-        smv = s2;
-      }
-      double c1 = cmv, s1 = smv, c0 = 0.0, s0 = 0.0;
-      if (m == 0) {
-        R[0] = (T)kMonic.N[0];
-      } else {
-        R[m * m + 2 * m] = (T)(cmv * kMonic.N[m * m + 2 * m]);
-        R[m * m] = (T)(smv * kMonic.N[m * m]);
-      }
-#pragma unroll
-      for (int l = m + 1; l <= LA; ++l) {
-        double cn, sn = 0.0;
-        if (l == m + 1) {
-          cn = m == 0 ? zd : zd * c1;
-          if (m > 0) sn = zd * s1;
-        } else {
-          const double b = kMonic.beta[l * (l + 1) / 2 + m];
-          cn = fma(zd, c1, -b * c0);
-          if (m > 0) sn = fma(zd, s1, -b * s0);
-        }
-        c0 = c1;
-        c1 = cn;
-        s0 = s1;
-        s1 = sn;
-        if (m == 0) {
-          R[l * l + l] = (T)(cn * kMonic.N[l * l + l]);
-        } else {
-          R[l * l + l + m] = (T)(cn * kMonic.N[l * l + l + m]);
-          R[l * l + l - m] = (T)(sn * kMonic.N[l * l + l - m]);
-        }
-      }
-    }
+  } else {  // the monic recurrence in FP64, each value normalised and rounded as it is made
+    sh_monic_recurrence<LA, double>((double)x, (double)y, (double)z,
+                                    [&](int c, double v) { R[c] = (T)(v * kMonic.N[c]); });
   }
 }
 
