@@ -2507,9 +2507,11 @@ __device__ __forceinline__ double fft_sign(int set, bool c_even, bool cp_even) {
 
 // The two real systems of a frequency run on adjacent lanes (set = lane parity), so the pair's table
 // loads are one memory transaction and the table spectrum (larger than L2 at benchmark sizes) streams
-// from HBM once per right-hand side instead of once per set.
+// from HBM once per right-hand side instead of once per set.  Three CTAs per SM (168 registers, a small
+// spill) keep more table loads in flight than two at 255 registers: 33^3 L=5 uniform solve 23.6 -> 22.5
+// ms (four CTAs: 22.4 ms with a 3 KB spill).
 template <int LA>
-__global__ void __launch_bounds__(128) k_fft_product_reg(const double* tau, const double2* Wh, double2* Oh, int C,
+__global__ void __launch_bounds__(128, 3) k_fft_product_reg(const double* tau, const double2* Wh, double2* Oh, int C,
                                                          int nb, size_t Mk) {
   constexpr int CA = (LA + 1) * (LA + 1);
   __shared__ double sv[CA][128];  // this thread's inputs of its set (column tid)
